@@ -1,0 +1,223 @@
+"""Host-side mirror of the reference's ``struct system`` hot-path interface.
+
+The reference drives its fluid update through argument-free member functions
+of ``fvmhd3d::system`` (MPI/fvmhd3d.h:298-575):
+
+    fluid_update(true)  = slope_limiter, compute_update, compute_pvel,
+                          compute_timesteps(false)      (MPI/iterate.cpp:97-107)
+    fluid_update(false) = compute_update0, compute_reconstruction
+                                                        (MPI/iterate.cpp:108-112)
+
+:class:`System` keeps those names and that order over the C-ABI of
+``libfvmhd3d_b200.so`` (include/fvmhd3d_b200.h); all arrays live on the GPU
+inside the context.  Errors raise :class:`FvmError` (the reference aborts on
+a failed ``assert``).
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .mesh import Mesh
+
+FVM_PREC_FP64 = 0
+FVM_PREC_FP32 = 1
+
+
+class FvmError(RuntimeError):
+    pass
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+class System:
+    """One context on one CUDA device (one rank of the reference)."""
+
+    def __init__(self, gamma=5.0 / 3.0, courant=0.4, box=(1.0, 1.0, 1.0), dtmax=1.0 / 64, eos=0,
+                 iso_GM=1.0, iso_cfac=0.05, precision=FVM_PREC_FP64, device=0):
+        self.L = _lib.lib()
+        prm = _lib.FvmParams()
+        prm.gamma, prm.courant = gamma, courant
+        box = np.broadcast_to(np.asarray(box, dtype=np.float64), (3,))
+        for a in range(3):
+            prm.box[a] = float(box[a])
+        prm.dtmax, prm.eos, prm.iso_GM, prm.iso_cfac, prm.precision = dtmax, eos, iso_GM, iso_cfac, precision
+        self.params = prm
+        h = self.L.fvm_create(ctypes.byref(prm), int(device))
+        if not h:
+            raise FvmError("fvm_create failed (no CUDA device?)")
+        self.h = ctypes.c_void_p(h)
+        self.mesh: Mesh | None = None
+
+    # -- lifetime ---------------------------------------------------------
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.fvm_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, what):
+        if rc < 0:
+            raise FvmError(f"{what}: rc={rc}: {self.L.fvm_last_error(self.h).decode()}")
+        return rc
+
+    # -- inputs -----------------------------------------------------------
+    def set_mesh(self, m: Mesh):
+        self.mesh = m
+        arrs = [np.ascontiguousarray(m.s1, np.int32), np.ascontiguousarray(m.s2, np.int32),
+                np.ascontiguousarray(m.n, np.float64), np.ascontiguousarray(m.centroid, np.float64),
+                np.ascontiguousarray(m.volume, np.float64), np.ascontiguousarray(m.cell_centroid, np.float64),
+                np.ascontiguousarray(m.cell_face_off, np.int64), np.ascontiguousarray(m.cell_face_ids, np.int32)]
+        self._check(self.L.fvm_set_mesh(self.h, m.ncell, m.nface, *[_p(a) for a in arrs]), "fvm_set_mesh")
+
+    def init_problem(self, W, bnd=None, rung_offset=0):
+        W = np.ascontiguousarray(W, np.float64)
+        pos = np.ascontiguousarray(self.mesh.pos, np.float64)
+        b = None if bnd is None else np.ascontiguousarray(bnd, np.int32)
+        self._check(self.L.fvm_init_problem(self.h, _p(W), _p(pos), _p(b), int(rung_offset)), "fvm_init_problem")
+
+    # -- the reference call sequence --------------------------------------
+    def begin_step(self):
+        return self._check(self.L.fvm_begin_step(self.h), "fvm_begin_step")
+
+    def slope_limiter(self):
+        self._check(self.L.fvm_slope_limiter(self.h), "fvm_slope_limiter")
+
+    def compute_update(self):
+        self._check(self.L.fvm_compute_update(self.h), "fvm_compute_update")
+
+    def compute_pvel(self):
+        self._check(self.L.fvm_compute_pvel(self.h), "fvm_compute_pvel")
+
+    def compute_timesteps(self, shared=False):
+        dt = ctypes.c_double(0.0)
+        self._check(self.L.fvm_compute_timesteps(self.h, int(bool(shared)), ctypes.byref(dt)),
+                    "fvm_compute_timesteps")
+        return dt.value
+
+    def collect_results(self):
+        self._check(self.L.fvm_collect_results(self.h), "fvm_collect_results")
+
+    def compute_update0(self):
+        self._check(self.L.fvm_compute_update0(self.h), "fvm_compute_update0")
+
+    def compute_reconstruction(self):
+        self._check(self.L.fvm_compute_reconstruction(self.h), "fvm_compute_reconstruction")
+
+    def end_step(self, shared=False):
+        return self._check(self.L.fvm_end_step(self.h, int(bool(shared))), "fvm_end_step")
+
+    def fluid_update(self, flag: bool, shared=False):
+        """system::fluid_update (MPI/iterate.cpp:95-113)."""
+        if flag:
+            self.slope_limiter()
+            self.compute_update()
+            self.compute_pvel()
+            self.compute_timesteps(shared)
+        else:
+            self.compute_update0()
+            self.compute_reconstruction()
+
+    def iterate_step(self, shared=True):
+        """One step of the reference's iterate_step on the fixed mesh; returns
+        the number of active cells."""
+        return self._check(self.L.fvm_step(self.h, int(bool(shared))), "fvm_step")
+
+    step = iterate_step
+
+    # -- outputs ----------------------------------------------------------
+    @property
+    def time(self) -> float:
+        return self.L.fvm_time(self.h)
+
+    @property
+    def tsys_ticks(self) -> int:
+        return int(self.L.fvm_tsys_ticks(self.h))
+
+    def get_state(self) -> dict:
+        n = self.mesh.ncell
+        st = dict(pos=np.zeros((n, 3)), vel=np.zeros((n, 3)), tlast=np.zeros(n), tend=np.zeros(n),
+                  rung=np.zeros(n, np.int32), U=np.zeros((n, 10)), dU=np.zeros((n, 14)), wrec=np.zeros((n, 50)))
+        self._check(self.L.fvm_get_state(self.h, *[_p(st[k]) for k in
+                                                   ("pos", "vel", "tlast", "tend", "rung", "U", "dU", "wrec")]),
+                    "fvm_get_state")
+        return st
+
+    def set_state(self, vel=None, tlast=None, tend=None, rung=None, U=None, dU=None, wrec=None, tsys_ticks=0):
+        conv = [None if a is None else np.ascontiguousarray(a, t) for a, t in
+                ((vel, np.float64), (tlast, np.float64), (tend, np.float64), (rung, np.int32),
+                 (U, np.float64), (dU, np.float64), (wrec, np.float64))]
+        self._check(self.L.fvm_set_state(self.h, *[_p(a) for a in conv], ctypes.c_ulonglong(tsys_ticks)),
+                    "fvm_set_state")
+
+    def active_faces(self) -> np.ndarray:
+        n = ctypes.c_int(0)
+        self._check(self.L.fvm_get_active_faces(self.h, None, ctypes.byref(n)), "fvm_get_active_faces")
+        ids = np.zeros(max(n.value, 1), np.int32)
+        self._check(self.L.fvm_get_active_faces(self.h, _p(ids), ctypes.byref(n)), "fvm_get_active_faces")
+        return ids[: n.value]
+
+    def limited_wrec(self) -> np.ndarray:
+        out = np.zeros((self.mesh.ncell, 50))
+        self._check(self.L.fvm_get_limited_wrec(self.h, _p(out)), "fvm_get_limited_wrec")
+        return out
+
+    def dt_list(self) -> np.ndarray:
+        out = np.zeros(self.mesh.ncell)
+        self._check(self.L.fvm_get_dt_list(self.h, _p(out)), "fvm_get_dt_list")
+        return out
+
+    def step_dU(self) -> np.ndarray:
+        out = np.zeros((self.mesh.ncell, 14))
+        self._check(self.L.fvm_get_step_dU(self.h, _p(out)), "fvm_get_step_dU")
+        return out
+
+    def counters(self) -> np.ndarray:
+        out = np.zeros(2, np.int64)
+        self._check(self.L.fvm_get_counters(self.h, _p(out)), "fvm_get_counters")
+        return out
+
+    def compute_flux(self, wij, Wi, Wj, jbnd, normal):
+        nf = Wi.shape[0]
+        wij, Wi, Wj, normal = (np.ascontiguousarray(a, np.float64) for a in (wij, Wi, Wj, normal))
+        jb = np.ascontiguousarray(jbnd, np.int32)
+        psi, Bn, flux = np.zeros(nf), np.zeros(nf), np.zeros((nf, 10))
+        self._check(self.L.fvm_compute_flux(self.h, nf, _p(wij), _p(Wi), _p(Wj), _p(jb), _p(normal),
+                                            _p(psi), _p(Bn), _p(flux)), "fvm_compute_flux")
+        return psi, Bn, flux
+
+    def last_step_ms(self) -> float:
+        return float(self.L.fvm_last_step_ms(self.h))
+
+    @property
+    def stream_ptr(self) -> int:
+        """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
+        return int(self.L.fvm_stream(self.h) or 0)
+
+    @property
+    def launch_count(self) -> int:
+        return int(self.L.fvm_launch_count(self.h))
+
+    def set_profiling(self, on=True):
+        self._check(self.L.fvm_set_profiling(self.h, int(bool(on))), "fvm_set_profiling")
+
+    def kernel_times(self) -> dict:
+        """{kernel class: (total ms, timed launches)} since set_profiling."""
+        out = {}
+        k = 0
+        name = ctypes.c_char_p()
+        ms = ctypes.c_double()
+        calls = ctypes.c_longlong()
+        while self.L.fvm_kernel_times(self.h, k, ctypes.byref(name), ctypes.byref(ms), ctypes.byref(calls)) == 1:
+            out[name.value.decode()] = (ms.value, calls.value)
+            k += 1
+        return out

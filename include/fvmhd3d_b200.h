@@ -1,0 +1,163 @@
+/*
+ * fvmhd3d_b200: C-ABI of the B200 (sm_100a) fluid hot path of fvmhd3d.
+ *
+ * The reference has no plugin or FFI layer: its hot path is a sequence of
+ * argument-free member functions of `struct system` (MPI/fvmhd3d.h:298-575)
+ * called from system::fluid_update (MPI/iterate.cpp:95-113) inside
+ * system::iterate_step (MPI/iterate.cpp:115-247), operating on member arrays.
+ * This header exposes the same sequence over a context that owns the device
+ * copies of those arrays.  Each entry point names the reference function it
+ * replaces.
+ *
+ * Conventions
+ *   - Return 0 on success, a negative FVM_E* code on error; the message is in
+ *     fvm_last_error().  No C++ exception crosses this boundary and no kernel
+ *     traps: kernels record failures in device counters read by the host.
+ *   - Host buffers are owned by the caller and only read/written during the
+ *     call.  Device buffers are owned by the context.
+ *   - One host thread per context; all work is ordered on the context's
+ *     CUDA stream.
+ *   - Layouts are row-major, one record per cell or face:
+ *       W, U      ncell x 10  (primitive / conserved, MPI/Fluid.h:9-32 order)
+ *       dU        ncell x 14  (dU[10], gradPsi[3], divB; MPI/Fluid.h:163-172)
+ *       wrec      ncell x 50  (w, x, y, z, t blocks; MPI/Fluid.h:147-161)
+ *       pos, vel  ncell x 3   (generator position / velocity)
+ *       n, c      nface x 3   (area-weighted normal s1->s2; centroid in the
+ *                              periodic frame of s1; MPI/fvmhd3d.h:169-191)
+ */
+#ifndef FVMHD3D_B200_H
+#define FVMHD3D_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  FVM_OK = 0,
+  FVM_EINVAL = -1,    /* bad argument or call order */
+  FVM_ECUDA = -2,     /* CUDA runtime error */
+  FVM_ENOMEM = -3,    /* device allocation failed */
+  FVM_ENOMESH = -4,   /* no mesh / state installed yet */
+  FVM_ERANGE = -5     /* a rung left [0, 32) or a size limit was exceeded */
+};
+
+enum { FVM_PREC_FP64 = 0, FVM_PREC_FP32 = 1 };
+
+typedef struct fvm_params {
+  double gamma;     /* system::gamma_gas */
+  double courant;   /* system::courant_no */
+  double box[3];    /* system::global_domain_size (periodic box) */
+  double dtmax;     /* Scheduler(dtmax), MPI/Scheduler.h:17-30 */
+  int eos;          /* 0: ideal gas (MPI/set_problem.cpp:123-137);
+                       1: isothermal disk (MPI/problems/mri_disk3d.cpp:368-389) */
+  double iso_GM;    /* disk: cs^2(r) = iso_GM/|r| * iso_cfac^2 */
+  double iso_cfac;
+  int precision;    /* FVM_PREC_FP64 (plain path) or FVM_PREC_FP32 */
+} fvm_params;
+
+typedef struct fvm_ctx fvm_ctx;
+
+/* Creates a context on CUDA device `device`.  Replaces the construction of
+ * `system` and its Scheduler (MPI/fvmhd3d.h:537-552, MPI/Scheduler.h:17-30). */
+fvm_ctx *fvm_create(const fvm_params *p, int device);
+void fvm_destroy(fvm_ctx *c);
+const char *fvm_last_error(const fvm_ctx *c);
+
+/* Installs the Voronoi mesh (copied to the device).  Replaces the cell_list /
+ * face_list produced by system::build_mesh_active
+ * (MPI/build_mesh_active.cpp:663-851).  cell_face_off has ncell+1 entries. */
+int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
+                 const double *n, const double *centroid, const double *cell_volume,
+                 const double *cell_centroid, const long long *cell_face_off,
+                 const int *cell_face_ids);
+
+/* Initial state from primitives W, following the tail of the reference's
+ * set_problem (MPI/problems/mri_disk3d.cpp:832-880): Wrec=(W,0,0,0,0),
+ * U=cons(W), dU=0, compute_pvel, compute_timesteps(true), rung += rung_offset,
+ * tend = dt(rung).  bnd may be NULL (no boundary cells). */
+int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *bnd,
+                     int rung_offset);
+
+/* Full per-cell state between steps (any pointer may be NULL).  set_state also
+ * sets the scheduler clock (integer ticks of dtmax/2^31). */
+int fvm_get_state(fvm_ctx *c, double *pos, double *vel, double *tlast, double *tend, int *rung,
+                  double *U, double *dU, double *wrec);
+int fvm_set_state(fvm_ctx *c, const double *vel, const double *tlast, const double *tend,
+                  const int *rung, const double *U, const double *dU, const double *wrec,
+                  unsigned long long tsys_ticks);
+
+/* ---- the reference's step, one entry point per member function ---------- */
+
+/* system::get_active_ptcl(false) + Scheduler::pull_active_list + the site
+ * flags of build_mesh_active + system::get_active_faces
+ * (MPI/iterate.cpp:12-93, MPI/Scheduler.h:108-154,
+ * MPI/build_mesh_active.cpp:524-528).  Returns the number of active cells. */
+int fvm_begin_step(fvm_ctx *c);
+/* system::slope_limiter (MPI/compute_reconstruction.cpp:201-602) */
+int fvm_slope_limiter(fvm_ctx *c);
+/* system::compute_update (MPI/compute_update.cpp:22-499) */
+int fvm_compute_update(fvm_ctx *c);
+/* system::compute_pvel (MPI/compute_pvel.cpp:5-52) */
+int fvm_compute_pvel(fvm_ctx *c);
+/* system::compute_timesteps(false) + adjust_timesteps
+ * (MPI/compute_timestep.cpp:54-207).  shared != 0 puts every active cell on
+ * the rung of the global minimum (the effect of compute_timesteps(true)).
+ * dt_min_out (may be NULL) receives the global minimum timestep. */
+int fvm_compute_timesteps(fvm_ctx *c, int shared, double *dt_min_out);
+/* system::collect_results + distribute_fluid_update_data
+ * (MPI/distribute_work.cpp:537-797), one rank */
+int fvm_collect_results(fvm_ctx *c);
+/* system::compute_update0 (MPI/compute_update.cpp:695-970) */
+int fvm_compute_update0(fvm_ctx *c);
+/* system::compute_reconstruction (MPI/compute_reconstruction.cpp:24-199) */
+int fvm_compute_reconstruction(fvm_ctx *c);
+/* system::collect_reconstruction (MPI/distribute_work.cpp:799-864) and the
+ * rung re-insertion of iterate_step (MPI/iterate.cpp:199-217) */
+int fvm_end_step(fvm_ctx *c, int shared);
+
+/* One full step: begin_step, slope_limiter, compute_update, compute_pvel,
+ * compute_timesteps, collect_results, compute_update0, compute_reconstruction,
+ * end_step.  Returns the number of active cells. */
+int fvm_step(fvm_ctx *c, int shared);
+
+/* ---- inspection ----------------------------------------------------------- */
+
+double fvm_time(const fvm_ctx *c);                       /* system::t_global */
+unsigned long long fvm_tsys_ticks(const fvm_ctx *c);     /* Scheduler::tsysU */
+/* face_active_list of the current step as face ids, in the reference order
+ * (MPI/iterate.cpp:58-93); *n receives the count.  ids may be NULL. */
+int fvm_get_active_faces(fvm_ctx *c, int *ids, int *n);
+/* Wrec of the current step as the reference holds it after slope_limiter:
+ * x, y, z, t scaled by the per-cell limiter for imported cells. */
+int fvm_get_limited_wrec(fvm_ctx *c, double *wrec);
+/* dU_import after compute_update (ncell x 14). */
+int fvm_get_step_dU(fvm_ctx *c, double *dU);
+/* Per-cell timestep list of the last compute_timesteps (ncell). */
+int fvm_get_dt_list(fvm_ctx *c, double *dt);
+/* Device counters: [0] cells that took the failed-mass fallback of
+ * compute_update, [1] cells whose thermal energy went non-positive. */
+int fvm_get_counters(fvm_ctx *c, long long *out2);
+
+/* Per-face known-answer entry: system::compute_flux
+ * (MPI/compute_update.cpp:973-1095) on nface given face states, host
+ * buffers in and out. */
+int fvm_compute_flux(fvm_ctx *c, int nface, const double *wij, const double *Wi, const double *Wj,
+                     const int *jbnd, const double *normal, double *psi, double *Bn, double *flux);
+
+/* Timing helper: CUDA-event time in ms of the last fvm_step's kernels. */
+float fvm_last_step_ms(const fvm_ctx *c);
+/* The context's CUDA stream (a cudaStream_t), for callers that order their
+ * own work or events after the context's kernels. */
+void *fvm_stream(fvm_ctx *c);
+/* Number of kernels this context has launched so far. */
+long long fvm_launch_count(const fvm_ctx *c);
+/* Per-kernel CUDA-event timing: on != 0 enables it and clears the totals. */
+int fvm_set_profiling(fvm_ctx *c, int on);
+/* Totals of kernel class k (0, 1, ...): name, summed ms and number of
+ * timed launches.  Returns 1 while k is valid, 0 past the last class. */
+int fvm_kernel_times(const fvm_ctx *c, int k, const char **name, double *total_ms, long long *calls);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,46 @@
+"""Shared helpers for the parity tests."""
+import os
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_SO = os.path.join(ROOT, "oracle", "_ref", "libfvmref.so")
+ORACLE_SO = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
+
+# Tolerance of the plain FP64 GPU path against the FP64 oracle: per
+# variable, max |gpu - oracle| over cells divided by max |oracle| over cells.
+RTOL_FP64 = 1e-12
+
+
+def maxrel(a, b, axis=0):
+    """Per-column max-norm relative error of a against b."""
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    if a.ndim == 1:
+        a, b = a[:, None], b[:, None]
+    den = np.abs(b).max(axis=axis)
+    den = np.where(den > 0, den, 1.0)
+    return np.abs(a - b).max(axis=axis) / den
+
+
+def setup_case(nside=8, problem="alfven", seed=1, noise=0.05, gamma=5.0 / 3.0):
+    import fvmhd3d_b200 as F
+    m = F.build_periodic(F.jittered_lattice(nside, 0.1, seed=seed), 1.0)
+    W = getattr(F.problems, problem)(m.pos)
+    if noise:
+        W = F.problems.perturbed(W, noise, seed=seed + 100)
+    return m, W
+
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GOLDEN_STEP_CASES = ["ref_alfven4_shared.npz", "ref_ot5_shared.npz", "ref_blast7_individual.npz",
+                     "ref_blast8_individual.npz"]
+
+
+def load_golden(name):
+    """(mesh, fixture dict) of a golden fixture written by golden/make_golden.py."""
+    from fvmhd3d_b200.mesh import Mesh
+    z = dict(np.load(os.path.join(GOLDEN, name)))
+    m = Mesh(z["box"], z["pos"], z["s1"], z["s2"], z["n"], z["centroid"], z["volume"], z["cell_centroid"],
+             z["cell_face_off"], z["cell_face_ids"])
+    return m, z

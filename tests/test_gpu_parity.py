@@ -1,0 +1,130 @@
+"""Parity of the plain FP64 CUDA path with the FP64 oracle, through the
+C-ABI.  Tolerance: RTOL_FP64 = 1e-12 per variable (max-norm relative over
+cells); integer data (rungs, active sets, face lists) must match exactly."""
+import os
+
+import numpy as np
+import pytest
+
+from common import GOLDEN, GOLDEN_STEP_CASES, RTOL_FP64, load_golden, maxrel, setup_case
+
+pytestmark = pytest.mark.gpu
+
+
+def gpu_system(m, W, **kw):
+    import fvmhd3d_b200 as F
+    s = F.System(**kw)
+    s.set_mesh(m)
+    s.init_problem(W)
+    return s
+
+
+def oracle_system(m, W):
+    from oracle.pyoracle import OracleSystem
+    o = OracleSystem()
+    o.set_mesh(m)
+    o.init_problem(W)
+    return o
+
+
+def assert_state_close(a, b, rtol=RTOL_FP64, mask=None):
+    sel = slice(None) if mask is None else mask
+    for k in ("U", "wrec", "dU", "vel"):
+        e = maxrel(a[k][sel], b[k][sel])
+        assert e.max() <= rtol, (k, e.max(), int(e.argmax()))
+    for k in ("rung", "tend", "tlast"):
+        assert np.array_equal(a[k][sel], b[k][sel]), k
+
+
+def test_flux_kat_vs_reference_golden():
+    import fvmhd3d_b200 as F
+    z = np.load(os.path.join(GOLDEN, "ref_flux_kat.npz"))
+    s = F.System()
+    psi, Bn, flux = s.compute_flux(z["wij"], z["Wi"], z["Wj"], z["jbnd"], z["normal"])
+    assert maxrel(psi, z["psi"]).max() <= RTOL_FP64
+    assert maxrel(Bn, z["Bn"]).max() <= RTOL_FP64
+    assert maxrel(flux, z["flux"]).max() <= RTOL_FP64
+
+
+@pytest.mark.parametrize("name", GOLDEN_STEP_CASES)
+def test_steps_vs_reference_golden(name):
+    m, z = load_golden(name)
+    s = gpu_system(m, z["W"])
+    nact = [s.step(shared=bool(z["shared"])) for _ in range(int(z["nsteps"]))]
+    assert nact == list(z["out_nactive"])
+    assert np.array_equal(s.active_faces(), z["out_last_active_faces"])
+    st = s.get_state()
+    ref = {k[4:]: z[k] for k in z if k.startswith("out_")}
+    assert_state_close(st, ref)
+    assert s.time == float(z["out_time"])
+
+
+@pytest.mark.parametrize("shared", [True, False])
+def test_stage_by_stage_vs_oracle(shared):
+    m, W = setup_case(8, "blast", seed=12, noise=0.05)
+    s, o = gpu_system(m, W), oracle_system(m, W)
+    for _ in range(6):
+        snap = o.step(shared=shared, snap=True)
+        act_o = o.get_state()["tlast"] == o.time
+        s.begin_step()
+        assert np.array_equal(s.active_faces(), snap["active_faces"])
+        s.slope_limiter()
+        lw = s.limited_wrec()
+        imp = act_o.copy()
+        ngb = np.zeros(m.ncell, bool)
+        for f in snap["active_faces"]:
+            ngb[m.s1[f]] = ngb[m.s2[f]] = True
+        imp |= ngb
+        assert maxrel(lw[imp], snap["wrec_after_limiter"][imp]).max() <= RTOL_FP64
+        s.compute_update()
+        s.compute_pvel()
+        s.compute_timesteps(shared)
+        s.collect_results()
+        s.compute_update0()
+        s.compute_reconstruction()
+        s.end_step(shared)
+        a = s.get_state()
+        assert np.array_equal(a["tlast"] == s.time, act_o)
+        assert maxrel(a["U"][act_o], snap["U_after_update"][act_o]).max() <= RTOL_FP64
+        assert maxrel(a["vel"][act_o], snap["vel_after_pvel"][act_o]).max() <= RTOL_FP64
+        assert maxrel(a["wrec"][act_o], snap["wrec_after_recon"][act_o]).max() <= RTOL_FP64
+        assert_state_close(a, o.get_state())
+
+
+def test_alfven_32cubed_10_steps_vs_oracle():
+    """Configuration 1 at full size: circularly polarised Alfven wave, 32^3
+    jittered generators, global timestep, 10 steps."""
+    m, W = setup_case(32, "alfven", seed=1, noise=0.0)
+    s, o = gpu_system(m, W), oracle_system(m, W)
+    for _ in range(10):
+        assert s.step(shared=True) == o.step(shared=True) == m.ncell
+    assert s.time == o.time
+    assert_state_close(s.get_state(), o.get_state())
+
+
+def test_blast_individual_timesteps_vs_oracle():
+    m, W = setup_case(16, "blast", seed=4, noise=0.02)
+    s, o = gpu_system(m, W), oracle_system(m, W)
+    counts = []
+    for _ in range(12):
+        a, b = s.step(shared=False), o.step(shared=False)
+        assert a == b
+        counts.append(a)
+        assert s.time == o.time
+    assert min(counts) < m.ncell  # partial steps were exercised
+    assert_state_close(s.get_state(), o.get_state())
+
+
+def test_conservation_blast():
+    """Fluxes are antisymmetric per face, so total mass, momentum and energy
+    are conserved to round-off on a periodic mesh."""
+    m, W = setup_case(24, "blast", seed=6, noise=0.0)
+    s = gpu_system(m, W)
+    U0 = s.get_state()["U"].sum(axis=0)
+    for _ in range(15):
+        s.step(shared=True)
+    U1 = s.get_state()["U"].sum(axis=0)
+    scale = np.abs(s.get_state()["U"]).sum(axis=0)
+    for k in (0, 1, 2, 3, 4):
+        assert abs(U1[k] - U0[k]) <= 1e-13 * scale[k], k
+    assert s.counters().tolist() == [0, 0]

@@ -85,23 +85,27 @@ __global__ void k_ngbflags(int n, const int *__restrict__ off, const int *__rest
 }
 
 // ---- slope_limiter (MPI/compute_reconstruction.cpp:201-602) --------------
-// One thread per imported cell: face pass 1 (min/max of neighbour
-// differences) and face pass 2 (per-face limiter of the space+time
-// extrapolated difference) over the cell's active faces.  The result tau is
-// applied on the fly by the corrector, so the stored Wrec is not modified.
+// Two threads per imported cell, each owning five of the ten primitives: face
+// pass 1 (min/max of neighbour differences) and face pass 2 (limiter of the
+// space+time extrapolated difference) over the cell's active faces.  The
+// result tau is applied on the fly by the corrector, so Wrec is not modified.
+constexpr int KH = 5;  // primitives per thread in the two-threads-per-cell kernels
+
 __global__ void __launch_bounds__(128) k_limiter(int n, Params P, double t_global,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ cen,
     const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const double *__restrict__ pos, const double *__restrict__ tlast,
     const double *__restrict__ Wrec, double *__restrict__ tau) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = (int)(t >> 1);
+  const int k0 = (int)(t & 1) * KH;
   if (i >= n) return;
   if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
-  const double *ri = Wrec + 50 * (size_t)i;
-  double mn[NF], mx[NF], lim[NF];
+  const double *ri = Wrec + 50 * (size_t)i + k0;
+  double mn[KH], mx[KH], lim[KH], wi[KH];
 #pragma unroll
-  for (int k = 0; k < NF; k++) { mn[k] = 0.0; mx[k] = 0.0; lim[k] = 1.0; }
+  for (int k = 0; k < KH; k++) { mn[k] = 0.0; mx[k] = 0.0; lim[k] = 1.0; wi[k] = ri[k]; }
   const int q0 = off[i], q1 = off[i + 1];
   bool zero = false;
   for (int q = q0; q < q1; q++) {
@@ -110,19 +114,23 @@ __global__ void __launch_bounds__(128) k_limiter(int n, Params P, double t_globa
     if (!face_active(act, bnd, e.x, e.y)) continue;
     if (bnd[e.x] != NO_BOUNDARY || bnd[e.y] != NO_BOUNDARY) { zero = true; continue; }
     const int j = e.x == i ? e.y : e.x;
-    const double *rj = Wrec + 50 * (size_t)j;
+    const double *rj = Wrec + 50 * (size_t)j + k0;
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const double diff = rj[k] - ri[k];
+    for (int k = 0; k < KH; k++) {
+      const double diff = rj[k] - wi[k];
       mn[k] = smin(mn[k], diff);
       mx[k] = smax(mx[k], diff);
     }
   }
+  double *to = tau + 10 * (size_t)i + k0;
   if (zero) {
 #pragma unroll
-    for (int k = 0; k < NF; k++) tau[10 * (size_t)i + k] = 0.0;
+    for (int k = 0; k < KH; k++) to[k] = 0.0;
     return;
   }
+  double gx[KH], gy[KH], gz[KH], gt[KH];
+#pragma unroll
+  for (int k = 0; k < KH; k++) { gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k]; }
   for (int q = q0; q < q1; q++) {
     const int f = lnk[q];
     const int2 e = s12[f];
@@ -133,24 +141,19 @@ __global__ void __launch_bounds__(128) k_limiter(int n, Params P, double t_globa
     const double *pa = pos + 3 * (size_t)e.x;
     const double dri[3] = {c.x - pa[0], c.y - pa[1], c.z - pa[2]};
     const double dsh = dri[0] * g.x + dri[1] * g.y + dri[2] * g.z;
-    double dr[3], dtt;
-    if (e.x == i) {
-      dr[0] = dri[0]; dr[1] = dri[1]; dr[2] = dri[2];
-      dtt = dtI - dth;
-    } else {
-      const double dsl = 2.0 * dsh;
-      dr[0] = dri[0] - g.x * dsl; dr[1] = dri[1] - g.y * dsl; dr[2] = dri[2] - g.z * dsl;
-      dtt = dtJ - dth;
-    }
+    const bool own = e.x == i;
+    const double dsl = own ? 0.0 : 2.0 * dsh;
+    const double dr[3] = {dri[0] - g.x * dsl, dri[1] - g.y * dsl, dri[2] - g.z * dsl};
+    const double dtt = own ? dtI - dth : dtJ - dth;
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const double dWx = ri[10 + k] * dr[0] + ri[20 + k] * dr[1] + ri[30 + k] * dr[2];
-      const double dW = dWx + ri[40 + k] * dtt;
+    for (int k = 0; k < KH; k++) {
+      const double dWx = gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2];
+      const double dW = dWx + gt[k] * dtt;
       lim[k] = smin(lim[k], limiter(dW, mn[k], mx[k]));
     }
   }
 #pragma unroll
-  for (int k = 0; k < NF; k++) tau[10 * (size_t)i + k] = lim[k];
+  for (int k = 0; k < KH; k++) to[k] = lim[k];
 }
 
 // ---- compute_update face pass (MPI/compute_update.cpp:106-269) -----------
@@ -429,7 +432,8 @@ __device__ __forceinline__ void atomic_min_pos(double *addr, double v) {
   atomicMin((unsigned long long *)addr, (unsigned long long)__double_as_longlong(v));
 }
 
-// compute_timesteps(false) first loops (MPI/compute_timestep.cpp:78-96)
+// compute_timesteps(false) first loops (MPI/compute_timestep.cpp:78-96); the
+// global minimum is reduced per warp before one atomic per warp
 __global__ void k_timestep(int n, Params P, const int *__restrict__ off, const int *__restrict__ lnk,
                            const int2 *__restrict__ s12, const unsigned char *__restrict__ act,
                            const int *__restrict__ bnd, const double *__restrict__ U,
@@ -438,14 +442,22 @@ __global__ void k_timestep(int n, Params P, const int *__restrict__ off, const i
                            const double *__restrict__ tend, double *__restrict__ dtl,
                            double *__restrict__ dmin) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const unsigned char a = act[i];
-  if (!(a & (A_ACTIVE | A_LNGB))) { dtl[i] = FVM_HUGE; return; }
-  if (!(a & A_ACTIVE)) { dtl[i] = (tend[i] - tlast[i]) * (bnd[i] != NO_BOUNDARY ? -1.0 : 1.0); return; }
-  const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
-                          cell_timestep(P, i, true, off, lnk, s12, bnd, U, volp, vel));
-  atomic_min_pos(dmin, dti);
-  dtl[i] = bnd[i] != NO_BOUNDARY ? -1.0 * dti : dti;
+  double vmin = FVM_HUGE;
+  if (i < n) {
+    const unsigned char a = act[i];
+    if (!(a & (A_ACTIVE | A_LNGB))) {
+      dtl[i] = FVM_HUGE;
+    } else if (!(a & A_ACTIVE)) {
+      dtl[i] = (tend[i] - tlast[i]) * (bnd[i] != NO_BOUNDARY ? -1.0 : 1.0);
+    } else {
+      const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
+                              cell_timestep(P, i, true, off, lnk, s12, bnd, U, volp, vel));
+      vmin = dti;
+      dtl[i] = bnd[i] != NO_BOUNDARY ? -1.0 * dti : dti;
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) vmin = smin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+  if ((threadIdx.x & 31) == 0 && vmin < FVM_HUGE) atomic_min_pos(dmin, vmin);
 }
 
 // dt >= 8 dt_min halving (MPI/compute_timestep.cpp:103-104)
@@ -586,62 +598,48 @@ __global__ void __launch_bounds__(128) k_pred_flux(int nf, Params P,
   fcode[f] = code;
 }
 
-// ---- compute_update0 cell pass + compute_reconstruction + collect ---------
-// (MPI/compute_update.cpp:812-964; MPI/compute_reconstruction.cpp:41-198;
-//  MPI/distribute_work.cpp:820-834)
-__global__ void __launch_bounds__(128) k_pred_recon(int n, Params P, double t_global, int min_rung,
+// ---- compute_update0 cell pass + collect_reconstruction -------------------
+// (MPI/compute_update.cpp:812-964; MPI/distribute_work.cpp:820-834)
+// Writes the predicted time derivative t into the cell's Wrec and the
+// cell's final rung/tend.
+__global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, double t_global, int min_rung,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double4 *__restrict__ geo, const double4 *__restrict__ cen, const double *__restrict__ cvol,
-    const unsigned char *__restrict__ act, const int *__restrict__ bnd, const double *__restrict__ pos,
-    const double *__restrict__ U, const double *__restrict__ Wst,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const double *__restrict__ pos, const double *__restrict__ U,
     const double *__restrict__ fcon, const unsigned char *__restrict__ fcode,
-    int *__restrict__ rung, double *__restrict__ tend, double *__restrict__ Wrec,
-    int *__restrict__ iscal) {
+    int *__restrict__ rung, double *__restrict__ tend, double *__restrict__ Wrec) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n || !(act[c] & A_ACTIVE)) return;
-  double *r = Wrec + 50 * (size_t)c;
-  const double *Wi = Wst + 10 * (size_t)c;
-  if (bnd[c] != NO_BOUNDARY) {
-#pragma unroll
-    for (int k = 0; k < NF; k++) r[k] = Wi[k];
-    for (int k = 10; k < 50; k++) r[k] = 0.0;
-    atomicMax(&iscal[0], rung[c]);
-    return;
-  }
-  const int q0 = off[c], q1 = off[c + 1];
+  if (c >= n || !(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
   const double V = cvol[c];
-  // predictor: gather dU/dt
   double dot[14];
 #pragma unroll
   for (int k = 0; k < 14; k++) dot[k] = 0.0;
-  for (int q = q0; q < q1; q++) {
+  for (int q = off[c]; q < off[c + 1]; q++) {
     const int f = lnk[q];
     const unsigned char code = fcode[f];
     if (code & F_OFF) continue;
     const int2 e = s12[f];
     const int fi = (code & F_SWAP) ? e.y : e.x;
     const double *o = fcon + 14 * (size_t)f;
-    if (c == fi) {
+    const double sg = c == fi ? -1.0 : 1.0;
 #pragma unroll
-      for (int k = 0; k < NF; k++) dot[k] -= o[k];
-      dot[10] = dot[10] + o[10]; dot[11] = dot[11] + o[11]; dot[12] = dot[12] + o[12];
-      dot[13] += o[13];
-    } else {
-#pragma unroll
-      for (int k = 0; k < NF; k++) dot[k] += o[k];
-      dot[10] = dot[10] - o[10]; dot[11] = dot[11] - o[11]; dot[12] = dot[12] - o[12];
-      dot[13] -= o[13];
-    }
+    for (int k = 0; k < NF; k++) dot[k] = sg < 0.0 ? dot[k] - o[k] : dot[k] + o[k];
+    dot[10] = sg < 0.0 ? dot[10] + o[10] : dot[10] - o[10];
+    dot[11] = sg < 0.0 ? dot[11] + o[11] : dot[11] - o[11];
+    dot[12] = sg < 0.0 ? dot[12] + o[12] : dot[12] - o[12];
+    dot[13] = sg < 0.0 ? dot[13] + o[13] : dot[13] - o[13];
   }
   const double *U0 = U + 10 * (size_t)c;
-  double W0[NF];
-  to_primitive(U0, V, W0);
+  double u0[NF], W0[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) u0[k] = U0[k];
+  to_primitive(u0, V, W0);
   int rg = rung[c];
-  while (rg < RUNGMAX - 1 && U0[MASS] + dot[MASS] * get_dt(P, rg) <= 0.0 * U0[MASS]) rg++;
+  while (rg < RUNGMAX - 1 && u0[MASS] + dot[MASS] * get_dt(P, rg) <= 0.0 * u0[MASS]) rg++;
   const double dt = get_dt(P, rg);
   double Uc[NF];
 #pragma unroll
-  for (int k = 0; k < NF; k++) Uc[k] = U0[k] + dot[k] * dt;
+  for (int k = 0; k < NF; k++) Uc[k] = u0[k] + dot[k] * dt;
   {
     const double divB = dot[13];
     Uc[WBX] -= W0[VELX] * divB * dt;
@@ -664,21 +662,51 @@ __global__ void __launch_bounds__(128) k_pred_recon(int n, Params P, double t_gl
   if (W1[ETHM] <= 0.0) W1[ETHM] = W0[ETHM];
   else W1[ENTR] = entropy_from_ethm(P, W1);
   const double idt = 1.0 / dt;
-  double tt[NF];
+  double *r = Wrec + 50 * (size_t)c;
 #pragma unroll
-  for (int k = 0; k < NF; k++) tt[k] = (W1[k] - W0[k]) * idt;
+  for (int k = 0; k < NF; k++) r[40 + k] = (W1[k] - W0[k]) * idt;
+  // collect_reconstruction: rung = max(rung, get_rung(dt)), tend = t + dt(rung)
+  int rf = rung[c];
+  const int rb = get_rung(P, dt, min_rung);
+  rf = rf < rb ? rb : rf;
+  rung[c] = rf;
+  tend[c] = t_global + get_dt(P, rf);
+}
 
-  // reconstruction: Voronoi face gradient of Wst, local limiter, positivity
-  double Wx[NF], Wy[NF], Wz[NF], mn[NF], mx[NF];
+// ---- compute_reconstruction (MPI/compute_reconstruction.cpp:41-198) -------
+// Two threads per active cell, five primitives each: Voronoi face gradient of
+// the updated primitives, local limiter, density positivity rescale.
+__global__ void __launch_bounds__(128) k_recon(int n, Params P,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const double4 *__restrict__ geo, const double4 *__restrict__ cen, const double *__restrict__ cvol,
+    const unsigned char *__restrict__ act, const int *__restrict__ bnd, const double *__restrict__ pos,
+    const double *__restrict__ Wst, const int *__restrict__ rung, double *__restrict__ Wrec) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int c = (int)(t >> 1);
+  const int k0 = (int)(t & 1) * KH;
+  if (c >= n || !(act[c] & A_ACTIVE)) return;
+  double *r = Wrec + 50 * (size_t)c + k0;
+  const double *wsi = Wst + 10 * (size_t)c + k0;
+  double Wi[KH];
 #pragma unroll
-  for (int k = 0; k < NF; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = 0.0; }
+  for (int k = 0; k < KH; k++) Wi[k] = wsi[k];
+  if (bnd[c] != NO_BOUNDARY) {
+#pragma unroll
+    for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = 0.0; r[20 + k] = 0.0; r[30 + k] = 0.0; r[40 + k] = 0.0; }
+    return;
+  }
+  const int q0 = off[c], q1 = off[c + 1];
+  double Wx[KH], Wy[KH], Wz[KH], mn[KH], mx[KH];
+#pragma unroll
+  for (int k = 0; k < KH; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = 0.0; }
   const double *ip = pos + 3 * (size_t)c;
+  const double px = ip[0], py = ip[1], pz = ip[2];
   double sc[3] = {0.0, 0.0, 0.0};
   bool zero = false;
   for (int q = q0; q < q1; q++) {
     const int f = lnk[q];
     const double4 g = geo[f], ce = cen[f];
-    double d[3] = {ce.x - ip[0], ce.y - ip[1], ce.z - ip[2]};
+    double d[3] = {ce.x - px, ce.y - py, ce.z - pz};
 #pragma unroll
     for (int a = 0; a < 3; a++) {
       const double L = P.box[a];
@@ -696,11 +724,12 @@ __global__ void __launch_bounds__(128) k_pred_recon(int n, Params P, double t_gl
     const int2 e = s12[f];
     const int j = e.x == c ? e.y : e.x;
     if (bnd[j] != NO_BOUNDARY) { zero = true; break; }
-    const double *Wj = Wst + 10 * (size_t)j;
+    const double *Wj = Wst + 10 * (size_t)j + k0;
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const double sum = Wj[k] + Wi[k];
-      const double diff = Wj[k] - Wi[k];
+    for (int k = 0; k < KH; k++) {
+      const double wj = Wj[k];
+      const double sum = wj + Wi[k];
+      const double diff = wj - Wi[k];
       mn[k] = smin(mn[k], diff);
       mx[k] = smax(mx[k], diff);
       Wx[k] += (sum * drh[0] + diff * fij[0]) * idsA;
@@ -710,53 +739,46 @@ __global__ void __launch_bounds__(128) k_pred_recon(int n, Params P, double t_gl
   }
   if (zero) {
 #pragma unroll
-    for (int k = 0; k < NF; k++) { r[k] = Wi[k]; r[10 + k] = 0.0; r[20 + k] = 0.0; r[30 + k] = 0.0; r[40 + k] = 0.0; }
-  } else {
-    const double invV = 1.0 / V;
-    double lm[NF];
-#pragma unroll
-    for (int k = 0; k < NF; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; lm[k] = 1.0; }
-    for (int q = q0; q < q1; q++) {
-      const double4 ce = cen[lnk[q]];
-      double d[3] = {ce.x - ip[0], ce.y - ip[1], ce.z - ip[2]};
-#pragma unroll
-      for (int a = 0; a < 3; a++) {
-        const double L = P.box[a];
-        if (d[a] > 0.5 * L) d[a] -= L;
-        else if (d[a] < -0.5 * L) d[a] += L;
-      }
-#pragma unroll
-      for (int k = 0; k < NF; k++) {
-        const double dWx = Wx[k] * d[0] + Wy[k] * d[1] + Wz[k] * d[2];
-        lm[k] = smin(lm[k], limiter(dWx, mn[k], mx[k]));
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < NF; k++) {
-      Wx[k] *= lm[k]; Wy[k] *= lm[k]; Wz[k] *= lm[k];
-      tt[k] *= lm[k];
-    }
-    {
-      const double sum_dt = dt;
-      const double dWx = Wx[DENS] * sc[0] + Wy[DENS] * sc[1] + Wz[DENS] * sc[2];
-      const double dWp = dWx + tt[DENS] * sum_dt;
-      const double dW = smax(dWx, dWp);
-      if (dW > 0.0) {
-        const double alpha = smin(1.0, 0.9 * Wi[DENS] / dW);
-        Wx[DENS] *= alpha; Wy[DENS] *= alpha; Wz[DENS] *= alpha; tt[DENS] *= alpha;
-      }
-    }
-#pragma unroll
-    for (int k = 0; k < NF; k++) { r[k] = Wi[k]; r[10 + k] = Wx[k]; r[20 + k] = Wy[k]; r[30 + k] = Wz[k]; r[40 + k] = tt[k]; }
+    for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = 0.0; r[20 + k] = 0.0; r[30 + k] = 0.0; r[40 + k] = 0.0; }
+    return;
   }
-  // collect_reconstruction: rung = max(rung, get_rung(dt)), tend = t + dt(rung)
-  int rf = rung[c];
-  const int rb = get_rung(P, dt, min_rung);
-  rf = rf < rb ? rb : rf;
-  if (rg > rf) rf = rg;
-  rung[c] = rf;
-  tend[c] = t_global + get_dt(P, rf);
-  atomicMax(&iscal[0], rf);
+  const double invV = 1.0 / cvol[c];
+  double lm[KH];
+#pragma unroll
+  for (int k = 0; k < KH; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; lm[k] = 1.0; }
+  for (int q = q0; q < q1; q++) {
+    const double4 ce = cen[lnk[q]];
+    double d[3] = {ce.x - px, ce.y - py, ce.z - pz};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double L = P.box[a];
+      if (d[a] > 0.5 * L) d[a] -= L;
+      else if (d[a] < -0.5 * L) d[a] += L;
+    }
+#pragma unroll
+    for (int k = 0; k < KH; k++) {
+      const double dWx = Wx[k] * d[0] + Wy[k] * d[1] + Wz[k] * d[2];
+      lm[k] = smin(lm[k], limiter(dWx, mn[k], mx[k]));
+    }
+  }
+  double tt[KH];
+#pragma unroll
+  for (int k = 0; k < KH; k++) {
+    Wx[k] *= lm[k]; Wy[k] *= lm[k]; Wz[k] *= lm[k];
+    tt[k] = r[40 + k] * lm[k];
+  }
+  if (k0 == 0) {  // density positivity for the *-state (MPI/compute_reconstruction.cpp:179-197)
+    const double sum_dt = get_dt(P, rung[c]);
+    const double dWx = Wx[0] * sc[0] + Wy[0] * sc[1] + Wz[0] * sc[2];
+    const double dWp = dWx + tt[0] * sum_dt;
+    const double dW = smax(dWx, dWp);
+    if (dW > 0.0) {
+      const double alpha = smin(1.0, 0.9 * Wi[0] / dW);
+      Wx[0] *= alpha; Wy[0] *= alpha; Wz[0] *= alpha; tt[0] *= alpha;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = Wx[k]; r[20 + k] = Wy[k]; r[30 + k] = Wz[k]; r[40 + k] = tt[k]; }
 }
 
 __global__ void k_shared_sync(int n, Params P, double t_global, const unsigned char *__restrict__ act,
@@ -780,10 +802,12 @@ __global__ void k_init_dt(int n, Params P, const int *__restrict__ bnd, const do
                           const double *__restrict__ volp, const double *__restrict__ vel,
                           const double *__restrict__ pos, double *__restrict__ dmin) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
-                          cell_timestep(P, i, false, nullptr, nullptr, nullptr, bnd, U, volp, vel));
-  atomic_min_pos(dmin, dti);
+  double vmin = FVM_HUGE;
+  if (i < n)
+    vmin = smin(extra_timestep(P, i, bnd, pos, vel),
+                cell_timestep(P, i, false, nullptr, nullptr, nullptr, bnd, U, volp, vel));
+  for (int o = 16; o > 0; o >>= 1) vmin = smin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+  if ((threadIdx.x & 31) == 0) atomic_min_pos(dmin, vmin);
 }
 
 __global__ void k_init_state(int n, const double *__restrict__ W, const double *__restrict__ cvol,
@@ -835,9 +859,9 @@ inline int nblk(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 // ============================== host context ================================
 
 enum KernelId { KT_FLAGS = 0, KT_LIMITER, KT_CORR_FLUX, KT_CORR_CELL, KT_PVEL, KT_TIMESTEP, KT_RUNGS,
-                KT_WST, KT_PRED_FLUX, KT_PRED_RECON, KT_SYNC, KT_COUNT };
+                KT_WST, KT_PRED_FLUX, KT_PRED_CELL, KT_RECON, KT_SYNC, KT_COUNT };
 static const char *kKernelNames[KT_COUNT] = {"flags", "limiter", "corr_flux", "corr_cell", "pvel", "timestep",
-                                             "rungs", "wst", "pred_flux", "pred_recon", "sync"};
+                                             "rungs", "wst", "pred_flux", "pred_cell", "recon", "sync"};
 
 struct fvm_ctx {
   int device;
@@ -1174,7 +1198,7 @@ int fvm_slope_limiter(fvm_ctx *c) {
   if (!c || !c->in_step) { if (c) c->err = "fvm_slope_limiter: call fvm_begin_step first"; return FVM_EINVAL; }
   Dev &d = c->d;
   kt_begin(c, KT_LIMITER);
-  k_limiter<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, c->t_global, d.off, d.lnk, d.s12, d.geo, d.cen,
+  k_limiter<<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, c->t_global, d.off, d.lnk, d.s12, d.geo, d.cen,
                                                  d.act, d.bnd, d.pos, d.tlast, d.Wrec, d.tau);
   LAUNCH_CHECK();
   kt_end(c, KT_LIMITER);
@@ -1262,13 +1286,17 @@ int fvm_compute_update0(fvm_ctx *c) {
 int fvm_compute_reconstruction(fvm_ctx *c) {
   if (!c || !c->in_step) { if (c) c->err = "fvm_compute_reconstruction: call fvm_begin_step first"; return FVM_EINVAL; }
   Dev &d = c->d;
-  CK(cudaMemsetAsync(d.iscal, 0, sizeof(int), c->st));
-  kt_begin(c, KT_PRED_RECON);
-  k_pred_recon<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, c->t_global, c->min_rung, d.off, d.lnk, d.s12,
-                                                   d.geo, d.cen, d.cvol, d.act, d.bnd, d.pos, d.U, d.Wst,
-                                                   d.fcon2, d.fcode2, d.rung, d.tend, d.Wrec, d.iscal);
+  kt_begin(c, KT_PRED_CELL);
+  k_pred_cell<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, c->t_global, c->min_rung, d.off, d.lnk, d.s12,
+                                                  d.cvol, d.act, d.bnd, d.pos, d.U, d.fcon2, d.fcode2, d.rung,
+                                                  d.tend, d.Wrec);
   LAUNCH_CHECK();
-  kt_end(c, KT_PRED_RECON);
+  kt_end(c, KT_PRED_CELL);
+  kt_begin(c, KT_RECON);
+  k_recon<<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.s12, d.geo, d.cen, d.cvol, d.act,
+                                                    d.bnd, d.pos, d.Wst, d.rung, d.Wrec);
+  LAUNCH_CHECK();
+  kt_end(c, KT_RECON);
   return 0;
 }
 
@@ -1277,6 +1305,9 @@ int fvm_end_step(fvm_ctx *c, int shared) {
   Dev &d = c->d;
   if (shared) {
     kt_begin(c, KT_SYNC);
+  CK(cudaMemsetAsync(d.iscal, 0, sizeof(int), c->st));
+  k_maxrung<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, d.rung, d.iscal);
+  LAUNCH_CHECK();
   k_shared_sync<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, c->P, c->t_global, d.act, d.iscal, d.rung, d.tend);
     LAUNCH_CHECK();
   kt_end(c, KT_SYNC);

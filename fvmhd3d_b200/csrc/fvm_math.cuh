@@ -279,11 +279,16 @@ __device__ __forceinline__ T Phi(T x) {
   const T e = T(0.2 * 1.0e-16);
   return (x * x + T(2) * x + e) / (x * x + x + T(2) + e);
 }
+// Branch-free form: both candidate ratios share one division, and the
+// threshold test selects the result, so a warp never splits on the sign of
+// dWi.  The selected value is the one the reference's branches compute.
 template <typename T>
 __device__ __forceinline__ T limiter(T dWi, T dWj_min, T dWj_max) {
-  if (fabs(dWi) <= T(1.0e-16) * smax(fabs(dWj_max), fabs(dWj_min))) return T(1);
-  else if (dWi < T(0)) return Phi(dWj_min / dWi);
-  else return Phi(dWj_max / dWi);
+  const bool flat = fabs(dWi) <= T(1.0e-16) * smax(fabs(dWj_max), fabs(dWj_min));
+  const T num = dWi < T(0) ? dWj_min : dWj_max;
+  const T den = flat ? T(1) : dWi;
+  const T phi = Phi(num / den);
+  return flat ? T(1) : phi;
 }
 
 }  // namespace fvm

@@ -12,13 +12,17 @@ ORACLE_SO = os.path.join(ROOT, "oracle", "_ref", "liboracle.so")
 RTOL_FP64 = 1e-12
 
 
-def maxrel(a, b, axis=0):
-    """Per-column max-norm relative error of a against b."""
+def maxrel(a, b, axis=0, scale=None):
+    """Per-column max-norm relative error of a against b.  The denominator is
+    max |b| over cells per column, or max |scale| when a subset of cells is
+    compared (so that a column that is near zero on the subset is measured
+    against its magnitude over the whole mesh)."""
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     if a.ndim == 1:
         a, b = a[:, None], b[:, None]
-    den = np.abs(b).max(axis=axis)
+    ref = b if scale is None else np.asarray(scale, dtype=np.float64).reshape(-1, a.shape[1])
+    den = np.abs(ref).max(axis=axis)
     den = np.where(den > 0, den, 1.0)
     return np.abs(a - b).max(axis=axis) / den
 

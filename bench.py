@@ -51,8 +51,10 @@ def kernel_bytes(name, N, F, prec_bytes=8):
         # reads face contributions (each face by its two cells), U, dU, Wrec w,t, tau; writes U, dU
         "corr_cell": F * (14 * 8 + 1) + N * (80 + 112 + 20 * w + 10 * w) + N * (80 + 112),
         "pred_flux": N * (10 * w + 24 + 24) + F * 56 + F * (14 * 8 + 1),
-        # reads face contributions, U, Wst (neighbours), face records; writes Wrec
-        "pred_recon": F * (14 * 8 + 1) + F * 56 + N * (80 + 10 * w) + N * 50 * w,
+        # reads face contributions and U; writes Wrec t, rung, tend
+        "pred_cell": F * (14 * 8 + 1) + N * 80 + N * (10 * w + 12),
+        # reads Wst (neighbours), face records, Wrec t; writes Wrec
+        "recon": F * 56 + N * (10 * w + 24 + 10 * w) + N * 50 * w,
         "timestep": N * (80 + 24 + 8 + 8) + F * 8 + N * 8,
         "pvel": N * (80 + 24 + 24 + 8) + N * 24,
         "wst": N * 80 + N * 10 * w,
@@ -280,7 +282,7 @@ def run_gpu(args):
     if dom:
         tot, calls = ktimes[dom]
         per_launch_s = tot / max(calls, 1) / 1e3
-        alg = kernel_bytes(dom, N, Fc, pb)
+        alg = kernel_bytes(dom, N, Fc, pb) or 0
         ach = alg / per_launch_s / 1e9
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(ach / peak, 4), "peak_source": peak_kind,

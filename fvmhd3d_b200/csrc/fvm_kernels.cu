@@ -103,9 +103,9 @@ __global__ void __launch_bounds__(128) k_limiter(int n, Params P, double t_globa
   if (i >= n) return;
   if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
   const double *ri = Wrec + 50 * (size_t)i + k0;
-  double mn[KH], mx[KH], lim[KH], wi[KH];
+  double mn[KH], mx[KH], ln[KH], lq[KH], wi[KH];
 #pragma unroll
-  for (int k = 0; k < KH; k++) { mn[k] = 0.0; mx[k] = 0.0; lim[k] = 1.0; wi[k] = ri[k]; }
+  for (int k = 0; k < KH; k++) { mn[k] = 0.0; mx[k] = 0.0; ln[k] = 1.0; lq[k] = 1.0; wi[k] = ri[k]; }
   const int q0 = off[i], q1 = off[i + 1];
   bool zero = false;
   for (int q = q0; q < q1; q++) {
@@ -149,11 +149,11 @@ __global__ void __launch_bounds__(128) k_limiter(int n, Params P, double t_globa
     for (int k = 0; k < KH; k++) {
       const double dWx = gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2];
       const double dW = dWx + gt[k] * dtt;
-      lim[k] = smin(lim[k], limiter(dW, mn[k], mx[k]));
+      limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
     }
   }
 #pragma unroll
-  for (int k = 0; k < KH; k++) to[k] = lim[k];
+  for (int k = 0; k < KH; k++) to[k] = ln[k] / lq[k];
 }
 
 // ---- compute_update face pass (MPI/compute_update.cpp:106-269) -----------
@@ -743,9 +743,9 @@ __global__ void __launch_bounds__(128) k_recon(int n, Params P,
     return;
   }
   const double invV = 1.0 / cvol[c];
-  double lm[KH];
+  double ln[KH], lq[KH];
 #pragma unroll
-  for (int k = 0; k < KH; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; lm[k] = 1.0; }
+  for (int k = 0; k < KH; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; ln[k] = 1.0; lq[k] = 1.0; }
   for (int q = q0; q < q1; q++) {
     const double4 ce = cen[lnk[q]];
     double d[3] = {ce.x - px, ce.y - py, ce.z - pz};
@@ -758,14 +758,15 @@ __global__ void __launch_bounds__(128) k_recon(int n, Params P,
 #pragma unroll
     for (int k = 0; k < KH; k++) {
       const double dWx = Wx[k] * d[0] + Wy[k] * d[1] + Wz[k] * d[2];
-      lm[k] = smin(lm[k], limiter(dWx, mn[k], mx[k]));
+      limiter_min(ln[k], lq[k], dWx, mn[k], mx[k]);
     }
   }
   double tt[KH];
 #pragma unroll
   for (int k = 0; k < KH; k++) {
-    Wx[k] *= lm[k]; Wy[k] *= lm[k]; Wz[k] *= lm[k];
-    tt[k] = r[40 + k] * lm[k];
+    const double lm = ln[k] / lq[k];
+    Wx[k] *= lm; Wy[k] *= lm; Wz[k] *= lm;
+    tt[k] = r[40 + k] * lm;
   }
   if (k0 == 0) {  // density positivity for the *-state (MPI/compute_reconstruction.cpp:179-197)
     const double sum_dt = get_dt(P, rung[c]);

@@ -291,4 +291,21 @@ __device__ __forceinline__ T limiter(T dWi, T dWj_min, T dWj_max) {
   return flat ? T(1) : phi;
 }
 
+// Running minimum of limiter values, kept as a fraction n/q (q > 0) so that
+// each face costs one division (x = dWj/dWi) instead of two: Phi(x) is
+// n(x)/q(x) with q >= 2, and n1/q1 < n2/q2 <=> n1*q2 < n2*q1.  The caller
+// starts from n = q = 1 (the reference's initial 1.0) and finishes with one
+// division n/q per primitive.
+template <typename T>
+__device__ __forceinline__ void limiter_min(T &n, T &q, T dWi, T dWj_min, T dWj_max) {
+  const bool flat = fabs(dWi) <= T(1.0e-16) * smax(fabs(dWj_max), fabs(dWj_min));
+  const T num = dWi < T(0) ? dWj_min : dWj_max;
+  const T x = num / (flat ? T(1) : dWi);
+  const T e = T(0.2 * 1.0e-16);
+  T pn = x * x + T(2) * x + e;
+  T pq = x * x + x + T(2) + e;
+  if (flat) { pn = T(1); pq = T(1); }
+  if (pn * q < n * pq) { n = pn; q = pq; }
+}
+
 }  // namespace fvm

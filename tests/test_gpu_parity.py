@@ -27,7 +27,7 @@ def oracle_system(m, W):
     return o
 
 
-def wrec_err(a, b, h, dt):
+def wrec_err(a, b, h, dt, scale=None):
     """Error of reconstruction records (ncell x 50) in units of the face state
     they produce: the w block relative to max |w|, the gradient blocks as
     |d grad| * h and the time-derivative block as |d t| * dt, both relative to
@@ -36,7 +36,8 @@ def wrec_err(a, b, h, dt):
     by cancellation; what enters the flux is w + grad.dr + t.dt.)"""
     a = a.reshape(-1, 5, 10)
     b = b.reshape(-1, 5, 10)
-    wmax = np.abs(b[:, 0, :]).max(axis=0)
+    ref = b if scale is None else np.asarray(scale).reshape(-1, 5, 10)
+    wmax = np.abs(ref[:, 0, :]).max(axis=0)
     wmax = np.where(wmax > 0, wmax, 1.0)
     d = np.abs(a - b).max(axis=0)
     scale = np.array([1.0, h, h, h, dt])[:, None]
@@ -52,7 +53,7 @@ def assert_state_close(a, b, rtol=RTOL_FP64, mask=None, h=None, dt=None):
     h = (1.0 / n) ** (1.0 / 3.0) if h is None else h
     if dt is None:
         dt = 2.0 ** -float(np.max(b["rung"])) / 64.0
-    e = wrec_err(a["wrec"][sel], b["wrec"][sel], h, dt)
+    e = wrec_err(a["wrec"][sel], b["wrec"][sel], h, dt, scale=b["wrec"])
     assert e <= rtol, ("wrec", e)
     for k in ("rung", "tend", "tlast"):
         assert np.array_equal(a[k][sel], b[k][sel]), k
@@ -99,7 +100,7 @@ def test_stage_by_stage_vs_oracle(shared):
         imp |= ngb
         h = (1.0 / m.ncell) ** (1.0 / 3.0)
         dt = 2.0 ** -float(o.get_state()["rung"].max()) / 64.0
-        assert wrec_err(lw[imp], snap["wrec_after_limiter"][imp], h, dt) <= RTOL_FP64
+        assert wrec_err(lw[imp], snap["wrec_after_limiter"][imp], h, dt, scale=o.get_state()["wrec"]) <= RTOL_FP64
         s.compute_update()
         s.compute_pvel()
         s.compute_timesteps(shared)
@@ -112,7 +113,7 @@ def test_stage_by_stage_vs_oracle(shared):
         ref = o.get_state()
         assert maxrel(a["U"][act_o], snap["U_after_update"][act_o], scale=ref["U"]).max() <= RTOL_FP64
         assert maxrel(a["vel"][act_o], snap["vel_after_pvel"][act_o], scale=ref["vel"]).max() <= RTOL_FP64
-        assert wrec_err(a["wrec"][act_o], snap["wrec_after_recon"][act_o], h, dt) <= RTOL_FP64
+        assert wrec_err(a["wrec"][act_o], snap["wrec_after_recon"][act_o], h, dt, scale=ref["wrec"]) <= RTOL_FP64
         assert_state_close(a, o.get_state())
 
 

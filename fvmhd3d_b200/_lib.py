@@ -46,6 +46,7 @@ SIGNATURES = {
     "fvm_compute_reconstruction": (c_int, [c_void_p]),
     "fvm_end_step": (c_int, [c_void_p, c_int]),
     "fvm_step": (c_int, [c_void_p, c_int]),
+    "fvm_run": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "fvm_time": (c_double, [c_void_p]),
     "fvm_tsys_ticks": (c_ull, [c_void_p]),
     "fvm_get_active_faces": (c_int, [c_void_p, c_void_p, c_void_p]),
@@ -56,6 +57,7 @@ SIGNATURES = {
     "fvm_compute_flux": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_last_step_ms": (c_float, [c_void_p]),
     "fvm_stream": (c_void_p, [c_void_p]),
+    "fvm_last_step_counts": (c_int, [c_void_p, c_void_p, c_void_p]),
     "fvm_launch_count": (c_ll, [c_void_p]),
     "fvm_set_profiling": (c_int, [c_void_p, c_int]),
     "fvm_kernel_times": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(c_double),

@@ -21,30 +21,73 @@
 #include <cstdlib>
 #include <vector>
 #include <string>
+#include <algorithm>
 
 using namespace fvm;
+
+// Minimum resident 128-thread blocks per SM for the face-flux kernels (caps
+// their registers: 3 -> 168 for FP64, 4 -> 128 for FP32, no spills) and for
+// the two-threads-per-cell kernels.
+#ifndef FVM_FLUX_MINB_D
+#define FVM_FLUX_MINB_D 3
+#endif
+#ifndef FVM_FLUX_MINB_F
+#define FVM_FLUX_MINB_F 4
+#endif
+#ifndef FVM_CELL_MINB
+#define FVM_CELL_MINB 1
+#endif
+#define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
+// cell-kernel mappings: grouped (16 lanes per cell) or two threads per cell
+#ifndef FVM_CELLMAP_GROUPED
+#define FVM_CELLMAP_GROUPED 0
+#endif
+#ifndef FVM_GATHER_GROUPED
+#define FVM_GATHER_GROUPED 0
+#endif
+// Thread-to-cell indirection: inside each window of CPW consecutive cells the
+// threads visit cells in order of face count, so the lanes of a warp run face
+// loops of similar length (less divergence) while memory locality stays
+// within the window.  Pure relabelling of which thread does which cell.
+#ifndef FVM_CELL_PERM
+#define FVM_CELL_PERM 0
+#endif
+constexpr int CPW = 64;
 
 namespace {
 
 enum : unsigned char { A_ACTIVE = 1, A_LNGB = 2, A_HASNGB = 4 };
 enum : unsigned char { F_SWAP = 1, F_SKIPJ = 2, F_OFF = 4 };
 
+// Scheduler state kept on the device so that a whole step is a fixed
+// sequence of launches (MPI/Scheduler.h:4-30, 108-154).
+struct Sched {
+  unsigned long long tsysU, flags;
+  double t_global, dtmin;
+  int min_rung, max_rung;
+  int iscal[8];  // [0] rung maximum, [1] active cells, [2] error flags, [3] active faces,
+                 // [4] dirty sites of adjust_timesteps, [5] active non-boundary sites
+  unsigned long long nactive_total, nfaces_total, steps;
+};
+
 struct Dev {
   // mesh
   int2 *s12;
-  double4 *geo, *cen;
+  double4 *geo, *cen, *dr1, *dr2;
   double *cvol, *ccen;
   int *off, *lnk;
+  int *perm;  // thread slot -> cell (face-count order inside windows of CPW cells)
+  int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
   // state
   double *pos, *vel, *tlast, *tend, *volp;
   int *rung, *bnd;
-  double *U, *dU, *Wrec;
+  double *U, *dU;
+  void *Wrec;  // bulk type (double or float), ncell x 50
   // per-step work
-  unsigned char *act0, *act, *hash, *fcode, *fcode2;
-  double *tau, *fcon, *fcon2, *Wst, *dtl, *stepdU;
-  // scalars: dmin (double), ints [maxrung, nactive], counters
-  double *dscal;
-  int *iscal;
+  unsigned char *act0, *act, *hash, *fcode, *fcode2, *fflag;
+  void *tau, *fcon, *fcon2, *Wst, *fst;  // bulk type
+  double *dtl, *stepdU;
+  Sched *S;
   unsigned long long *counters;
 };
 
@@ -55,33 +98,96 @@ __device__ __forceinline__ bool face_active(const unsigned char *act, const int 
 __device__ __forceinline__ void ld3(const double *p, double *o) { o[0] = p[0]; o[1] = p[1]; o[2] = p[2]; }
 
 // ---- begin_step: active flags (Scheduler::pull_active_list) ---------------
-__global__ void k_active(int n, const int *__restrict__ rung, unsigned long long flags,
-                         unsigned char *__restrict__ act0) {
+__global__ void k_active(int n, const int *__restrict__ rung, const Sched *__restrict__ S,
+                         unsigned char *__restrict__ act, int *__restrict__ nactive) {
+  const unsigned long long flags = S->flags;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const int r = rung[i];
-  act0[i] = (r >= 0 && r < RUNGMAX && ((flags >> (RUNGMAX - 1 - r)) & 1ULL)) ? A_ACTIVE : 0;
+  bool a = false;
+  if (i < n) {
+    const int r = rung[i];
+    a = r >= 0 && r < RUNGMAX && ((flags >> (RUNGMAX - 1 - r)) & 1ULL);
+    act[i] = a ? A_ACTIVE : 0;
+  }
+  __shared__ int bsum;
+  if (threadIdx.x == 0) bsum = 0;
+  __syncthreads();
+  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, a));
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bsum, (int)cnt);
+  __syncthreads();
+  if (threadIdx.x == 0 && bsum) atomicAdd(nactive, bsum);
 }
 
-// site flags of build_mesh_active (MPI/build_mesh_active.cpp:524-528)
-__global__ void k_ngbflags(int n, const int *__restrict__ off, const int *__restrict__ lnk,
-                           const int2 *__restrict__ s12, const unsigned char *__restrict__ act0,
-                           unsigned char *__restrict__ act, int *__restrict__ iscal) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const bool ai = act0[i] & A_ACTIVE;
-  bool other = false;
-  for (int q = off[i]; q < off[i + 1]; q++) {
-    const int2 e = s12[lnk[q]];
-    const int j = e.x == i ? e.y : e.x;
-    const bool aj = act0[j] & A_ACTIVE;
-    if (ai != aj) { other = true; break; }
+// per-step face flags: active face (a face of an active non-boundary cell,
+// MPI/iterate.cpp:58-93) and the boundary flags of its two cells
+enum : unsigned char { FF_ACTIVE = 1, FF_BND1 = 2, FF_BND2 = 4 };
+// Per face: active flag and boundary flags, and the site flags of
+// build_mesh_active (MPI/build_mesh_active.cpp:524-528): a face between an
+// active and an inactive cell marks the inactive one a local neighbour and the
+// active one as having one.  A cell only ever receives one kind of mark, so
+// concurrent byte stores to it write the same value; the active bit they
+// test never changes during this kernel.
+__global__ void k_faceflags(int nf, const int2 *__restrict__ s12, unsigned char *__restrict__ act,
+                            const int *__restrict__ bnd, unsigned char *__restrict__ fflag,
+                            int *__restrict__ nface_active) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  bool a = false;
+  if (f < nf) {
+    const int2 e = s12[f];
+    const bool a1 = act[e.x] & A_ACTIVE, a2 = act[e.y] & A_ACTIVE;
+    const bool b1 = bnd[e.x] != NO_BOUNDARY, b2 = bnd[e.y] != NO_BOUNDARY;
+    a = (a1 && !b1) || (a2 && !b2);
+    unsigned char v = a ? FF_ACTIVE : 0;
+    if (b1) v |= FF_BND1;
+    if (b2) v |= FF_BND2;
+    fflag[f] = v;
+    if (a1 != a2) {
+      act[a1 ? e.y : e.x] = A_LNGB;
+      act[a1 ? e.x : e.y] = A_ACTIVE | A_HASNGB;
+    }
   }
-  unsigned char f = ai ? A_ACTIVE : 0;
-  if (ai && other) f |= A_HASNGB;
-  if (!ai && other) f |= A_LNGB;
-  act[i] = f;
-  if (ai) atomicAdd(&iscal[1], 1);
+  __shared__ int bsum;
+  if (threadIdx.x == 0) bsum = 0;
+  __syncthreads();
+  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, a));
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bsum, (int)cnt);
+  __syncthreads();
+  if (threadIdx.x == 0 && bsum) atomicAdd(nface_active, bsum);
+}
+
+// Face offsets used by every face loop, computed once per generator layout:
+//   dr1 = centroid - x_s1 (the reference's dri, MPI/compute_update.cpp:136)
+//         with w = dri . n (dsh, :164)
+//   dr2 = wrap(centroid - x_s2) (MPI/compute_reconstruction.cpp:74-83 seen
+//         from s2)
+__global__ void k_face_geom(int nf, Params P, const int2 *__restrict__ s12, const double4 *__restrict__ geo,
+                            const double4 *__restrict__ cen, const double *__restrict__ pos,
+                            double4 *__restrict__ dr1, double4 *__restrict__ dr2) {
+  const int f = blockIdx.x * blockDim.x + threadIdx.x;
+  if (f >= nf) return;
+  const int2 e = s12[f];
+  const double4 g = geo[f], c = cen[f];
+  const double *pa = pos + 3 * (size_t)e.x, *pb = pos + 3 * (size_t)e.y;
+  const double d1[3] = {c.x - pa[0], c.y - pa[1], c.z - pa[2]};
+  double d2[3] = {c.x - pb[0], c.y - pb[1], c.z - pb[2]};
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double L = P.box[a];
+    if (d2[a] > 0.5 * L) d2[a] -= L;
+    else if (d2[a] < -0.5 * L) d2[a] += L;
+  }
+  dr1[f] = make_double4(d1[0], d1[1], d1[2], d1[0] * g.x + d1[1] * g.y + d1[2] * g.z);
+  dr2[f] = make_double4(d2[0], d2[1], d2[2], 0.0);
+}
+
+// min-image of the s1 offset for the reconstruction (a no-op for meshes that
+// keep the centroid in the frame of s1, as the reference asserts)
+__device__ __forceinline__ void wrap3(const Params &P, double *d) {
+#pragma unroll
+  for (int a = 0; a < 3; a++) {
+    const double L = P.box[a];
+    if (d[a] > 0.5 * L) d[a] -= L;
+    else if (d[a] < -0.5 * L) d[a] += L;
+  }
 }
 
 // ---- slope_limiter (MPI/compute_reconstruction.cpp:201-602) --------------
@@ -89,178 +195,520 @@ __global__ void k_ngbflags(int n, const int *__restrict__ off, const int *__rest
 // pass 1 (min/max of neighbour differences) and face pass 2 (limiter of the
 // space+time extrapolated difference) over the cell's active faces.  The
 // result tau is applied on the fly by the corrector, so Wrec is not modified.
+// R is the bulk type (double: plain path; float: FP32 path); face geometry
+// stays double and is rounded to R only where it multiplies bulk data.
 constexpr int KH = 5;  // primitives per thread in the two-threads-per-cell kernels
 
-__global__ void __launch_bounds__(128) k_limiter(int n, Params P, double t_global,
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_CELL_MINB) k_limiter(int n, Params P, const Sched *__restrict__ S,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double4 *__restrict__ geo, const double4 *__restrict__ cen,
-    const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const double *__restrict__ pos, const double *__restrict__ tlast,
-    const double *__restrict__ Wrec, double *__restrict__ tau) {
+    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
+    const unsigned char *__restrict__ act, const double *__restrict__ tlast,
+    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm) {
+  const double t_global = S->t_global;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int i = (int)(t >> 1);
+  if ((t >> 1) >= n) return;
+  const int i = perm[t >> 1];
   const int k0 = (int)(t & 1) * KH;
-  if (i >= n) return;
   if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
-  const double *ri = Wrec + 50 * (size_t)i + k0;
-  double mn[KH], mx[KH], ln[KH], lq[KH], wi[KH];
+  const R *ri = Wrec + 50 * (size_t)i + k0;
+  R mn[KH], mx[KH], ln[KH], lq[KH], wi[KH];
 #pragma unroll
-  for (int k = 0; k < KH; k++) { mn[k] = 0.0; mx[k] = 0.0; ln[k] = 1.0; lq[k] = 1.0; wi[k] = ri[k]; }
+  for (int k = 0; k < KH; k++) { mn[k] = R(0); mx[k] = R(0); ln[k] = R(1); lq[k] = R(1); wi[k] = ri[k]; }
   const int q0 = off[i], q1 = off[i + 1];
   bool zero = false;
+  // pass 1: min/max of neighbour differences over active interior faces
   for (int q = q0; q < q1; q++) {
     const int f = lnk[q];
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE)) continue;
+    if (ff & (FF_BND1 | FF_BND2)) { zero = true; continue; }
     const int2 e = s12[f];
-    if (!face_active(act, bnd, e.x, e.y)) continue;
-    if (bnd[e.x] != NO_BOUNDARY || bnd[e.y] != NO_BOUNDARY) { zero = true; continue; }
     const int j = e.x == i ? e.y : e.x;
-    const double *rj = Wrec + 50 * (size_t)j + k0;
+    const R *rj = Wrec + 50 * (size_t)j + k0;
 #pragma unroll
     for (int k = 0; k < KH; k++) {
-      const double diff = rj[k] - wi[k];
+      const R diff = rj[k] - wi[k];
       mn[k] = smin(mn[k], diff);
       mx[k] = smax(mx[k], diff);
     }
   }
-  double *to = tau + 10 * (size_t)i + k0;
+  R *to = tau + 10 * (size_t)i + k0;
+  R gx[KH], gy[KH], gz[KH], gt[KH];
   if (zero) {
+    // a boundary face zeroes the limiter: the face states are w itself
 #pragma unroll
-    for (int k = 0; k < KH; k++) to[k] = 0.0;
-    return;
-  }
-  double gx[KH], gy[KH], gz[KH], gt[KH];
+    for (int k = 0; k < KH; k++) { to[k] = R(0); gx[k] = gy[k] = gz[k] = gt[k] = R(0); }
+  } else {
 #pragma unroll
-  for (int k = 0; k < KH; k++) { gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k]; }
-  for (int q = q0; q < q1; q++) {
-    const int f = lnk[q];
-    const int2 e = s12[f];
-    if (!face_active(act, bnd, e.x, e.y)) continue;
-    const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
-    const double dth = 0.5 * smin(dtI, dtJ);
-    const double4 g = geo[f], c = cen[f];
-    const double *pa = pos + 3 * (size_t)e.x;
-    const double dri[3] = {c.x - pa[0], c.y - pa[1], c.z - pa[2]};
-    const double dsh = dri[0] * g.x + dri[1] * g.y + dri[2] * g.z;
-    const bool own = e.x == i;
-    const double dsl = own ? 0.0 : 2.0 * dsh;
-    const double dr[3] = {dri[0] - g.x * dsl, dri[1] - g.y * dsl, dri[2] - g.z * dsl};
-    const double dtt = own ? dtI - dth : dtJ - dth;
+    for (int k = 0; k < KH; k++) { gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k]; }
+    // pass 2: limiter of the extrapolated difference at each active face
+    for (int q = q0; q < q1; q++) {
+      const int f = lnk[q];
+      if (!(fflag[f] & FF_ACTIVE)) continue;
+      const int2 e = s12[f];
+      const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
+      const double dth = 0.5 * smin(dtI, dtJ);
+      const double4 g = geo[f], d = dr1[f];
+      const bool own = e.x == i;
+      const double dsl = own ? 0.0 : 2.0 * d.w;
+      const R dr[3] = {R(d.x - g.x * dsl), R(d.y - g.y * dsl), R(d.z - g.z * dsl)};
+      const R dtt = R(own ? dtI - dth : dtJ - dth);
+#pragma unroll
+      for (int k = 0; k < KH; k++) {
+        const R dWx = gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2];
+        const R dW = dWx + gt[k] * dtt;
+        limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
+      }
+    }
 #pragma unroll
     for (int k = 0; k < KH; k++) {
-      const double dWx = gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2];
-      const double dW = dWx + gt[k] * dtt;
-      limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
+      const R tk = ln[k] / lq[k];
+      to[k] = tk;
+      gx[k] *= tk; gy[k] *= tk; gz[k] *= tk; gt[k] *= tk;
+    }
+  }
+  // pass 3: the half-step extrapolated state of this cell at each active
+  // interior face (MPI/compute_update.cpp:157-212), stored per face side
+  for (int q = q0; q < q1; q++) {
+    const int f = lnk[q];
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE) || (ff & (FF_BND1 | FF_BND2))) continue;
+    const int2 e = s12[f];
+    const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
+    const double dt = smin(dtI, dtJ);
+    const double4 g = geo[f], d = dr1[f];
+    const bool own = e.x == i;
+    const double dsl = own ? 0.0 : 2.0 * d.w;
+    const R dr[3] = {R(d.x - g.x * dsl), R(d.y - g.y * dsl), R(d.z - g.z * dsl)};
+    const R dtt = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
+    R *o = fst + 20 * (size_t)f + (own ? 0 : 10) + k0;
+#pragma unroll
+    for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2]) + gt[k] * dtt);
+  }
+}
+
+// ---- grouped cell kernels -------------------------------------------------
+// Each cell is handled by 16 lanes: two subgroups of GL = 8 lanes, one per
+// half of the ten primitives (KV = 5 each).  Lane l of a subgroup takes the
+// cell's faces l, l+8, ..., so a cell's faces are read by 8 lanes at once; the
+// cell record is staged in shared memory and the per-face partials are
+// combined with 3-step shuffle reductions inside the subgroup.  Min/max
+// reductions are exact; sums are reassociated (a few ulps).
+constexpr int GL = 8;                 // lanes per subgroup (faces in flight per cell)
+constexpr int KV = 5;                 // primitives per subgroup
+constexpr int GTB = 256;              // threads per block
+constexpr int GCB = GTB / (2 * GL);   // cells per block
+
+template <typename T>
+__device__ __forceinline__ T gmin(T v) {
+#pragma unroll
+  for (int o = GL / 2; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T gmax(T v) {
+#pragma unroll
+  for (int o = GL / 2; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+template <typename T>
+__device__ __forceinline__ T gsum(T v) {
+#pragma unroll
+  for (int o = GL / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+// minimum of the fractions n/q (q > 0) held by the lanes of a subgroup
+template <typename T>
+__device__ __forceinline__ void gmin_frac(T &n, T &q) {
+#pragma unroll
+  for (int o = GL / 2; o > 0; o >>= 1) {
+    const T n2 = __shfl_xor_sync(0xffffffffu, n, o), q2 = __shfl_xor_sync(0xffffffffu, q, o);
+    if (n2 * q < n * q2) { n = n2; q = q2; }
+  }
+}
+__device__ __forceinline__ unsigned group_mask() {  // the 16 lanes of this cell
+  return 0xffffu << ((threadIdx.x & 31) & 16);
+}
+__device__ __forceinline__ bool gany(bool v) {      // any lane of this cell
+  return (__ballot_sync(0xffffffffu, v) & group_mask()) != 0;
+}
+
+// slope_limiter (MPI/compute_reconstruction.cpp:201-602): pass 1 min/max of
+// neighbour differences, pass 2 limiter minimum of the extrapolated
+// difference, pass 3 the half-step extrapolated face states.
+template <typename R>
+__global__ void __launch_bounds__(GTB) k_limiter_g(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
+    const unsigned char *__restrict__ act, const double *__restrict__ tlast,
+    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst) {
+  __shared__ R sh[GCB][50];
+  const double t_global = S->t_global;
+  const int g = threadIdx.x / (2 * GL), k0 = ((threadIdx.x / GL) & 1) * KV, l = threadIdx.x % GL;
+  const int c = blockIdx.x * GCB + g;
+  const bool valid = c < n && (act[c] & (A_ACTIVE | A_LNGB));
+  R *rec = sh[g];
+  if (valid)
+    for (int k = threadIdx.x % (2 * GL); k < 50; k += 2 * GL) rec[k] = Wrec[50 * (size_t)c + k];
+  __syncthreads();
+  const int q0 = valid ? off[c] : 0, q1 = valid ? off[c + 1] : 0;
+  R mn[KV], mx[KV];
+#pragma unroll
+  for (int k = 0; k < KV; k++) { mn[k] = R(0); mx[k] = R(0); }
+  bool zero = false;
+  for (int q = q0 + l; q < q1; q += GL) {
+    const int f = lnk[q];
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE)) continue;
+    if (ff & (FF_BND1 | FF_BND2)) { zero = true; continue; }
+    const int2 e = s12[f];
+    const int j = e.x == c ? e.y : e.x;
+    const R *rj = Wrec + 50 * (size_t)j + k0;
+#pragma unroll
+    for (int k = 0; k < KV; k++) {
+      const R diff = rj[k] - rec[k0 + k];
+      mn[k] = smin(mn[k], diff);
+      mx[k] = smax(mx[k], diff);
+    }
+  }
+  zero = gany(zero);
+#pragma unroll
+  for (int k = 0; k < KV; k++) { mn[k] = gmin(mn[k]); mx[k] = gmax(mx[k]); }
+  R ln[KV], lq[KV];
+#pragma unroll
+  for (int k = 0; k < KV; k++) { ln[k] = R(1); lq[k] = R(1); }
+  if (!zero) {
+    for (int q = q0 + l; q < q1; q += GL) {
+      const int f = lnk[q];
+      if (!(fflag[f] & FF_ACTIVE)) continue;
+      const int2 e = s12[f];
+      const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
+      const double dth = 0.5 * smin(dtI, dtJ);
+      const double4 gg = geo[f], d = dr1[f];
+      const bool own = e.x == c;
+      const double dsl = own ? 0.0 : 2.0 * d.w;
+      const R dr[3] = {R(d.x - gg.x * dsl), R(d.y - gg.y * dsl), R(d.z - gg.z * dsl)};
+      const R dtt = R(own ? dtI - dth : dtJ - dth);
+#pragma unroll
+      for (int k = 0; k < KV; k++) {
+        const R dWx = rec[10 + k0 + k] * dr[0] + rec[20 + k0 + k] * dr[1] + rec[30 + k0 + k] * dr[2];
+        const R dW = dWx + rec[40 + k0 + k] * dtt;
+        limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
+      }
+    }
+  }
+  R tk[KV];
+#pragma unroll
+  for (int k = 0; k < KV; k++) {
+    gmin_frac(ln[k], lq[k]);
+    tk[k] = zero ? R(0) : ln[k] / lq[k];
+  }
+  if (valid) {
+#pragma unroll
+    for (int k = 0; k < KV; k++)
+      if (k == l) tau[10 * (size_t)c + k0 + k] = tk[k];
+  }
+  for (int q = q0 + l; q < q1; q += GL) {
+    const int f = lnk[q];
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE) || (ff & (FF_BND1 | FF_BND2))) continue;
+    const int2 e = s12[f];
+    const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
+    const double dt = smin(dtI, dtJ);
+    const double4 gg = geo[f], d = dr1[f];
+    const bool own = e.x == c;
+    const double dsl = own ? 0.0 : 2.0 * d.w;
+    const R dr[3] = {R(d.x - gg.x * dsl), R(d.y - gg.y * dsl), R(d.z - gg.z * dsl)};
+    const R dtt = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
+    R *o = fst + 20 * (size_t)f + (own ? 0 : 10) + k0;
+#pragma unroll
+    for (int k = 0; k < KV; k++) {
+      const R t = tk[k];
+      const int kk = k0 + k;
+      o[k] = rec[kk] + (((rec[10 + kk] * t) * dr[0] + (rec[20 + kk] * t) * dr[1] + (rec[30 + kk] * t) * dr[2]) +
+                        (rec[40 + kk] * t) * dtt);
+    }
+  }
+}
+
+// compute_reconstruction (MPI/compute_reconstruction.cpp:41-198): Voronoi
+// face gradient, local limiter, density positivity, per active cell.
+template <typename R>
+__global__ void __launch_bounds__(GTB) k_recon_g(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec) {
+  __shared__ R wsh[GCB][NF];
+  __shared__ R gsh[GCB][3 * NF];
+  const int g = threadIdx.x / (2 * GL), k0 = ((threadIdx.x / GL) & 1) * KV, l = threadIdx.x % GL;
+  const int c = blockIdx.x * GCB + g;
+  const bool valid = c < n && (act[c] & A_ACTIVE);
+  const bool boundary = valid && bnd[c] != NO_BOUNDARY;
+  R *wi = wsh[g];
+  if (valid && threadIdx.x % (2 * GL) < NF) wi[threadIdx.x % (2 * GL)] = Wst[10 * (size_t)c + threadIdx.x % (2 * GL)];
+  __syncthreads();
+  const int q0 = (valid && !boundary) ? off[c] : 0, q1 = (valid && !boundary) ? off[c + 1] : 0;
+  R Wx[KV], Wy[KV], Wz[KV], mn[KV], mx[KV];
+#pragma unroll
+  for (int k = 0; k < KV; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = R(0); }
+  double sc[3] = {0.0, 0.0, 0.0};
+  bool zero = false;
+  for (int q = q0 + l; q < q1; q += GL) {
+    const int f = lnk[q];
+    const int2 e = s12[f];
+    const bool own = e.x == c;
+    const int j = own ? e.y : e.x;
+    const double4 gg = geo[f];
+    const double4 o4 = own ? dr1[f] : dr2[f];
+    double d[3] = {o4.x, o4.y, o4.z};
+    if (own) wrap3(P, d);
+    sc[0] += d[0]; sc[1] += d[1]; sc[2] += d[2];
+    if (bnd[j] != NO_BOUNDARY) { zero = true; continue; }
+    const double area = gg.w;
+    const double sgn = (d[0] * gg.x + d[1] * gg.y + d[2] * gg.z) < 0.0 ? -1.0 : 1.0;
+    const double nrm[3] = {gg.x * sgn, gg.y * sgn, gg.z * sgn};
+    const double dsh = d[0] * nrm[0] + d[1] * nrm[1] + d[2] * nrm[2];
+    const double idsA = area * ((dsh != 0.0) ? 0.5 / dsh : 0.0);
+    const R drh[3] = {R(nrm[0] * dsh), R(nrm[1] * dsh), R(nrm[2] * dsh)};
+    const R fij[3] = {R(d[0] - nrm[0] * dsh), R(d[1] - nrm[1] * dsh), R(d[2] - nrm[2] * dsh)};
+    const R ia = R(idsA);
+    const R *Wj = Wst + 10 * (size_t)j + k0;
+#pragma unroll
+    for (int k = 0; k < KV; k++) {
+      const R wj = Wj[k], w0 = wi[k0 + k];
+      const R sum = wj + w0;
+      const R diff = wj - w0;
+      mn[k] = smin(mn[k], diff);
+      mx[k] = smax(mx[k], diff);
+      Wx[k] += (sum * drh[0] + diff * fij[0]) * ia;
+      Wy[k] += (sum * drh[1] + diff * fij[1]) * ia;
+      Wz[k] += (sum * drh[2] + diff * fij[2]) * ia;
+    }
+  }
+  zero = gany(zero);
+  const R invV = valid ? R(1.0 / cvol[c]) : R(0);
+  R *gr = gsh[g];
+#pragma unroll
+  for (int k = 0; k < KV; k++) {
+    mn[k] = gmin(mn[k]);
+    mx[k] = gmax(mx[k]);
+    const R gx = gsum(Wx[k]) * invV, gy = gsum(Wy[k]) * invV, gz = gsum(Wz[k]) * invV;
+    if (l == 0) { gr[k0 + k] = gx; gr[NF + k0 + k] = gy; gr[2 * NF + k0 + k] = gz; }
+  }
+  sc[0] = gsum(sc[0]); sc[1] = gsum(sc[1]); sc[2] = gsum(sc[2]);
+  __syncwarp();
+  R ln[KV], lq[KV];
+#pragma unroll
+  for (int k = 0; k < KV; k++) { ln[k] = R(1); lq[k] = R(1); }
+  if (!zero) {
+    for (int q = q0 + l; q < q1; q += GL) {
+      const int f = lnk[q];
+      const bool own = s12[f].x == c;
+      const double4 o4 = own ? dr1[f] : dr2[f];
+      double d[3] = {o4.x, o4.y, o4.z};
+      if (own) wrap3(P, d);
+      const R dd[3] = {R(d[0]), R(d[1]), R(d[2])};
+#pragma unroll
+      for (int k = 0; k < KV; k++) {
+        const int kk = k0 + k;
+        const R dWx = gr[kk] * dd[0] + gr[NF + kk] * dd[1] + gr[2 * NF + kk] * dd[2];
+        limiter_min(ln[k], lq[k], dWx, mn[k], mx[k]);
+      }
     }
   }
 #pragma unroll
-  for (int k = 0; k < KH; k++) to[k] = ln[k] / lq[k];
+  for (int k = 0; k < KV; k++) gmin_frac(ln[k], lq[k]);
+  if (!valid) return;
+  R *r = Wrec + 50 * (size_t)c;
+  if (boundary || zero) {
+    for (int k5 = l; k5 < 5 * KV; k5 += GL) {
+      const int blk = k5 / KV, k = k0 + k5 % KV;
+      r[blk * NF + k] = blk == 0 ? wi[k] : R(0);
+    }
+    return;
+  }
+  // density positivity (subgroup k0 == 0 holds DENS): every lane reads t of DENS
+  R a0 = R(1);
+  if (k0 == 0) {
+    const R lm0 = ln[0] / lq[0];
+    const R t0 = r[40] * lm0;
+    const R sum_dt = R(get_dt(P, rung[c]));
+    const R dWx = (gr[0] * lm0) * R(sc[0]) + (gr[NF] * lm0) * R(sc[1]) + (gr[2 * NF] * lm0) * R(sc[2]);
+    const R dWp = dWx + t0 * sum_dt;
+    const R dW = smax(dWx, dWp);
+    if (dW > R(0)) a0 = smin(R(1), R(0.9) * wi[0] / dW);
+  }
+  // every lane of the cell has read r[40] before it is rewritten
+  __syncwarp(group_mask());
+  for (int k5 = l; k5 < 5 * KV; k5 += GL) {
+    const int blk = k5 / KV, kv = k5 % KV, k = k0 + kv;
+    R v;
+    if (blk == 0) {
+      v = wi[k];
+    } else {
+      R lmk = R(1);
+#pragma unroll
+      for (int t = 0; t < KV; t++)
+        if (t == kv) lmk = ln[t] / lq[t];
+      const R base = blk == 4 ? r[40 + k] : gr[(blk - 1) * NF + k];
+      v = base * lmk;
+      if (k == 0) v *= a0;
+    }
+    r[blk * NF + k] = v;
+  }
 }
 
 // ---- compute_update face pass (MPI/compute_update.cpp:106-269) -----------
 // One thread per face: half-step extrapolated face states, face velocity,
 // rotated-frame HLLD flux.  Stores flux*dt*area, gradPsi and divB
-// contributions for the owning cells to gather.
-__global__ void __launch_bounds__(128) k_corr_flux(int nf, Params P, double t_global,
-    const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ cen,
-    const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const double *__restrict__ pos, const double *__restrict__ vel, const double *__restrict__ tlast,
-    const double *__restrict__ Wrec, const double *__restrict__ tau,
-    double *__restrict__ fcon, unsigned char *__restrict__ fcode) {
+// contributions (in the bulk type) for the owning cells to gather.
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Params P, const Sched *__restrict__ S,
+    const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
+    const unsigned char *__restrict__ fflag, const int *__restrict__ bnd, const double *__restrict__ vel,
+    const double *__restrict__ tlast, const R *__restrict__ Wrec, const R *__restrict__ fst,
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode) {
+  const double t_global = S->t_global;
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
+  const unsigned char ff = fflag[f];
+  if (!(ff & FF_ACTIVE)) { fcode[f] = F_OFF; return; }
   const int2 e = s12[f];
-  if (!face_active(act, bnd, e.x, e.y)) { fcode[f] = F_OFF; return; }
   int i = e.x, j = e.y;
-  const double4 g = geo[f], c = cen[f];
+  const double4 g = geo[f], d = dr1[f];
   const double area = g.w;
   double nrm[3] = {g.x, g.y, g.z};
-  const double *pa = pos + 3 * (size_t)e.x;
-  double dri[3] = {c.x - pa[0], c.y - pa[1], c.z - pa[2]};
+  double dri[3] = {d.x, d.y, d.z};
   unsigned char code = 0;
-  if (bnd[i] != NO_BOUNDARY) {
+  if (ff & FF_BND1) {
     i = e.y; j = e.x;
     nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2];
     dri[0] = -dri[0]; dri[1] = -dri[1]; dri[2] = -dri[2];
     code |= F_SWAP;
   }
-  const int jb = bnd[j];
-  if (jb != NO_BOUNDARY) code |= F_SKIPJ;
+  const bool jbnd = (code & F_SWAP) ? (ff & FF_BND1) : (ff & FF_BND2);
+  if (jbnd) code |= F_SKIPJ;
   const double dtI = t_global - tlast[i], dtJ = t_global - tlast[j];
   const double dt = smin(dtI, dtJ);
-  const double dti = dtI - 0.5 * dt, dtj = dtJ - 0.5 * dt;
-  const double dsh = dri[0] * nrm[0] + dri[1] * nrm[1] + dri[2] * nrm[2];
-  const double dsl = 2.0 * dsh;
-  const double drj[3] = {dri[0] - nrm[0] * dsl, dri[1] - nrm[1] * dsl, dri[2] - nrm[2] * dsl};
-  const double *ri = Wrec + 50 * (size_t)i, *rj = Wrec + 50 * (size_t)j;
-  double Wi[NF], Wj[NF];
-  if (jb != NO_BOUNDARY) {
+  const double dsh = d.w;  // (-dri).(-n) = dri.n
+  R Wi[NF], Wj[NF];
+  if (jbnd) {
+    const R *ri = Wrec + 50 * (size_t)i;
 #pragma unroll
     for (int k = 0; k < NF; k++) Wi[k] = Wj[k] = ri[k];
   } else {
-    const double *ti = tau + 10 * (size_t)i, *tj = tau + 10 * (size_t)j;
+    const R *fs = fst + 20 * (size_t)f;
 #pragma unroll
-    for (int k = 0; k < NF; k++) {
-      const double a = ti[k], b = tj[k];
-      Wi[k] = ri[k] + (((ri[10 + k] * a) * dri[0] + (ri[20 + k] * a) * dri[1] + (ri[30 + k] * a) * dri[2]) +
-                       (ri[40 + k] * a) * dti);
-      Wj[k] = rj[k] + (((rj[10 + k] * b) * drj[0] + (rj[20 + k] * b) * drj[1] + (rj[30 + k] * b) * drj[2]) +
-                       (rj[40 + k] * b) * dtj);
-    }
+    for (int k = 0; k < NF; k++) { Wi[k] = fs[k]; Wj[k] = fs[10 + k]; }
   }
   const double *vi = vel + 3 * (size_t)i, *vj = vel + 3 * (size_t)j;
   const double fij[3] = {dri[0] - nrm[0] * dsh, dri[1] - nrm[1] * dsh, dri[2] - nrm[2] * dsh};
   const double fdv = (vj[0] - vi[0]) * fij[0] + (vj[1] - vi[1]) * fij[1] + (vj[2] - vi[2]) * fij[2];
   const double ids2 = -0.5 * fdv * ((dsh > 0.0) ? 1.0 / sqr(dsh) : 0.0);
-  const double wij[3] = {(vj[0] + vi[0]) * 0.5 + dri[0] * ids2, (vj[1] + vi[1]) * 0.5 + dri[1] * ids2,
-                         (vj[2] + vi[2]) * 0.5 + dri[2] * ids2};
-  double psi, Bn, flux[NF];
-  compute_flux<double>(P, wij, Wi, Wj, jb, nrm, psi, Bn, flux);
+  const R wij[3] = {R((vj[0] + vi[0]) * 0.5 + dri[0] * ids2), R((vj[1] + vi[1]) * 0.5 + dri[1] * ids2),
+                    R((vj[2] + vi[2]) * 0.5 + dri[2] * ids2)};
+  const R nr[3] = {R(nrm[0]), R(nrm[1]), R(nrm[2])};
+  R psi, Bn, flux[NF];
+  const int jb = jbnd ? bnd[j] : NO_BOUNDARY;
+  compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
   const double tarea = dt * area;
-  double *o = fcon + 14 * (size_t)f;
+  R *o = fcon + 14 * (size_t)f;
 #pragma unroll
-  for (int k = 0; k < NF; k++) o[k] = flux[k] * tarea;
-  const double pt = psi * tarea;
-  o[10] = nrm[0] * pt; o[11] = nrm[1] * pt; o[12] = nrm[2] * pt;
-  o[13] = Bn * tarea;
+  for (int k = 0; k < NF; k++) o[k] = R(double(flux[k]) * tarea);
+  const double pt = double(psi) * tarea;
+  o[10] = R(nrm[0] * pt); o[11] = R(nrm[1] * pt); o[12] = R(nrm[2] * pt);
+  o[13] = R(double(Bn) * tarea);
   fcode[f] = code;
 }
 
-// ---- compute_update cell pass (MPI/compute_update.cpp:274-498) -----------
-__global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, double t_global,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const double *__restrict__ pos, const double *__restrict__ tlast, double *__restrict__ volp,
-    const double *__restrict__ Wrec, const double *__restrict__ tau,
-    const double *__restrict__ fcon, const unsigned char *__restrict__ fcode,
-    double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
-    unsigned long long *__restrict__ counters) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n) return;
-  const unsigned char ac = act[c];
-  if (!(ac & (A_ACTIVE | A_LNGB))) return;
-  double s[14];
+// Sum of the face contributions of cell c in its face order (the reference
+// scatters in active-face order; both orders sum the same terms).  The FP32
+// path accumulates its single-precision contributions in double with
+// compensated (Kahan) summation.
+template <typename R>
+__device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int *__restrict__ lnk,
+                                               const int2 *__restrict__ s12, const R *__restrict__ fcon,
+                                               const unsigned char *__restrict__ fcode, bool skipj_allowed,
+                                               double *s) {
+  constexpr bool kahan = sizeof(R) == 4;
+  double comp[14];
 #pragma unroll
-  for (int k = 0; k < 14; k++) s[k] = 0.0;
-  for (int q = off[c]; q < off[c + 1]; q++) {
+  for (int k = 0; k < 14; k++) { s[k] = 0.0; comp[k] = 0.0; }
+  for (int q = q0; q < q1; q++) {
     const int f = lnk[q];
     const unsigned char code = fcode[f];
     if (code & F_OFF) continue;
     const int2 e = s12[f];
     const int fi = (code & F_SWAP) ? e.y : e.x;
-    const double *o = fcon + 14 * (size_t)f;
-    if (c == fi) {
+    const bool is_i = c == fi;
+    if (!is_i && skipj_allowed && (code & F_SKIPJ)) continue;
+    const R *o = fcon + 14 * (size_t)f;
+    // U: i gets -F, j gets +F;  gradPsi and divB: i gets +, j gets -
 #pragma unroll
-      for (int k = 0; k < NF; k++) s[k] -= o[k];
-      s[10] = s[10] + o[10]; s[11] = s[11] + o[11]; s[12] = s[12] + o[12];
-      s[13] += o[13];
-    } else {
-      if (code & F_SKIPJ) continue;
-#pragma unroll
-      for (int k = 0; k < NF; k++) s[k] += o[k];
-      s[10] = s[10] - o[10]; s[11] = s[11] - o[11]; s[12] = s[12] - o[12];
-      s[13] -= o[13];
+    for (int k = 0; k < 14; k++) {
+      const double v = double(o[k]);
+      const double term = ((k < NF) == is_i) ? -v : v;
+      if (kahan) {
+        const double y = term - comp[k];
+        const double t = s[k] + y;
+        comp[k] = (t - s[k]) - y;
+        s[k] = t;
+      } else {
+        s[k] += term;
+      }
     }
   }
+}
+
+// Grouped form of gather_contrib: the GL lanes of a group split the cell's
+// faces and their partial sums (in double) are added in a fixed tree, so the
+// result is the same on every run.
+template <typename R>
+__device__ __forceinline__ void gather_contrib_g(int c, int q0, int q1, int l, const int *__restrict__ lnk,
+                                                 const int2 *__restrict__ s12, const R *__restrict__ fcon,
+                                                 const unsigned char *__restrict__ fcode, bool skipj_allowed,
+                                                 double *s) {
+#pragma unroll
+  for (int k = 0; k < 14; k++) s[k] = 0.0;
+  for (int q = q0 + l; q < q1; q += GL) {
+    const int f = lnk[q];
+    const unsigned char code = fcode[f];
+    if (code & F_OFF) continue;
+    const int2 e = s12[f];
+    const int fi = (code & F_SWAP) ? e.y : e.x;
+    const bool is_i = c == fi;
+    if (!is_i && skipj_allowed && (code & F_SKIPJ)) continue;
+    const R *o = fcon + 14 * (size_t)f;
+#pragma unroll
+    for (int k = 0; k < 14; k++) {
+      const double v = double(o[k]);
+      s[k] += ((k < NF) == is_i) ? -v : v;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 14; k++) s[k] = gsum(s[k]);
+}
+
+// ---- compute_update cell pass (MPI/compute_update.cpp:274-498) -----------
+template <typename R>
+__global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const double *__restrict__ pos, const double *__restrict__ tlast, double *__restrict__ volp,
+    const R *__restrict__ Wrec, const R *__restrict__ tau,
+    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
+    double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
+    unsigned long long *__restrict__ counters, const int *__restrict__ perm) {
+  const double t_global = S->t_global;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = perm[t];
+  const unsigned char ac = act[c];
+  if (!(ac & (A_ACTIVE | A_LNGB))) return;
+  double s[14];
+  gather_contrib<R>(c, off[c], off[c + 1], lnk, s12, fcon, fcode, true, s);
   double *d0 = dU + 14 * (size_t)c;
   if (!(ac & A_ACTIVE)) {
     // inactive neighbour: accumulate until its own step (collect_results,
@@ -303,22 +751,127 @@ __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, double t_glo
     for (int k = 0; k < 13; k++) sd[k] = 0.0;
     sd[13] = dt > 0.0 ? divB / dt / V : divB;
   }
-  const double *r = Wrec + 50 * (size_t)c;
-  const double *tc = tau + 10 * (size_t)c;
+  const R *r = Wrec + 50 * (size_t)c;
+  const R *tc = tau + 10 * (size_t)c;
   double W1[NF];
   if (Uc[MASS] <= 0.0) {
     // failed-mass fallback (MPI/compute_update.cpp:438-468)
     atomicAdd(&counters[0], 1ULL);
     double Ut[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) W1[k] = r[k] + (r[40 + k] * tc[k]) * dt;
+    for (int k = 0; k < NF; k++) W1[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dt;
     to_conservative(W1, volp[c], Ut);
     to_primitive(Ut, V, W1);
   } else {
     const double dth = 0.5 * dt;
     double Wh[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) Wh[k] = r[k] + (r[40 + k] * tc[k]) * dth;
+    for (int k = 0; k < NF; k++) Wh[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dth;
+    Uc[WBX] -= Wh[VELX] * divB;
+    Uc[WBY] -= Wh[VELY] * divB;
+    Uc[WBZ] -= Wh[VELZ] * divB;
+    // Dedner divergence cleaning (MPI/compute_update.cpp:373-387, 403-405)
+    const double pres = pressure(P, Wh);
+    const double B2 = Wh[BX] * Wh[BX] + Wh[BY] * Wh[BY] + Wh[BZ] * Wh[BZ];
+    const double dcs2 = P.gamma * pres + B2;
+    const double ch_sig = sqrt(dcs2 / Wh[DENS]);
+    Uc[WBX] -= dPsi[0];
+    Uc[WBY] -= dPsi[1];
+    Uc[WBZ] -= dPsi[2];
+    Uc[MPSI] -= dcs2 * divB;
+    const double l_min = pow(V / (4.0 * M_PI / 3.0), 1.0 / 3.0);
+    Uc[MPSI] *= exp(-0.5 * ch_sig / l_min * dt);
+    to_primitive(Uc, V, W1);
+  }
+  volp[c] = V;
+  W1[ETHM] = ethm_update(P, W1, pos + 3 * (size_t)c);
+  if (W1[ETHM] <= 0.0) {
+    atomicAdd(&counters[1], 1ULL);
+    W1[ETHM] = ethm_from_entropy(P, W1);
+  } else {
+    W1[ENTR] = entropy_from_ethm(P, W1);
+  }
+  double Un[NF];
+  to_conservative(W1, V, Un);
+  double *Uo = U + 10 * (size_t)c;
+#pragma unroll
+  for (int k = 0; k < NF; k++) Uo[k] = Un[k];
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_corr_cell_g(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const double *__restrict__ pos, const double *__restrict__ tlast, double *__restrict__ volp,
+    const R *__restrict__ Wrec, const R *__restrict__ tau,
+    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
+    double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
+    unsigned long long *__restrict__ counters) {
+  const double t_global = S->t_global;
+  const int c = blockIdx.x * (256 / GL) + threadIdx.x / GL, l = threadIdx.x % GL;
+  const unsigned char ac = c < n ? act[c] : 0;
+  const bool valid = ac & (A_ACTIVE | A_LNGB);
+  double s[14];
+  gather_contrib_g<R>(c, valid ? off[c] : 0, valid ? off[c + 1] : 0, l, lnk, s12, fcon, fcode, true, s);
+  if (!valid || l != 0) return;
+  double *d0 = dU + 14 * (size_t)c;
+  if (!(ac & A_ACTIVE)) {
+    // inactive neighbour: accumulate until its own step (collect_results,
+    // MPI/distribute_work.cpp:714-720)
+    if (stepdU) {
+#pragma unroll
+      for (int k = 0; k < 14; k++) stepdU[14 * (size_t)c + k] = s[k];
+    }
+    if (bnd[c] == NO_BOUNDARY) {
+#pragma unroll
+      for (int k = 0; k < NF; k++) d0[k] += s[k];
+      d0[13] += s[13];
+      d0[10] = d0[10] + s[10]; d0[11] = d0[11] + s[11]; d0[12] = d0[12] + s[12];
+    }
+    return;
+  }
+  const double V = cvol[c];
+  if (bnd[c] != NO_BOUNDARY) {
+    volp[c] = V;
+#pragma unroll
+    for (int k = 0; k < 14; k++) d0[k] = 0.0;
+    if (stepdU) {
+#pragma unroll
+      for (int k = 0; k < 14; k++) stepdU[14 * (size_t)c + k] = s[k];
+    }
+    return;
+  }
+  double Uc[NF];
+  const double *Ui = U + 10 * (size_t)c;
+#pragma unroll
+  for (int k = 0; k < NF; k++) Uc[k] = Ui[k] + (d0[k] + s[k]);
+  const double divB = d0[13] + s[13];
+  const double dPsi[3] = {d0[10] + s[10], d0[11] + s[11], d0[12] + s[12]};
+  const double dt = t_global - tlast[c];
+#pragma unroll
+  for (int k = 0; k < 14; k++) d0[k] = 0.0;  // dU_local = 0 (collect_results)
+  if (stepdU) {
+    double *sd = stepdU + 14 * (size_t)c;
+#pragma unroll
+    for (int k = 0; k < 13; k++) sd[k] = 0.0;
+    sd[13] = dt > 0.0 ? divB / dt / V : divB;
+  }
+  const R *r = Wrec + 50 * (size_t)c;
+  const R *tc = tau + 10 * (size_t)c;
+  double W1[NF];
+  if (Uc[MASS] <= 0.0) {
+    // failed-mass fallback (MPI/compute_update.cpp:438-468)
+    atomicAdd(&counters[0], 1ULL);
+    double Ut[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) W1[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dt;
+    to_conservative(W1, volp[c], Ut);
+    to_primitive(Ut, V, W1);
+  } else {
+    const double dth = 0.5 * dt;
+    double Wh[NF];
+#pragma unroll
+    for (int k = 0; k < NF; k++) Wh[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dth;
     Uc[WBX] -= Wh[VELX] * divB;
     Uc[WBY] -= Wh[VELY] * divB;
     Uc[WBZ] -= Wh[VELZ] * divB;
@@ -469,22 +1022,111 @@ __global__ void k_halve(int n, const unsigned char *__restrict__ act, const doub
 }
 
 // adjust_timesteps relaxation (MPI/compute_timestep.cpp:123-142).  The
-// reference relaxes neighbour pairs sequentially in site order and the
-// result depends on that order, so it is reproduced by one thread.
-__global__ void k_adjust_seq(int n, const int *__restrict__ off, const int *__restrict__ lnk,
-                             const int2 *__restrict__ s12, const unsigned char *__restrict__ act,
-                             const int *__restrict__ bnd, double *__restrict__ dtl,
-                             unsigned char *__restrict__ hash) {
+// reference relaxes neighbour pairs sequentially in site order and the result
+// depends on that order.  Exact reproduction in three parts:
+//  1. k_adjust_mark (parallel): hash marks, which do not depend on the order,
+//     and a count of "dirty" sites, active sites with a neighbour whose dt is
+//     outside a factor 2 of their own;
+//  2. with no dirty site every pair already satisfies the bound, no value
+//     changes, and the sweep is skipped;
+//  3. otherwise k_adjust_seq sweeps the ascending list of active
+//     non-boundary sites (compacted in parallel) in one thread, exactly as
+//     the reference does.
+__global__ void k_adjust_mark(int n, const int *__restrict__ off, const int *__restrict__ lnk,
+                              const int2 *__restrict__ s12, const unsigned char *__restrict__ act,
+                              const int *__restrict__ bnd, const double *__restrict__ dtl,
+                              unsigned char *__restrict__ hash, int *__restrict__ ndirty,
+                              unsigned char *__restrict__ site) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool dirty = false, s = false;
+  if (i < n && (act[i] & A_ACTIVE) && bnd[i] == NO_BOUNDARY) {
+    s = true;
+    const double di = dtl[i];
+    for (int q = off[i]; q < off[i + 1]; q++) {
+      const int2 e = s12[lnk[q]];
+      const int j = e.x == i ? e.y : e.x;
+      const double dj = dtl[j];
+      if (dj < 0.0) continue;
+      hash[j] = 1;
+      if (2.0 * dj < di || 2.0 * di < dj) dirty = true;
+    }
+  }
+  if (i < n) site[i] = s ? 1 : 0;
+  __shared__ int bsum;
+  if (threadIdx.x == 0) bsum = 0;
+  __syncthreads();
+  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, dirty));
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bsum, (int)cnt);
+  __syncthreads();
+  if (threadIdx.x == 0 && bsum) atomicAdd(ndirty, bsum);
+}
+
+// Order-preserving compaction of flagged cells: per-block counts, one-block
+// exclusive scan of the counts, then per-block placement.
+constexpr int CB = 1024;
+__global__ void k_count_flags(int n, const unsigned char *__restrict__ flag, int *__restrict__ bcount) {
+  const int i = blockIdx.x * CB + threadIdx.x;
+  const bool v = i < n && flag[i];
+  __shared__ int bs;
+  if (threadIdx.x == 0) bs = 0;
+  __syncthreads();
+  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, v));
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bs, (int)cnt);
+  __syncthreads();
+  if (threadIdx.x == 0) bcount[blockIdx.x] = bs;
+}
+__global__ void k_scan_counts(int nb, int *__restrict__ bcount, int *__restrict__ total) {
+  // one block of CB threads; nb <= CB * 16
+  __shared__ int part[CB];
+  const int per = (nb + CB - 1) / CB;
+  const int b0 = threadIdx.x * per;
+  int sum = 0;
+  for (int b = b0; b < b0 + per && b < nb; b++) sum += bcount[b];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int o = 1; o < CB; o <<= 1) {
+    const int v = threadIdx.x >= o ? part[threadIdx.x - o] : 0;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  int run = part[threadIdx.x] - sum;  // exclusive prefix of this thread's range
+  for (int b = b0; b < b0 + per && b < nb; b++) {
+    const int c = bcount[b];
+    bcount[b] = run;
+    run += c;
+  }
+  if (threadIdx.x == CB - 1) *total = part[CB - 1];
+}
+__global__ void k_place_flags(int n, const unsigned char *__restrict__ flag, const int *__restrict__ boff,
+                              int *__restrict__ list) {
+  const int i = blockIdx.x * CB + threadIdx.x;
+  const bool v = i < n && flag[i];
+  __shared__ int wsum[CB / 32];
+  const unsigned b = __ballot_sync(0xffffffffu, v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(b);
+  __syncthreads();
+  int base = boff[blockIdx.x];
+  for (int k = 0; k < w; k++) base += wsum[k];
+  if (v) list[base + __popc(b & ((1u << lane) - 1u))] = i;
+}
+
+__global__ void k_adjust_seq(const int *__restrict__ off, const int *__restrict__ lnk,
+                             const int2 *__restrict__ s12, const int *__restrict__ alist,
+                             const int *__restrict__ nsite, const int *__restrict__ ndirty,
+                             double *__restrict__ dtl) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  for (int i = 0; i < n; i++) {
-    if (!(act[i] & A_ACTIVE) || bnd[i] != NO_BOUNDARY) continue;
+  if (*ndirty == 0) return;
+  const int m = *nsite;
+  for (int a = 0; a < m; a++) {
+    const int i = alist[a];
     double di = dtl[i];
     for (int q = off[i]; q < off[i + 1]; q++) {
       const int2 e = s12[lnk[q]];
       const int j = e.x == i ? e.y : e.x;
       double dj = dtl[j];
       if (dj < 0.0) continue;
-      hash[j] = 1;
       di = smin(di, 2.0 * dj);
       dj = smin(dj, 2.0 * di);
       dtl[j] = dj;
@@ -496,11 +1138,14 @@ __global__ void k_adjust_seq(int n, const int *__restrict__ off, const int *__re
 // rung assignment and inactive-neighbour promotion (MPI/compute_timestep.cpp
 // :144-199) fused with collect_results (MPI/distribute_work.cpp:676-713) and
 // the tlast/tend update of correct() (set_problem.cpp generic hook)
-__global__ void k_rungs(int n, Params P, double t_global, int min_rung, int shared,
+template <typename R>
+__global__ void k_rungs(int n, Params P, const Sched *__restrict__ S, int shared,
                         const unsigned char *__restrict__ act, const unsigned char *__restrict__ hash,
                         const double *__restrict__ dtl, const double *__restrict__ dmin,
                         int *__restrict__ rung, double *__restrict__ tlast, double *__restrict__ tend,
-                        double *__restrict__ Wrec, int *__restrict__ iscal) {
+                        R *__restrict__ Wrec, int *__restrict__ iscal) {
+  const double t_global = S->t_global;
+  const int min_rung = S->min_rung;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const unsigned char a = act[i];
@@ -533,102 +1178,95 @@ __global__ void k_rungs(int n, Params P, double t_global, int min_rung, int shar
     rung[i] = rn < 0 ? -1 - rn : rn;
     tend[i] = tn;
     if (rn < 0) {
-      double *w = Wrec + 50 * (size_t)i;
-      for (int k = 10; k < 50; k++) w[k] = 0.0;
+      R *w = Wrec + 50 * (size_t)i;
+      for (int k = 10; k < 50; k++) w[k] = R(0);
     }
   }
 }
 
 // distribute_fluid_update_data: primitives of the updated state
-template <typename T>
+template <typename R>
 __global__ void k_wst(int n, const unsigned char *__restrict__ act, const double *__restrict__ U,
-                      const double *__restrict__ volp, T *__restrict__ Wst) {
+                      const double *__restrict__ volp, R *__restrict__ Wst) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !(act[i] & (A_ACTIVE | A_LNGB))) return;
   double W[NF];
   to_primitive(U + 10 * (size_t)i, volp[i], W);
 #pragma unroll
-  for (int k = 0; k < NF; k++) Wst[10 * (size_t)i + k] = (T)W[k];
+  for (int k = 0; k < NF; k++) Wst[10 * (size_t)i + k] = R(W[k]);
 }
 
 // ---- compute_update0 face pass (MPI/compute_update.cpp:713-810) ----------
-__global__ void __launch_bounds__(128) k_pred_flux(int nf, Params P,
-    const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ cen,
-    const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const double *__restrict__ pos, const double *__restrict__ vel, const double *__restrict__ Wst,
-    double *__restrict__ fcon, unsigned char *__restrict__ fcode) {
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Params P,
+    const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
+    const unsigned char *__restrict__ fflag, const int *__restrict__ bnd,
+    const double *__restrict__ vel, const R *__restrict__ Wst,
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   if (f >= nf) return;
+  const unsigned char ff = fflag[f];
+  if (!(ff & FF_ACTIVE)) { fcode[f] = F_OFF; return; }
   const int2 e = s12[f];
-  if (!face_active(act, bnd, e.x, e.y)) { fcode[f] = F_OFF; return; }
   int i = e.x, j = e.y;
-  const double4 g = geo[f], c = cen[f];
+  const double4 g = geo[f], d = dr1[f];
   const double area = g.w;
   double nrm[3] = {g.x, g.y, g.z};
-  const double *pa = pos + 3 * (size_t)e.x;
-  double dri[3] = {c.x - pa[0], c.y - pa[1], c.z - pa[2]};
+  double dri[3] = {d.x, d.y, d.z};
   unsigned char code = 0;
-  if (bnd[i] != NO_BOUNDARY) {
+  bool ib = ff & FF_BND1, jbf = ff & FF_BND2;
+  if (ib) {
     i = e.y; j = e.x;
     nrm[0] = -nrm[0]; nrm[1] = -nrm[1]; nrm[2] = -nrm[2];
     dri[0] = -dri[0]; dri[1] = -dri[1]; dri[2] = -dri[2];
     code |= F_SWAP;
+    const bool tmp = ib; ib = jbf; jbf = tmp;
   }
-  if (bnd[i] != NO_BOUNDARY) { fcode[f] = F_OFF; return; }
-  const int jb = bnd[j];
-  const double dsh = dri[0] * nrm[0] + dri[1] * nrm[1] + dri[2] * nrm[2];
-  double Wi[NF], Wj[NF];
-  const double *wi = Wst + 10 * (size_t)i, *wj = Wst + 10 * (size_t)(jb == NO_BOUNDARY ? j : i);
+  if (ib) { fcode[f] = F_OFF; return; }
+  const int jb = jbf ? bnd[j] : NO_BOUNDARY;
+  const double dsh = d.w;
+  R Wi[NF], Wj[NF];
+  const R *wi = Wst + 10 * (size_t)i, *wj = Wst + 10 * (size_t)(jb == NO_BOUNDARY ? j : i);
 #pragma unroll
   for (int k = 0; k < NF; k++) { Wi[k] = wi[k]; Wj[k] = wj[k]; }
   const double *vi = vel + 3 * (size_t)i, *vj = vel + 3 * (size_t)j;
   const double fij[3] = {dri[0] - nrm[0] * dsh, dri[1] - nrm[1] * dsh, dri[2] - nrm[2] * dsh};
   const double fdv = (vj[0] - vi[0]) * fij[0] + (vj[1] - vi[1]) * fij[1] + (vj[2] - vi[2]) * fij[2];
   const double ids2 = -0.5 * fdv * ((dsh > 0.0) ? 1.0 / sqr(dsh) : 0.0);
-  const double wij[3] = {(vj[0] + vi[0]) * 0.5 + dri[0] * ids2, (vj[1] + vi[1]) * 0.5 + dri[1] * ids2,
-                         (vj[2] + vi[2]) * 0.5 + dri[2] * ids2};
-  double psi, Bn, flux[NF];
-  compute_flux<double>(P, wij, Wi, Wj, jb, nrm, psi, Bn, flux);
-  double *o = fcon + 14 * (size_t)f;
+  const R wij[3] = {R((vj[0] + vi[0]) * 0.5 + dri[0] * ids2), R((vj[1] + vi[1]) * 0.5 + dri[1] * ids2),
+                    R((vj[2] + vi[2]) * 0.5 + dri[2] * ids2)};
+  const R nr[3] = {R(nrm[0]), R(nrm[1]), R(nrm[2])};
+  R psi, Bn, flux[NF];
+  compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
+  R *o = fcon + 14 * (size_t)f;
 #pragma unroll
-  for (int k = 0; k < NF; k++) o[k] = flux[k] * area;
-  const double pa2 = psi * area;
-  o[10] = nrm[0] * pa2; o[11] = nrm[1] * pa2; o[12] = nrm[2] * pa2;
-  o[13] = Bn * area;
+  for (int k = 0; k < NF; k++) o[k] = R(double(flux[k]) * area);
+  const double pa2 = double(psi) * area;
+  o[10] = R(nrm[0] * pa2); o[11] = R(nrm[1] * pa2); o[12] = R(nrm[2] * pa2);
+  o[13] = R(double(Bn) * area);
   fcode[f] = code;
 }
 
 // ---- compute_update0 cell pass + collect_reconstruction -------------------
 // (MPI/compute_update.cpp:812-964; MPI/distribute_work.cpp:820-834)
 // Writes the predicted time derivative t into the cell's Wrec and the
-// cell's final rung/tend.
-__global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, double t_global, int min_rung,
+// cell's final rung/tend.  Arithmetic in double for both bulk types.
+template <typename R>
+__global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched *__restrict__ S,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const double *__restrict__ pos, const double *__restrict__ U,
-    const double *__restrict__ fcon, const unsigned char *__restrict__ fcode,
-    int *__restrict__ rung, double *__restrict__ tend, double *__restrict__ Wrec) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= n || !(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
+    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
+    int *__restrict__ rung, double *__restrict__ tend, R *__restrict__ Wrec, const int *__restrict__ perm) {
+  const double t_global = S->t_global;
+  const int min_rung = S->min_rung;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int c = perm[t];
+  if (!(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
   const double V = cvol[c];
   double dot[14];
-#pragma unroll
-  for (int k = 0; k < 14; k++) dot[k] = 0.0;
-  for (int q = off[c]; q < off[c + 1]; q++) {
-    const int f = lnk[q];
-    const unsigned char code = fcode[f];
-    if (code & F_OFF) continue;
-    const int2 e = s12[f];
-    const int fi = (code & F_SWAP) ? e.y : e.x;
-    const double *o = fcon + 14 * (size_t)f;
-    const double sg = c == fi ? -1.0 : 1.0;
-#pragma unroll
-    for (int k = 0; k < NF; k++) dot[k] = sg < 0.0 ? dot[k] - o[k] : dot[k] + o[k];
-    dot[10] = sg < 0.0 ? dot[10] + o[10] : dot[10] - o[10];
-    dot[11] = sg < 0.0 ? dot[11] + o[11] : dot[11] - o[11];
-    dot[12] = sg < 0.0 ? dot[12] + o[12] : dot[12] - o[12];
-    dot[13] = sg < 0.0 ? dot[13] + o[13] : dot[13] - o[13];
-  }
+  gather_contrib<R>(c, off[c], off[c + 1], lnk, s12, fcon, fcode, false, dot);
   const double *U0 = U + 10 * (size_t)c;
   double u0[NF], W0[NF];
 #pragma unroll
@@ -662,9 +1300,68 @@ __global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, double t_glo
   if (W1[ETHM] <= 0.0) W1[ETHM] = W0[ETHM];
   else W1[ENTR] = entropy_from_ethm(P, W1);
   const double idt = 1.0 / dt;
-  double *r = Wrec + 50 * (size_t)c;
+  R *r = Wrec + 50 * (size_t)c;
 #pragma unroll
-  for (int k = 0; k < NF; k++) r[40 + k] = (W1[k] - W0[k]) * idt;
+  for (int k = 0; k < NF; k++) r[40 + k] = R((W1[k] - W0[k]) * idt);
+  // collect_reconstruction: rung = max(rung, get_rung(dt)), tend = t + dt(rung)
+  int rf = rung[c];
+  const int rb = get_rung(P, dt, min_rung);
+  rf = rf < rb ? rb : rf;
+  rung[c] = rf;
+  tend[c] = t_global + get_dt(P, rf);
+}
+
+template <typename R>
+__global__ void __launch_bounds__(256) k_pred_cell_g(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const double *__restrict__ pos, const double *__restrict__ U,
+    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
+    int *__restrict__ rung, double *__restrict__ tend, R *__restrict__ Wrec) {
+  const double t_global = S->t_global;
+  const int min_rung = S->min_rung;
+  const int c = blockIdx.x * (256 / GL) + threadIdx.x / GL, l = threadIdx.x % GL;
+  const bool valid = c < n && (act[c] & A_ACTIVE) && bnd[c] == NO_BOUNDARY;
+  double dot[14];
+  gather_contrib_g<R>(c, valid ? off[c] : 0, valid ? off[c + 1] : 0, l, lnk, s12, fcon, fcode, false, dot);
+  if (!valid || l != 0) return;
+  const double V = cvol[c];
+  const double *U0 = U + 10 * (size_t)c;
+  double u0[NF], W0[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) u0[k] = U0[k];
+  to_primitive(u0, V, W0);
+  int rg = rung[c];
+  while (rg < RUNGMAX - 1 && u0[MASS] + dot[MASS] * get_dt(P, rg) <= 0.0 * u0[MASS]) rg++;
+  const double dt = get_dt(P, rg);
+  double Uc[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) Uc[k] = u0[k] + dot[k] * dt;
+  {
+    const double divB = dot[13];
+    Uc[WBX] -= W0[VELX] * divB * dt;
+    Uc[WBY] -= W0[VELY] * divB * dt;
+    Uc[WBZ] -= W0[VELZ] * divB * dt;
+    const double pres = pressure(P, W0);
+    const double B2 = W0[BX] * W0[BX] + W0[BY] * W0[BY] + W0[BZ] * W0[BZ];
+    const double dcs2 = P.gamma * pres + B2;
+    const double ch_sig = sqrt(dcs2 / W0[DENS]);
+    Uc[WBX] -= dot[10] * dt;
+    Uc[WBY] -= dot[11] * dt;
+    Uc[WBZ] -= dot[12] * dt;
+    Uc[MPSI] -= dcs2 * divB * dt;
+    const double l_min = pow(V / (4.0 * M_PI / 3.0), 1.0 / 3.0);
+    Uc[MPSI] *= exp(-0.5 * ch_sig / l_min * dt);
+  }
+  double W1[NF];
+  to_primitive(Uc, V, W1);
+  W1[ETHM] = ethm_update(P, W1, pos + 3 * (size_t)c);
+  if (W1[ETHM] <= 0.0) W1[ETHM] = W0[ETHM];
+  else W1[ENTR] = entropy_from_ethm(P, W1);
+  const double idt = 1.0 / dt;
+  R *r = Wrec + 50 * (size_t)c;
+#pragma unroll
+  for (int k = 0; k < NF; k++) r[40 + k] = R((W1[k] - W0[k]) * idt);
   // collect_reconstruction: rung = max(rung, get_rung(dt)), tend = t + dt(rung)
   int rf = rung[c];
   const int rb = get_rung(P, dt, min_rung);
@@ -676,105 +1373,100 @@ __global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, double t_glo
 // ---- compute_reconstruction (MPI/compute_reconstruction.cpp:41-198) -------
 // Two threads per active cell, five primitives each: Voronoi face gradient of
 // the updated primitives, local limiter, density positivity rescale.
-__global__ void __launch_bounds__(128) k_recon(int n, Params P,
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_CELL_MINB) k_recon(int n, Params P,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double4 *__restrict__ geo, const double4 *__restrict__ cen, const double *__restrict__ cvol,
-    const unsigned char *__restrict__ act, const int *__restrict__ bnd, const double *__restrict__ pos,
-    const double *__restrict__ Wst, const int *__restrict__ rung, double *__restrict__ Wrec) {
+    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const int c = (int)(t >> 1);
+  if ((t >> 1) >= n) return;
+  const int c = perm[t >> 1];
   const int k0 = (int)(t & 1) * KH;
-  if (c >= n || !(act[c] & A_ACTIVE)) return;
-  double *r = Wrec + 50 * (size_t)c + k0;
-  const double *wsi = Wst + 10 * (size_t)c + k0;
-  double Wi[KH];
+  if (!(act[c] & A_ACTIVE)) return;
+  R *r = Wrec + 50 * (size_t)c + k0;
+  const R *wsi = Wst + 10 * (size_t)c + k0;
+  R Wi[KH];
 #pragma unroll
   for (int k = 0; k < KH; k++) Wi[k] = wsi[k];
   if (bnd[c] != NO_BOUNDARY) {
 #pragma unroll
-    for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = 0.0; r[20 + k] = 0.0; r[30 + k] = 0.0; r[40 + k] = 0.0; }
+    for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = R(0); r[20 + k] = R(0); r[30 + k] = R(0); r[40 + k] = R(0); }
     return;
   }
   const int q0 = off[c], q1 = off[c + 1];
-  double Wx[KH], Wy[KH], Wz[KH], mn[KH], mx[KH];
+  R Wx[KH], Wy[KH], Wz[KH], mn[KH], mx[KH];
 #pragma unroll
-  for (int k = 0; k < KH; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = 0.0; }
-  const double *ip = pos + 3 * (size_t)c;
-  const double px = ip[0], py = ip[1], pz = ip[2];
+  for (int k = 0; k < KH; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = R(0); }
   double sc[3] = {0.0, 0.0, 0.0};
   bool zero = false;
   for (int q = q0; q < q1; q++) {
     const int f = lnk[q];
-    const double4 g = geo[f], ce = cen[f];
-    double d[3] = {ce.x - px, ce.y - py, ce.z - pz};
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const double L = P.box[a];
-      if (d[a] > 0.5 * L) d[a] -= L;
-      else if (d[a] < -0.5 * L) d[a] += L;
-    }
+    const int2 e = s12[f];
+    const double4 g = geo[f];
+    const double4 o4 = e.x == c ? dr1[f] : dr2[f];
+    double d[3] = {o4.x, o4.y, o4.z};
+    if (e.x == c) wrap3(P, d);
     sc[0] = sc[0] + d[0]; sc[1] = sc[1] + d[1]; sc[2] = sc[2] + d[2];
     const double area = g.w;
     const double sgn = (d[0] * g.x + d[1] * g.y + d[2] * g.z) < 0.0 ? -1.0 : 1.0;
     const double nrm[3] = {g.x * sgn, g.y * sgn, g.z * sgn};
     const double dsh = d[0] * nrm[0] + d[1] * nrm[1] + d[2] * nrm[2];
     const double idsA = area * ((dsh != 0.0) ? 0.5 / dsh : 0.0);
-    const double drh[3] = {nrm[0] * dsh, nrm[1] * dsh, nrm[2] * dsh};
-    const double fij[3] = {d[0] - drh[0], d[1] - drh[1], d[2] - drh[2]};
-    const int2 e = s12[f];
+    const R drh[3] = {R(nrm[0] * dsh), R(nrm[1] * dsh), R(nrm[2] * dsh)};
+    const R fij[3] = {R(d[0] - nrm[0] * dsh), R(d[1] - nrm[1] * dsh), R(d[2] - nrm[2] * dsh)};
+    const R ia = R(idsA);
     const int j = e.x == c ? e.y : e.x;
     if (bnd[j] != NO_BOUNDARY) { zero = true; break; }
-    const double *Wj = Wst + 10 * (size_t)j + k0;
+    const R *Wj = Wst + 10 * (size_t)j + k0;
 #pragma unroll
     for (int k = 0; k < KH; k++) {
-      const double wj = Wj[k];
-      const double sum = wj + Wi[k];
-      const double diff = wj - Wi[k];
+      const R wj = Wj[k];
+      const R sum = wj + Wi[k];
+      const R diff = wj - Wi[k];
       mn[k] = smin(mn[k], diff);
       mx[k] = smax(mx[k], diff);
-      Wx[k] += (sum * drh[0] + diff * fij[0]) * idsA;
-      Wy[k] += (sum * drh[1] + diff * fij[1]) * idsA;
-      Wz[k] += (sum * drh[2] + diff * fij[2]) * idsA;
+      Wx[k] += (sum * drh[0] + diff * fij[0]) * ia;
+      Wy[k] += (sum * drh[1] + diff * fij[1]) * ia;
+      Wz[k] += (sum * drh[2] + diff * fij[2]) * ia;
     }
   }
   if (zero) {
 #pragma unroll
-    for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = 0.0; r[20 + k] = 0.0; r[30 + k] = 0.0; r[40 + k] = 0.0; }
+    for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = R(0); r[20 + k] = R(0); r[30 + k] = R(0); r[40 + k] = R(0); }
     return;
   }
-  const double invV = 1.0 / cvol[c];
-  double ln[KH], lq[KH];
+  const R invV = R(1.0 / cvol[c]);
+  R ln[KH], lq[KH];
 #pragma unroll
-  for (int k = 0; k < KH; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; ln[k] = 1.0; lq[k] = 1.0; }
+  for (int k = 0; k < KH; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; ln[k] = R(1); lq[k] = R(1); }
   for (int q = q0; q < q1; q++) {
-    const double4 ce = cen[lnk[q]];
-    double d[3] = {ce.x - px, ce.y - py, ce.z - pz};
-#pragma unroll
-    for (int a = 0; a < 3; a++) {
-      const double L = P.box[a];
-      if (d[a] > 0.5 * L) d[a] -= L;
-      else if (d[a] < -0.5 * L) d[a] += L;
-    }
+    const int f = lnk[q];
+    const bool own = s12[f].x == c;
+    const double4 o4 = own ? dr1[f] : dr2[f];
+    double d[3] = {o4.x, o4.y, o4.z};
+    if (own) wrap3(P, d);
+    const R dd[3] = {R(d[0]), R(d[1]), R(d[2])};
 #pragma unroll
     for (int k = 0; k < KH; k++) {
-      const double dWx = Wx[k] * d[0] + Wy[k] * d[1] + Wz[k] * d[2];
+      const R dWx = Wx[k] * dd[0] + Wy[k] * dd[1] + Wz[k] * dd[2];
       limiter_min(ln[k], lq[k], dWx, mn[k], mx[k]);
     }
   }
-  double tt[KH];
+  R tt[KH];
 #pragma unroll
   for (int k = 0; k < KH; k++) {
-    const double lm = ln[k] / lq[k];
+    const R lm = ln[k] / lq[k];
     Wx[k] *= lm; Wy[k] *= lm; Wz[k] *= lm;
     tt[k] = r[40 + k] * lm;
   }
   if (k0 == 0) {  // density positivity for the *-state (MPI/compute_reconstruction.cpp:179-197)
-    const double sum_dt = get_dt(P, rung[c]);
-    const double dWx = Wx[0] * sc[0] + Wy[0] * sc[1] + Wz[0] * sc[2];
-    const double dWp = dWx + tt[0] * sum_dt;
-    const double dW = smax(dWx, dWp);
-    if (dW > 0.0) {
-      const double alpha = smin(1.0, 0.9 * Wi[0] / dW);
+    const R sum_dt = R(get_dt(P, rung[c]));
+    const R dWx = Wx[0] * R(sc[0]) + Wy[0] * R(sc[1]) + Wz[0] * R(sc[2]);
+    const R dWp = dWx + tt[0] * sum_dt;
+    const R dW = smax(dWx, dWp);
+    if (dW > R(0)) {
+      const R alpha = smin(R(1), R(0.9) * Wi[0] / dW);
       Wx[0] *= alpha; Wy[0] *= alpha; Wz[0] *= alpha; tt[0] *= alpha;
     }
   }
@@ -782,13 +1474,55 @@ __global__ void __launch_bounds__(128) k_recon(int n, Params P,
   for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = Wx[k]; r[20 + k] = Wy[k]; r[30 + k] = Wz[k]; r[40 + k] = tt[k]; }
 }
 
-__global__ void k_shared_sync(int n, Params P, double t_global, const unsigned char *__restrict__ act,
+__global__ void k_shared_sync(int n, Params P, const Sched *__restrict__ S, const unsigned char *__restrict__ act,
                               const int *__restrict__ iscal, int *__restrict__ rung, double *__restrict__ tend) {
+  const double t_global = S->t_global;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !(act[i] & A_ACTIVE)) return;
   const int r = iscal[0];
   rung[i] = r;
   tend[i] = t_global + get_dt(P, r);
+}
+
+// Scheduler::pull_active_list (MPI/Scheduler.h:108-154) on the device: the
+// active rungs of this step are the set bits of tsysU ^ tnextU.
+__global__ void k_sched_begin(Params P, Sched *S) {
+  int max_rung = S->iscal[0];
+  if (max_rung < 0 || max_rung >= RUNGMAX - 1) {
+    S->iscal[2] |= 2;
+    max_rung = max_rung < 0 ? 0 : RUNGMAX - 2;
+  }
+  const unsigned long long dtU = 1ULL << (RUNGMAX - 1 - max_rung);
+  const unsigned long long tnextU = (S->tsysU / dtU + 1) * dtU;
+  const unsigned long long flags = S->tsysU ^ tnextU;
+  int min_rung = S->min_rung;
+  for (int b = 0; b < RUNGMAX; b++)
+    if (flags & (1ULL << b)) min_rung = RUNGMAX - 1 - b;
+  S->max_rung = max_rung;
+  S->min_rung = min_rung;
+  S->flags = flags;
+  S->tsysU = tnextU;
+  S->t_global = P.dt_tick * (double)tnextU;
+  S->dtmin = FVM_HUGE;
+  S->iscal[0] = 0;
+  S->iscal[1] = 0;
+  S->iscal[3] = 0;
+}
+
+__global__ void k_sched_end(Sched *S) {
+  S->nactive_total += (unsigned long long)S->iscal[1];
+  S->nfaces_total += (unsigned long long)S->iscal[3];
+  S->steps += 1;
+}
+
+__global__ void k_sched_set(Params P, Sched *S, unsigned long long tsysU, int reset_err) {
+  S->tsysU = tsysU;
+  S->t_global = P.dt_tick * (double)tsysU;
+  if (reset_err) {
+    S->min_rung = 0;
+    S->iscal[2] = 0;
+    S->nactive_total = S->nfaces_total = S->steps = 0;
+  }
 }
 
 __global__ void k_maxrung(int n, const int *__restrict__ rung, int *__restrict__ out) {
@@ -811,8 +1545,9 @@ __global__ void k_init_dt(int n, Params P, const int *__restrict__ bnd, const do
   if ((threadIdx.x & 31) == 0) atomic_min_pos(dmin, vmin);
 }
 
+template <typename R>
 __global__ void k_init_state(int n, const double *__restrict__ W, const double *__restrict__ cvol,
-                             double *__restrict__ U, double *__restrict__ dU, double *__restrict__ Wrec,
+                             double *__restrict__ U, double *__restrict__ dU, R *__restrict__ Wrec,
                              double *__restrict__ volp) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -823,21 +1558,28 @@ __global__ void k_init_state(int n, const double *__restrict__ W, const double *
 #pragma unroll
   for (int k = 0; k < NF; k++) U[10 * (size_t)i + k] = u[k];
   for (int k = 0; k < 14; k++) dU[14 * (size_t)i + k] = 0.0;
-  for (int k = 0; k < 50; k++) Wrec[50 * (size_t)i + k] = k < NF ? w[k] : 0.0;
+  for (int k = 0; k < 50; k++) Wrec[50 * (size_t)i + k] = R(k < NF ? w[k] : 0.0);
   volp[i] = cvol[i];
 }
 
-__global__ void k_limited_wrec(int n, const unsigned char *__restrict__ act, const double *__restrict__ Wrec,
-                               const double *__restrict__ tau, double *__restrict__ out) {
+template <typename R>
+__global__ void k_limited_wrec(int n, const unsigned char *__restrict__ act, const R *__restrict__ Wrec,
+                               const R *__restrict__ tau, double *__restrict__ out) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const double *r = Wrec + 50 * (size_t)i;
+  const R *r = Wrec + 50 * (size_t)i;
   double *o = out + 50 * (size_t)i;
   const bool imp = act[i] & (A_ACTIVE | A_LNGB);
   for (int k = 0; k < 50; k++) {
     const int v = k % 10;
-    o[k] = (k >= 10 && imp) ? r[k] * tau[10 * (size_t)i + v] : r[k];
+    o[k] = double((k >= 10 && imp) ? r[k] * tau[10 * (size_t)i + v] : r[k]);
   }
+}
+
+template <typename A, typename B>
+__global__ void k_convert(long long n, const A *__restrict__ in, B *__restrict__ out) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = B(in[i]);
 }
 
 __global__ void k_flux_kat(int nf, Params P, const double *wij, const double *Wi, const double *Wj,
@@ -884,12 +1626,17 @@ struct fvm_ctx {
   int min_rung, max_rung;
   double t_global;
   bool have_mesh, have_state, in_step;
+  bool fp32;    // bulk (reconstruction, limiter, flux) in single precision
+  size_t rb;    // bytes of one bulk value
   unsigned long long cur_flags;
   Dev d;
   std::vector<long long> h_off;
   std::vector<int> h_ids;
   bool keep_step_dU;
   float last_ms;
+  // one captured step per mode (shared / individual), replayed by fvm_run
+  cudaGraphExec_t graph[2];
+  Sched hS;  // host copy of the device scheduler, refreshed after synchronisation
   std::string err;
 };
 
@@ -948,6 +1695,37 @@ static int dalloc(fvm_ctx *c, T **p, size_t count) {
   return 0;
 }
 
+static int dalloc_bytes(fvm_ctx *c, void **p, size_t bytes) {
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    c->err = std::string("cudaMalloc: ") + cudaGetErrorString(e);
+    return FVM_ENOMEM;
+  }
+  return 0;
+}
+
+// Runs the statement with R bound to the context's bulk type.
+#define BULK(...)                  \
+  do {                             \
+    if (c->fp32) {                 \
+      using R = float;             \
+      __VA_ARGS__;                 \
+    } else {                       \
+      using R = double;            \
+      __VA_ARGS__;                 \
+    }                              \
+  } while (0)
+
+static void drop_graphs(fvm_ctx *c) {
+  for (int k = 0; k < 2; k++)
+    if (c->graph[k]) {
+      cudaGraphExecDestroy(c->graph[k]);
+      c->graph[k] = nullptr;
+    }
+}
+
 static void free_all(fvm_ctx *c) {
   void **ptrs = (void **)&c->d;
   for (size_t k = 0; k < sizeof(Dev) / sizeof(void *); k++)
@@ -976,6 +1754,9 @@ fvm_ctx *fvm_create(const fvm_params *p, int device) {
   c->max_rung = RUNGMAX - 1;
   c->t_global = 0.0;
   c->keep_step_dU = getenv("FVM_KEEP_STEP_DU") != nullptr;
+  if (p->precision != FVM_PREC_FP64 && p->precision != FVM_PREC_FP32) { delete c; return nullptr; }
+  c->fp32 = p->precision == FVM_PREC_FP32;
+  c->rb = c->fp32 ? sizeof(float) : sizeof(double);
   if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
     delete c;
@@ -989,6 +1770,7 @@ void fvm_destroy(fvm_ctx *c) {
   if (!c) return;
   cudaSetDevice(c->device);
   cudaStreamSynchronize(c->st);
+  drop_graphs(c);
   free_all(c);
   for (int k = 0; k < 2 * KT_COUNT; k++) cudaEventDestroy(c->kev[k]);
   cudaEventDestroy(c->ev0);
@@ -1018,6 +1800,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   for (int i = 0; i < ncell; i++)
     if (off[i + 1] < off[i]) { c->err = "fvm_set_mesh: CSR offsets decrease"; return FVM_EINVAL; }
   CK(cudaSetDevice(c->device));
+  drop_graphs(c);
   free_all(c);
   c->n = ncell;
   c->nf = nface;
@@ -1025,20 +1808,26 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   int rc = 0;
   Dev &d = c->d;
   rc |= dalloc(c, &d.s12, nface); rc |= dalloc(c, &d.geo, nface); rc |= dalloc(c, &d.cen, nface);
+  rc |= dalloc(c, &d.dr1, nface); rc |= dalloc(c, &d.dr2, nface); rc |= dalloc(c, &d.fflag, nface);
+  rc |= dalloc_bytes(c, &d.fst, 20 * c->rb * (size_t)nface);
   rc |= dalloc(c, &d.cvol, ncell); rc |= dalloc(c, &d.ccen, 3 * (size_t)ncell);
-  rc |= dalloc(c, &d.off, ncell + 1); rc |= dalloc(c, &d.lnk, nl);
+  rc |= dalloc(c, &d.off, ncell + 1); rc |= dalloc(c, &d.lnk, nl); rc |= dalloc(c, &d.perm, ncell);
+  rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
+  if ((ncell + CB - 1) / CB > CB * 16) { c->err = "fvm_set_mesh: more than 16M cells"; return FVM_ERANGE; }
   rc |= dalloc(c, &d.pos, 3 * (size_t)ncell); rc |= dalloc(c, &d.vel, 3 * (size_t)ncell);
   rc |= dalloc(c, &d.tlast, ncell); rc |= dalloc(c, &d.tend, ncell); rc |= dalloc(c, &d.volp, ncell);
   rc |= dalloc(c, &d.rung, ncell); rc |= dalloc(c, &d.bnd, ncell);
   rc |= dalloc(c, &d.U, 10 * (size_t)ncell); rc |= dalloc(c, &d.dU, 14 * (size_t)ncell);
-  rc |= dalloc(c, &d.Wrec, 50 * (size_t)ncell);
+  rc |= dalloc_bytes(c, &d.Wrec, 50 * c->rb * (size_t)ncell);
   rc |= dalloc(c, &d.act0, ncell); rc |= dalloc(c, &d.act, ncell); rc |= dalloc(c, &d.hash, ncell);
   rc |= dalloc(c, &d.fcode, nface); rc |= dalloc(c, &d.fcode2, nface);
-  rc |= dalloc(c, &d.tau, 10 * (size_t)ncell); rc |= dalloc(c, &d.fcon, 14 * (size_t)nface);
-  rc |= dalloc(c, &d.fcon2, 14 * (size_t)nface); rc |= dalloc(c, &d.Wst, 10 * (size_t)ncell);
+  rc |= dalloc_bytes(c, &d.tau, 10 * c->rb * (size_t)ncell);
+  rc |= dalloc_bytes(c, &d.fcon, 14 * c->rb * (size_t)nface);
+  rc |= dalloc_bytes(c, &d.fcon2, 14 * c->rb * (size_t)nface);
+  rc |= dalloc_bytes(c, &d.Wst, 10 * c->rb * (size_t)ncell);
   rc |= dalloc(c, &d.dtl, ncell);
   if (c->keep_step_dU) rc |= dalloc(c, &d.stepdU, 14 * (size_t)ncell);
-  rc |= dalloc(c, &d.dscal, 4); rc |= dalloc(c, &d.iscal, 8); rc |= dalloc(c, &d.counters, 4);
+  rc |= dalloc(c, &d.S, 1); rc |= dalloc(c, &d.counters, 4);
   if (rc) return FVM_ENOMEM;
   std::vector<int2> hs(nface);
   std::vector<double4> hg(nface), hc(nface);
@@ -1062,6 +1851,18 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   CK(cudaMemcpy(d.ccen, cell_centroid, sizeof(double) * 3 * ncell, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d.off, hoff.data(), sizeof(int) * (ncell + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d.lnk, ids, sizeof(int) * nl, cudaMemcpyHostToDevice));
+  {
+    std::vector<int> perm(ncell);
+    for (int i = 0; i < ncell; i++) perm[i] = i;
+#if FVM_CELL_PERM
+    for (int w0 = 0; w0 < ncell; w0 += CPW) {
+      const int w1 = std::min(ncell, w0 + CPW);
+      std::stable_sort(perm.begin() + w0, perm.begin() + w1,
+                       [&](int a, int b) { return off[a + 1] - off[a] < off[b + 1] - off[b]; });
+    }
+#endif
+    CK(cudaMemcpy(d.perm, perm.data(), sizeof(int) * ncell, cudaMemcpyHostToDevice));
+  }
   CK(cudaMemsetAsync(d.counters, 0, 4 * sizeof(unsigned long long), c->st));
   CK(cudaStreamSynchronize(c->st));
   c->have_mesh = true;
@@ -1069,14 +1870,22 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   return 0;
 }
 
-static int sched_max_rung(fvm_ctx *c) {
-  CK(cudaMemsetAsync(c->d.iscal, 0, sizeof(int), c->st));
-  k_maxrung<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, c->d.rung, c->d.iscal);
-  LAUNCH_CHECK();
-  int r = 0;
-  CK(cudaMemcpyAsync(&r, c->d.iscal, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+// Synchronise and refresh the host copy of the scheduler.
+static int read_sched(fvm_ctx *c) {
+  CK(cudaMemcpyAsync(&c->hS, c->d.S, sizeof(Sched), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  c->max_rung = r;
+  c->tsysU = c->hS.tsysU;
+  c->t_global = c->hS.t_global;
+  c->min_rung = c->hS.min_rung;
+  c->max_rung = c->hS.max_rung;
+  return 0;
+}
+
+// Rung maximum over all cells into S->iscal[0] (the next step's max_rung).
+static int enqueue_maxrung(fvm_ctx *c) {
+  CK(cudaMemsetAsync(&c->d.S->iscal[0], 0, sizeof(int), c->st));
+  k_maxrung<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, c->d.rung, &c->d.S->iscal[0]);
+  LAUNCH_CHECK();
   return 0;
 }
 
@@ -1095,18 +1904,22 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   else CK(cudaMemsetAsync(d.bnd, 0, sizeof(int) * n, c->st));
   CK(cudaMemsetAsync(d.vel, 0, sizeof(double) * 3 * (size_t)n, c->st));
   CK(cudaMemsetAsync(d.tlast, 0, sizeof(double) * n, c->st));
-  k_init_state<<<nblk(n, 128), 128, 0, c->st>>>(n, dW, d.cvol, d.U, d.dU, d.Wrec, d.volp);
+  k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
+  LAUNCH_CHECK();
+  BULK(k_init_state<R><<<nblk(n, 128), 128, 0, c->st>>>(n, dW, d.cvol, d.U, d.dU, (R *)d.Wrec, d.volp));
   LAUNCH_CHECK();
   // compute_pvel on all cells, then the shared timestep
   CK(cudaMemsetAsync(d.act, A_ACTIVE, n, c->st));
   k_pvel<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel);
   LAUNCH_CHECK();
-  const double hugev = FVM_HUGE;
-  CK(cudaMemcpyAsync(d.dscal, &hugev, sizeof(double), cudaMemcpyHostToDevice, c->st));
-  k_init_dt<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.bnd, d.U, d.volp, d.vel, d.pos, d.dscal);
+  Sched h0;
+  memset(&h0, 0, sizeof(h0));
+  h0.dtmin = FVM_HUGE;
+  CK(cudaMemcpyAsync(d.S, &h0, sizeof(Sched), cudaMemcpyHostToDevice, c->st));
+  k_init_dt<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.bnd, d.U, d.volp, d.vel, d.pos, &d.S->dtmin);
   LAUNCH_CHECK();
   double dtmin = 0.0;
-  CK(cudaMemcpyAsync(&dtmin, d.dscal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(&dtmin, &d.S->dtmin, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   cudaFree(dW);
   c->min_rung = 0;
@@ -1116,11 +1929,16 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   std::vector<double> ht(n, 0.0 + get_dt(c->P, rung));
   CK(cudaMemcpy(d.rung, hr.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d.tend, ht.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+  h0.iscal[0] = rung;  // max rung for the first pull
+  CK(cudaMemcpyAsync(d.S, &h0, sizeof(Sched), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
   c->tsysU = 0;
   c->t_global = 0.0;
   c->max_rung = rung;
+  c->min_rung = 0;
   c->have_state = true;
   c->in_step = false;
+  drop_graphs(c);
   return 0;
 }
 
@@ -1137,7 +1955,14 @@ int fvm_get_state(fvm_ctx *c, double *pos, double *vel, double *tlast, double *t
   if (rung) CK(cudaMemcpyAsync(rung, c->d.rung, n * sizeof(int), cudaMemcpyDeviceToHost, s));
   if (U) CK(cudaMemcpyAsync(U, c->d.U, 10 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
   if (dU) CK(cudaMemcpyAsync(dU, c->d.dU, 14 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
-  if (wrec) CK(cudaMemcpyAsync(wrec, c->d.Wrec, 50 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (wrec && !c->fp32) CK(cudaMemcpyAsync(wrec, c->d.Wrec, 50 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  if (wrec && c->fp32) {
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(&tmp, 50 * n * sizeof(double), s));
+    k_convert<float, double><<<nblk(50LL * n, 256), 256, 0, s>>>(50LL * n, (const float *)c->d.Wrec, tmp);
+    CK(cudaMemcpyAsync(wrec, tmp, 50 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaFreeAsync(tmp, s));
+  }
   CK(cudaStreamSynchronize(s));
   return 0;
 }
@@ -1159,72 +1984,84 @@ int fvm_set_state(fvm_ctx *c, const double *vel, const double *tlast, const doub
   if (tend) CK(cudaMemcpyAsync(c->d.tend, tend, n * sizeof(double), cudaMemcpyHostToDevice, s));
   if (U) CK(cudaMemcpyAsync(c->d.U, U, 10 * n * sizeof(double), cudaMemcpyHostToDevice, s));
   if (dU) CK(cudaMemcpyAsync(c->d.dU, dU, 14 * n * sizeof(double), cudaMemcpyHostToDevice, s));
-  if (wrec) CK(cudaMemcpyAsync(c->d.Wrec, wrec, 50 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (wrec && !c->fp32) CK(cudaMemcpyAsync(c->d.Wrec, wrec, 50 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  if (wrec && c->fp32) {
+    double *tmp = nullptr;
+    CK(cudaMallocAsync(&tmp, 50 * n * sizeof(double), s));
+    CK(cudaMemcpyAsync(tmp, wrec, 50 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    k_convert<double, float><<<nblk(50LL * n, 256), 256, 0, s>>>(50LL * n, tmp, (float *)c->d.Wrec);
+    CK(cudaFreeAsync(tmp, s));
+  }
   CK(cudaMemcpyAsync(c->d.volp, c->d.cvol, n * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  c->tsysU = tsys_ticks;
-  c->t_global = c->P.dt_tick * (double)tsys_ticks;
+  k_sched_set<<<1, 1, 0, s>>>(c->P, c->d.S, tsys_ticks, 0);
+  LAUNCH_CHECK();
+  int rc = enqueue_maxrung(c);
+  if (rc) return rc;
   c->have_state = true;
-  return sched_max_rung(c);
+  rc = read_sched(c);
+  c->max_rung = c->hS.iscal[0];
+  return rc;
 }
 
-int fvm_begin_step(fvm_ctx *c) {
-  if (!c || !c->have_state) { if (c) c->err = "fvm_begin_step: no state"; return FVM_ENOMESH; }
-  if (c->in_step) { c->err = "fvm_begin_step: previous step not finished"; return FVM_EINVAL; }
-  CK(cudaSetDevice(c->device));
-  const int max_rung = c->max_rung;
-  if (max_rung < 0 || max_rung >= RUNGMAX - 1) { c->err = "fvm_begin_step: max rung out of range"; return FVM_ERANGE; }
-  // Scheduler::pull_active_list (MPI/Scheduler.h:108-154)
-  const unsigned long long dtU = 1ULL << (RUNGMAX - 1 - max_rung);
-  const unsigned long long tnextU = (c->tsysU / dtU + 1) * dtU;
-  const unsigned long long flags = c->tsysU ^ tnextU;
-  for (int b = 0; b < RUNGMAX; b++)
-    if (flags & (1ULL << b)) c->min_rung = RUNGMAX - 1 - b;
-  c->tsysU = tnextU;
-  c->t_global = c->P.dt_tick * (double)c->tsysU;
-  c->cur_flags = flags;
+// ---- step launches (no host synchronisation) ------------------------------
+
+static int enq_begin(fvm_ctx *c) {
   const int n = c->n;
   Dev &d = c->d;
-  CK(cudaMemsetAsync(d.iscal, 0, 8 * sizeof(int), c->st));
   kt_begin(c, KT_FLAGS);
-  k_active<<<nblk(n, 256), 256, 0, c->st>>>(n, d.rung, flags, d.act0);
+  k_sched_begin<<<1, 1, 0, c->st>>>(c->P, d.S);
   LAUNCH_CHECK();
-  k_ngbflags<<<nblk(n, 128), 128, 0, c->st>>>(n, d.off, d.lnk, d.s12, d.act0, d.act, d.iscal);
+  k_active<<<nblk(n, 256), 256, 0, c->st>>>(n, d.rung, d.S, d.act, &d.S->iscal[1]);
+  LAUNCH_CHECK();
+  k_faceflags<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, d.s12, d.act, d.bnd, d.fflag, &d.S->iscal[3]);
   LAUNCH_CHECK();
   kt_end(c, KT_FLAGS);
-  c->in_step = true;
   return 0;
 }
 
-int fvm_slope_limiter(fvm_ctx *c) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_slope_limiter: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_limiter(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_LIMITER);
-  k_limiter<<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, c->t_global, d.off, d.lnk, d.s12, d.geo, d.cen,
-                                                 d.act, d.bnd, d.pos, d.tlast, d.Wrec, d.tau);
+#if FVM_CELLMAP_GROUPED
+  BULK(k_limiter_g<R><<<nblk(c->n, GCB), GTB, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.geo, d.dr1,
+                                                          d.fflag, d.act, d.tlast, (const R *)d.Wrec, (R *)d.tau,
+                                                          (R *)d.fst));
+#else
+  BULK(k_limiter<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.geo, d.dr1,
+                                                              d.fflag, d.act, d.tlast, (const R *)d.Wrec,
+                                                              (R *)d.tau, (R *)d.fst, d.perm));
+#endif
   LAUNCH_CHECK();
   kt_end(c, KT_LIMITER);
   return 0;
 }
 
-int fvm_compute_update(fvm_ctx *c) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_compute_update: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_update(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_CORR_FLUX);
-  k_corr_flux<<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, c->t_global, d.s12, d.geo, d.cen, d.act, d.bnd,
-                                                   d.pos, d.vel, d.tlast, d.Wrec, d.tau, d.fcon, d.fcode);
+  BULK(k_corr_flux<R><<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd,
+                                                           d.vel, d.tlast, (const R *)d.Wrec, (const R *)d.fst,
+                                                           (R *)d.fcon, d.fcode));
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_FLUX);
   kt_begin(c, KT_CORR_CELL);
-  k_corr_cell<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, c->t_global, d.off, d.lnk, d.s12, d.cvol, d.act,
-                                                  d.bnd, d.pos, d.tlast, d.volp, d.Wrec, d.tau, d.fcon, d.fcode,
-                                                  d.U, d.dU, d.stepdU, d.counters);
+#if FVM_GATHER_GROUPED
+  BULK(k_corr_cell_g<R><<<nblk(c->n, 256 / GL), 256, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+                                                          d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
+                                                          (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
+                                                          d.stepdU, d.counters));
+#else
+  BULK(k_corr_cell<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+                                                          d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
+                                                          (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
+                                                          d.stepdU, d.counters, d.perm));
+#endif
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_CELL);
   return 0;
 }
 
-int fvm_compute_pvel(fvm_ctx *c) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_compute_pvel: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_pvel(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PVEL);
   k_pvel<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel);
@@ -1233,124 +2070,239 @@ int fvm_compute_pvel(fvm_ctx *c) {
   return 0;
 }
 
-int fvm_compute_timesteps(fvm_ctx *c, int shared, double *dt_min_out) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_compute_timesteps: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_timesteps(fvm_ctx *c, int shared) {
   Dev &d = c->d;
   const int n = c->n;
-  const double hugev = FVM_HUGE;
-  CK(cudaMemcpyAsync(d.dscal, &hugev, sizeof(double), cudaMemcpyHostToDevice, c->st));
   kt_begin(c, KT_TIMESTEP);
   k_timestep<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.off, d.lnk, d.s12, d.act, d.bnd, d.U, d.volp, d.vel,
-                                               d.pos, d.tlast, d.tend, d.dtl, d.dscal);
+                                               d.pos, d.tlast, d.tend, d.dtl, &d.S->dtmin);
   LAUNCH_CHECK();
-  kt_end(c, KT_TIMESTEP);
   if (!shared) {
-    k_halve<<<nblk(n, 256), 256, 0, c->st>>>(n, d.act, d.dscal, d.dtl);
+    k_halve<<<nblk(n, 256), 256, 0, c->st>>>(n, d.act, &d.S->dtmin, d.dtl);
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(d.hash, 0, n, c->st));
-    k_adjust_seq<<<1, 32, 0, c->st>>>(n, d.off, d.lnk, d.s12, d.act, d.bnd, d.dtl, d.hash);
+    CK(cudaMemsetAsync(&d.S->iscal[4], 0, 2 * sizeof(int), c->st));
+    k_adjust_mark<<<nblk(n, 128), 128, 0, c->st>>>(n, d.off, d.lnk, d.s12, d.act, d.bnd, d.dtl, d.hash,
+                                                   &d.S->iscal[4], d.act0);
+    LAUNCH_CHECK();
+    const int nb = (int)((n + CB - 1) / CB);
+    k_count_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount);
+    LAUNCH_CHECK();
+    k_scan_counts<<<1, CB, 0, c->st>>>(nb, d.bcount, &d.S->iscal[5]);
+    LAUNCH_CHECK();
+    k_place_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount, d.alist);
+    LAUNCH_CHECK();
+    k_adjust_seq<<<1, 32, 0, c->st>>>(d.off, d.lnk, d.s12, d.alist, &d.S->iscal[5], &d.S->iscal[4], d.dtl);
     LAUNCH_CHECK();
   }
+  kt_end(c, KT_TIMESTEP);
   kt_begin(c, KT_RUNGS);
-  k_rungs<<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, c->t_global, c->min_rung, shared, d.act, d.hash, d.dtl,
-                                            d.dscal, d.rung, d.tlast, d.tend, d.Wrec, d.iscal);
+  BULK(k_rungs<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.S, shared, d.act, d.hash, d.dtl, &d.S->dtmin, d.rung,
+                                                   d.tlast, d.tend, (R *)d.Wrec, d.S->iscal));
   LAUNCH_CHECK();
   kt_end(c, KT_RUNGS);
-  if (dt_min_out) {
-    CK(cudaMemcpyAsync(dt_min_out, d.dscal, sizeof(double), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-  }
   return 0;
 }
 
-int fvm_collect_results(fvm_ctx *c) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_collect_results: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_collect(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_WST);
-  k_wst<double><<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, d.act, d.U, d.volp, d.Wst);
+  BULK(k_wst<R><<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, d.act, d.U, d.volp, (R *)d.Wst));
   LAUNCH_CHECK();
   kt_end(c, KT_WST);
   return 0;
 }
 
-int fvm_compute_update0(fvm_ctx *c) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_compute_update0: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_update0(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_FLUX);
-  k_pred_flux<<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.act, d.bnd, d.pos, d.vel,
-                                                   d.Wst, d.fcon2, d.fcode2);
+  BULK(k_pred_flux<R><<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd,
+                                                           d.vel, (const R *)d.Wst, (R *)d.fcon2, d.fcode2));
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_FLUX);
   return 0;
 }
 
-int fvm_compute_reconstruction(fvm_ctx *c) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_compute_reconstruction: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_recon(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_CELL);
-  k_pred_cell<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, c->t_global, c->min_rung, d.off, d.lnk, d.s12,
-                                                  d.cvol, d.act, d.bnd, d.pos, d.U, d.fcon2, d.fcode2, d.rung,
-                                                  d.tend, d.Wrec);
+#if FVM_GATHER_GROUPED
+  BULK(k_pred_cell_g<R><<<nblk(c->n, 256 / GL), 256, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+                                                          d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
+                                                          d.tend, (R *)d.Wrec));
+#else
+  BULK(k_pred_cell<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+                                                          d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
+                                                          d.tend, (R *)d.Wrec, d.perm));
+#endif
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_CELL);
   kt_begin(c, KT_RECON);
-  k_recon<<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.s12, d.geo, d.cen, d.cvol, d.act,
-                                                    d.bnd, d.pos, d.Wst, d.rung, d.Wrec);
+#if FVM_CELLMAP_GROUPED
+  BULK(k_recon_g<R><<<nblk(c->n, GCB), GTB, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.geo, d.dr1,
+                                                        d.dr2, d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
+                                                        (R *)d.Wrec));
+#else
+  BULK(k_recon<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.s12, d.geo, d.dr1, d.dr2,
+                                                            d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
+                                                            (R *)d.Wrec, d.perm));
+#endif
   LAUNCH_CHECK();
   kt_end(c, KT_RECON);
   return 0;
 }
 
-int fvm_end_step(fvm_ctx *c, int shared) {
-  if (!c || !c->in_step) { if (c) c->err = "fvm_end_step: call fvm_begin_step first"; return FVM_EINVAL; }
+static int enq_end(fvm_ctx *c, int shared) {
   Dev &d = c->d;
-  if (shared) {
-    kt_begin(c, KT_SYNC);
-  CK(cudaMemsetAsync(d.iscal, 0, sizeof(int), c->st));
-  k_maxrung<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, d.rung, d.iscal);
-  LAUNCH_CHECK();
-  k_shared_sync<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, c->P, c->t_global, d.act, d.iscal, d.rung, d.tend);
-    LAUNCH_CHECK();
-  kt_end(c, KT_SYNC);
-    int h[3];
-    CK(cudaMemcpyAsync(h, d.iscal, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    kt_collect(c);
-    c->in_step = false;
-    if (h[2]) { c->err = "rung out of range"; return FVM_ERANGE; }
-    c->max_rung = h[0];
-    return h[1];
-  }
-  int h[3];
-  CK(cudaMemcpyAsync(h, d.iscal, 3 * sizeof(int), cudaMemcpyDeviceToHost, c->st));
-  c->in_step = false;
-  int rc = sched_max_rung(c);
-  kt_collect(c);
+  kt_begin(c, KT_SYNC);
+  int rc = enqueue_maxrung(c);
   if (rc) return rc;
-  if (h[2]) { c->err = "rung out of range"; return FVM_ERANGE; }
-  return h[1];
+  if (shared) {
+    k_shared_sync<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, c->P, d.S, d.act, d.S->iscal, d.rung, d.tend);
+    LAUNCH_CHECK();
+  }
+  k_sched_end<<<1, 1, 0, c->st>>>(d.S);
+  LAUNCH_CHECK();
+  kt_end(c, KT_SYNC);
+  return 0;
+}
+
+static int enq_step(fvm_ctx *c, int shared) {
+  int rc;
+  if ((rc = enq_begin(c))) return rc;
+  if ((rc = enq_limiter(c))) return rc;
+  if ((rc = enq_update(c))) return rc;
+  if ((rc = enq_pvel(c))) return rc;
+  if ((rc = enq_timesteps(c, shared))) return rc;
+  if ((rc = enq_collect(c))) return rc;
+  if ((rc = enq_update0(c))) return rc;
+  if ((rc = enq_recon(c))) return rc;
+  return enq_end(c, shared);
+}
+
+static int check_sched_errors(fvm_ctx *c) {
+  if (c->hS.iscal[2]) {
+    c->err = "rung left [0, 31) (flags " + std::to_string(c->hS.iscal[2]) + ")";
+    return FVM_ERANGE;
+  }
+  return 0;
+}
+
+// ---- the reference call sequence, one entry point per member function -----
+
+#define STEP_GUARD(name)                                                                  \
+  do {                                                                                    \
+    if (!c || !c->in_step) {                                                              \
+      if (c) c->err = std::string(name) + ": call fvm_begin_step first";                  \
+      return FVM_EINVAL;                                                                  \
+    }                                                                                     \
+  } while (0)
+
+int fvm_begin_step(fvm_ctx *c) {
+  if (!c || !c->have_state) { if (c) c->err = "fvm_begin_step: no state"; return FVM_ENOMESH; }
+  if (c->in_step) { c->err = "fvm_begin_step: previous step not finished"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  int rc = enq_begin(c);
+  if (rc) return rc;
+  if ((rc = read_sched(c))) return rc;
+  if ((rc = check_sched_errors(c))) return rc;
+  c->in_step = true;
+  return c->hS.iscal[1];
+}
+
+int fvm_slope_limiter(fvm_ctx *c) { STEP_GUARD("fvm_slope_limiter"); return enq_limiter(c); }
+int fvm_compute_update(fvm_ctx *c) { STEP_GUARD("fvm_compute_update"); return enq_update(c); }
+int fvm_compute_pvel(fvm_ctx *c) { STEP_GUARD("fvm_compute_pvel"); return enq_pvel(c); }
+
+int fvm_compute_timesteps(fvm_ctx *c, int shared, double *dt_min_out) {
+  STEP_GUARD("fvm_compute_timesteps");
+  int rc = enq_timesteps(c, shared);
+  if (rc) return rc;
+  if (dt_min_out) {
+    CK(cudaMemcpyAsync(dt_min_out, &c->d.S->dtmin, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return 0;
+}
+
+int fvm_collect_results(fvm_ctx *c) { STEP_GUARD("fvm_collect_results"); return enq_collect(c); }
+int fvm_compute_update0(fvm_ctx *c) { STEP_GUARD("fvm_compute_update0"); return enq_update0(c); }
+int fvm_compute_reconstruction(fvm_ctx *c) { STEP_GUARD("fvm_compute_reconstruction"); return enq_recon(c); }
+
+int fvm_end_step(fvm_ctx *c, int shared) {
+  STEP_GUARD("fvm_end_step");
+  c->in_step = false;
+  int rc = enq_end(c, shared);
+  if (rc) return rc;
+  if ((rc = read_sched(c))) return rc;
+  kt_collect(c);
+  c->max_rung = c->hS.iscal[0];
+  if ((rc = check_sched_errors(c))) return rc;
+  return c->hS.iscal[1];
 }
 
 int fvm_step(fvm_ctx *c, int shared) {
-  int rc;
-  if ((rc = fvm_begin_step(c)) < 0) return rc;
+  if (!c || !c->have_state) { if (c) c->err = "fvm_step: no state"; return FVM_ENOMESH; }
+  if (c->in_step) { c->err = "fvm_step: inside a step"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
   CK(cudaEventRecord(c->ev0, c->st));
-  if ((rc = fvm_slope_limiter(c)) < 0) return rc;
-  if ((rc = fvm_compute_update(c)) < 0) return rc;
-  if ((rc = fvm_compute_pvel(c)) < 0) return rc;
-  if ((rc = fvm_compute_timesteps(c, shared, nullptr)) < 0) return rc;
-  if ((rc = fvm_collect_results(c)) < 0) return rc;
-  if ((rc = fvm_compute_update0(c)) < 0) return rc;
-  if ((rc = fvm_compute_reconstruction(c)) < 0) return rc;
+  int rc = enq_step(c, shared);
+  if (rc) return rc;
   CK(cudaEventRecord(c->ev1, c->st));
-  rc = fvm_end_step(c, shared);
+  if ((rc = read_sched(c))) return rc;
+  kt_collect(c);
   cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
-  return rc;
+  c->max_rung = c->hS.iscal[0];
+  if ((rc = check_sched_errors(c))) return rc;
+  return c->hS.iscal[1];
+}
+
+// nsteps steps from one captured CUDA graph per mode, no host round trip
+// between steps.  Per-kernel profiling is not recorded in this mode.
+int fvm_run(fvm_ctx *c, int nsteps, int shared, long long *faces_out) {
+  if (!c || !c->have_state) { if (c) c->err = "fvm_run: no state"; return FVM_ENOMESH; }
+  if (c->in_step || nsteps < 0) { c->err = "fvm_run: bad call"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  const int g = shared ? 1 : 0;
+  if (!c->graph[g]) {
+    const bool prof = c->prof;
+    c->prof = false;
+    cudaGraph_t gr = nullptr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    int rc = enq_step(c, shared);
+    cudaError_t e = cudaStreamEndCapture(c->st, &gr);
+    c->prof = prof;
+    if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+    if (e != cudaSuccess) { c->err = std::string("graph capture: ") + cudaGetErrorString(e); return FVM_ECUDA; }
+    e = cudaGraphInstantiate(&c->graph[g], gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) { c->graph[g] = nullptr; c->err = std::string("graph instantiate: ") + cudaGetErrorString(e); return FVM_ECUDA; }
+  }
+  CK(cudaMemcpyAsync(&c->hS, c->d.S, sizeof(Sched), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const unsigned long long a0 = c->hS.nactive_total, f0 = c->hS.nfaces_total;
+  CK(cudaEventRecord(c->ev0, c->st));
+  for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(c->graph[g], c->st));
+  CK(cudaEventRecord(c->ev1, c->st));
+  int rc = read_sched(c);
+  if (rc) return rc;
+  cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
+  c->max_rung = c->hS.iscal[0];
+  if ((rc = check_sched_errors(c))) return rc;
+  if (faces_out) *faces_out = (long long)(c->hS.nfaces_total - f0);
+  return (int)(c->hS.nactive_total - a0);
 }
 
 double fvm_time(const fvm_ctx *c) { return c ? c->t_global : 0.0; }
 
 void *fvm_stream(fvm_ctx *c) { return c ? (void *)c->st : nullptr; }
+
+int fvm_last_step_counts(const fvm_ctx *c, int *ncell_active, int *nface_active) {
+  if (!c) return FVM_EINVAL;
+  if (ncell_active) *ncell_active = c->hS.iscal[1];
+  if (nface_active) *nface_active = c->hS.iscal[3];
+  return 0;
+}
 long long fvm_launch_count(const fvm_ctx *c) { return c ? c->launches : 0; }
 
 int fvm_set_profiling(fvm_ctx *c, int on) {
@@ -1400,7 +2352,8 @@ int fvm_get_limited_wrec(fvm_ctx *c, double *wrec) {
   CK(cudaSetDevice(c->device));
   double *tmp = nullptr;
   CK(cudaMalloc(&tmp, 50 * sizeof(double) * (size_t)c->n));
-  k_limited_wrec<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->d.act, c->d.Wrec, c->d.tau, tmp);
+  BULK(k_limited_wrec<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->d.act, (const R *)c->d.Wrec,
+                                                             (const R *)c->d.tau, tmp));
   cudaError_t e = cudaMemcpyAsync(wrec, tmp, 50 * sizeof(double) * (size_t)c->n, cudaMemcpyDeviceToHost, c->st);
   cudaStreamSynchronize(c->st);
   cudaFree(tmp);

@@ -296,14 +296,28 @@ __device__ __forceinline__ T limiter(T dWi, T dWj_min, T dWj_max) {
 // n(x)/q(x) with q >= 2, and n1/q1 < n2/q2 <=> n1*q2 < n2*q1.  The caller
 // starts from n = q = 1 (the reference's initial 1.0) and finishes with one
 // division n/q per primitive.
+#ifndef FVM_LIMITER_DIVFREE
+#define FVM_LIMITER_DIVFREE 1
+#endif
 template <typename T>
 __device__ __forceinline__ void limiter_min(T &n, T &q, T dWi, T dWj_min, T dWj_max) {
   const bool flat = fabs(dWi) <= T(1.0e-16) * smax(fabs(dWj_max), fabs(dWj_min));
   const T num = dWi < T(0) ? dWj_min : dWj_max;
-  const T x = num / (flat ? T(1) : dWi);
   const T e = T(0.2 * 1.0e-16);
-  T pn = x * x + T(2) * x + e;
-  T pq = x * x + x + T(2) + e;
+  T pn, pq;
+#if FVM_LIMITER_DIVFREE
+  // Phi(m/d) = (m^2 + 2md + e d^2) / (m^2 + md + (2+e) d^2): no division per
+  // face.  Not flat means |d| > 1e-16 |m|, so neither part underflows for
+  // m != 0; m == 0 is Phi(0) = e/(2+e) exactly as in the reference.
+  const T m = num, d = dWi;
+  pn = m * m + T(2) * m * d + e * d * d;
+  pq = m * m + m * d + (T(2) + e) * d * d;
+  if (m == T(0)) { pn = e; pq = T(2) + e; }
+#else
+  const T x = num / (flat ? T(1) : dWi);
+  pn = x * x + T(2) * x + e;
+  pq = x * x + x + T(2) + e;
+#endif
   if (flat) { pn = T(1); pq = T(1); }
   if (pn * q < n * pq) { n = pn; q = pq; }
 }

@@ -273,6 +273,10 @@ void build_cell(int i, int n, const double *pos, const Grid &G, double tol_rel, 
     fn = fn * 0.5;
     if (fn.norm() == 0.0) continue;
     if (fc.dot(fn) < 0.0) fn = fn * -1.0;
+    // a cell may meet each neighbour once: two faces with the same neighbour
+    // mean the cell spans more than half the periodic box
+    for (size_t q = 0; q < res.ngb.size(); q++)
+      if (res.ngb[q] == p.ngb) res.err |= 4;
     res.ngb.push_back(p.ngb);
     res.n.push_back(fn);
     res.c.push_back(fc);

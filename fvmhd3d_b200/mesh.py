@@ -91,7 +91,9 @@ def build_periodic(pos: np.ndarray, box, nthreads: int = 0) -> Mesh:
     try:
         err = lib.fvm_mesh_error(h)
         if err:
-            raise RuntimeError(f"Voronoi build error flag {err} (candidate search or bounding box)")
+            raise RuntimeError(f"Voronoi build error flag {err}: 1 candidate search exhausted, 2 cell reaches the "
+                               "bounding box, 4 a cell meets two periodic images of one neighbour (mesh too "
+                               "coarse for the box)")
         nface = ctypes.c_int(0)
         nlink = ctypes.c_longlong(0)
         lib.fvm_mesh_sizes(h, ctypes.byref(nface), ctypes.byref(nlink))
@@ -107,7 +109,16 @@ def build_periodic(pos: np.ndarray, box, nthreads: int = 0) -> Mesh:
         lib.fvm_mesh_fetch(h, _ptr(s1), _ptr(s2), _ptr(fn), _ptr(fc), _ptr(vol), _ptr(cc), _ptr(off), _ptr(ids))
     finally:
         lib.fvm_mesh_free(h)
-    return Mesh(box, pos, s1, s2, fn, fc, vol, cc, off, ids)
+    m = Mesh(box, pos, s1, s2, fn, fc, vol, cc, off, ids)
+    # The mesh holds one face per cell pair (minimum image), so every cell
+    # must be closed: a cell that meets two periodic images of a neighbour
+    # (mesh too coarse for the box) shows up here.  Same bound as the
+    # reference's check, MPI/compute_update.cpp:307-320.
+    bad = np.nonzero(m.closure_error() >= 1e-10)[0]
+    if bad.size:
+        raise RuntimeError(f"Voronoi mesh not closed for {bad.size} cells (first {int(bad[0])}): the generators "
+                           "are too coarse for the periodic box")
+    return m
 
 
 def jittered_lattice(nside: int, jitter: float = 0.1, seed: int = 1, box: float = 1.0) -> np.ndarray:

@@ -83,3 +83,64 @@ def perturbed(W: np.ndarray, rel: float = 0.05, seed: int = 7) -> np.ndarray:
     W[:, VELX:VELZ + 1] += rel * rng.uniform(-1, 1, (n, 3))
     W[:, BX:BZ + 1] += rel * rng.uniform(-1, 1, (n, 3))
     return W
+
+
+def disk_generators(n_total: int, seed: int = 3, box=(6.0, 6.0, 1.5), frac_bg: float = 0.125):
+    """Generators of the Keplerian-disk workload in the periodic box
+    [-box/2, box/2) centred on the disk: a fraction 1 - frac_bg sampled with
+    surface density proportional to 1/r on 0.5 < r < 2 (so r is uniform) and
+    a Gaussian vertical profile of scale height H = 0.1 r, the rest a
+    jittered lattice padding the whole box.  Positions stay centred on the
+    origin because the isothermal EOS depends on |x| (the mesh and the fluid
+    path only use positions modulo the box)."""
+    rng = np.random.default_rng(seed)
+    box = np.asarray(box, dtype=np.float64)
+    n_bg = int(round(n_total * frac_bg))
+    # background lattice with the box's aspect ratio
+    nz = max(2, int(round((n_bg * box[2] ** 2 / (box[0] * box[1])) ** (1.0 / 3.0))))
+    nxy = max(2, int(round(np.sqrt(n_bg / nz))))
+    n_bg = nxy * nxy * nz
+    ix, iy, iz = np.meshgrid(np.arange(nxy), np.arange(nxy), np.arange(nz), indexing="ij")
+    h = box / np.array([nxy, nxy, nz])
+    bg = (np.stack([ix.ravel(), iy.ravel(), iz.ravel()], 1) + 0.5 + rng.uniform(-0.1, 0.1, (n_bg, 3))) * h - box / 2
+    n_d = n_total - n_bg
+    r = rng.uniform(0.5, 2.0, n_d)
+    phi = rng.uniform(0.0, 2 * np.pi, n_d)
+    z = np.clip(rng.normal(0.0, 0.1 * r), -0.45 * box[2], 0.45 * box[2])
+    disk = np.stack([r * np.cos(phi), r * np.sin(phi), z], 1)
+    pos = np.concatenate([disk, bg])
+    return np.mod(pos + box / 2, box) - box / 2, box
+
+
+def disk(pos: np.ndarray, box, GM: float = 1.0, cfac: float = 0.05, beta: float = 400.0,
+         rho_bg: float = 1e-3, noise: float = 0.01, seed: int = 4, r_sink: float = 0.3):
+    """Keplerian disk with a weak vertical field on generators from
+    disk_generators: rho = max(Sigma(r)/(sqrt(2 pi) H) exp(-z^2/2H^2), rho_bg)
+    with Sigma = 1/r, isothermal P = rho cs^2 with cs = cfac v_K(|x|),
+    v = v_K azimuthal inside 0.5 < r < 2 plus `noise` relative random
+    velocity, B_z with plasma beta = 2P/B^2.  Returns (W, bnd): cells
+    with |x| < r_sink are DIOD boundary cells (the reference's inner sink,
+    MPI/problems/mri_disk3d.cpp:762-765)."""
+    rng = np.random.default_rng(seed)
+    x = np.asarray(pos, dtype=np.float64)
+    R = np.hypot(x[:, 0], x[:, 1])
+    rr = np.linalg.norm(x, axis=1)
+    H = 0.1 * np.maximum(R, 0.5)
+    sigma = np.where((R > 0.5) & (R < 2.0), 1.0 / np.maximum(R, 1e-3), 0.0)
+    rho = np.maximum(sigma / (np.sqrt(2 * np.pi) * H) * np.exp(-0.5 * (x[:, 2] / H) ** 2), rho_bg)
+    cs2 = GM / np.maximum(rr, 1e-3) * cfac ** 2
+    pres = rho * cs2
+    vk = np.sqrt(GM / np.maximum(R, 0.3))
+    inside = (R > 0.5) & (R < 2.0)
+    n = x.shape[0]
+    W = np.zeros((n, NVAR))
+    W[:, DENS] = rho
+    W[:, VELX] = np.where(inside, -vk * x[:, 1] / np.maximum(R, 1e-9), 0.0)
+    W[:, VELY] = np.where(inside, vk * x[:, 0] / np.maximum(R, 1e-9), 0.0)
+    W[:, VELX:VELZ + 1] += noise * vk[:, None] * rng.uniform(-1, 1, (n, 3))
+    W[:, ETHM] = pres          # isothermal: ETHM = P (MPI/problems/mri_disk3d.cpp:377-380)
+    W[:, BZ] = np.sqrt(2.0 * pres / beta)
+    W[:, PSI] = 0.0
+    W[:, ENTR] = 1.0
+    bnd = np.where(rr < r_sink, 3, 0).astype(np.int32)  # DIOD
+    return W, bnd

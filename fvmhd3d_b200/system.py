@@ -134,6 +134,13 @@ class System:
 
     step = iterate_step
 
+    def run(self, nsteps, shared=True):
+        """nsteps steps replayed from a captured CUDA graph; returns
+        (active cells summed over the steps, active faces summed)."""
+        faces = ctypes.c_longlong(0)
+        cells = self._check(self.L.fvm_run(self.h, int(nsteps), int(bool(shared)), ctypes.byref(faces)), "fvm_run")
+        return cells, faces.value
+
     # -- outputs ----------------------------------------------------------
     @property
     def time(self) -> float:
@@ -202,6 +209,12 @@ class System:
     def stream_ptr(self) -> int:
         """The context's cudaStream_t as an integer (for torch.cuda.ExternalStream)."""
         return int(self.L.fvm_stream(self.h) or 0)
+
+    def active_face_count(self) -> int:
+        """Active faces of the last completed step (face-updates of that step)."""
+        nf = ctypes.c_int(0)
+        self._check(self.L.fvm_last_step_counts(self.h, None, ctypes.byref(nf)), "fvm_last_step_counts")
+        return nf.value
 
     @property
     def launch_count(self) -> int:

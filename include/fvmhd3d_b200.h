@@ -120,6 +120,12 @@ int fvm_end_step(fvm_ctx *c, int shared);
  * end_step.  Returns the number of active cells. */
 int fvm_step(fvm_ctx *c, int shared);
 
+/* nsteps full steps replayed from one captured CUDA graph (the scheduler
+ * runs on the device, so there is no host round trip between steps).
+ * Returns the summed number of active cells; faces_out (may be NULL)
+ * receives the summed number of active faces. */
+int fvm_run(fvm_ctx *c, int nsteps, int shared, long long *faces_out);
+
 /* ---- inspection ----------------------------------------------------------- */
 
 double fvm_time(const fvm_ctx *c);                       /* system::t_global */
@@ -149,6 +155,8 @@ float fvm_last_step_ms(const fvm_ctx *c);
 /* The context's CUDA stream (a cudaStream_t), for callers that order their
  * own work or events after the context's kernels. */
 void *fvm_stream(fvm_ctx *c);
+/* Active cells and active faces of the last completed step. */
+int fvm_last_step_counts(const fvm_ctx *c, int *ncell_active, int *nface_active);
 /* Number of kernels this context has launched so far. */
 long long fvm_launch_count(const fvm_ctx *c);
 /* Per-kernel CUDA-event timing: on != 0 enables it and clears the totals. */

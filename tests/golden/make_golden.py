@@ -47,6 +47,31 @@ def run_case(name, nside, problem, shared, nsteps, seed, noise=0.05):
     print(name, m.ncell, "cells", m.nface, "faces; active per step", nact)
 
 
+def disk_case(name, n, nsteps, seed=3):
+    """Keplerian disk, isothermal EOS, individual timesteps, with a DIOD sink."""
+    pos, box = F.problems.disk_generators(n, seed=seed)
+    m = F.build_periodic(pos, box)
+    W, bnd = F.problems.disk(pos, box, r_sink=0.55)
+    prm = dict(gamma=1.0, courant=0.4, box=tuple(box), dtmax=1.0 / 16, eos=1, iso_GM=1.0, iso_cfac=0.05)
+    R = RefSystem(**prm)
+    R.set_mesh(m)
+    R.init_problem(W, bnd=bnd)
+    out = dict(mesh_arrays(m), W=W, bnd=bnd, shared=np.int32(0), nsteps=np.int32(nsteps),
+               params=np.array([prm["gamma"], prm["courant"], box[0], box[1], box[2], prm["dtmax"], 1.0, 1.0, 0.05]))
+    nact, faces = [], []
+    for _ in range(nsteps):
+        s = R.step(shared=False, snap=True)
+        nact.append(s["nactive"])
+        faces.append(s["active_faces"])
+    st = R.get_state()
+    out.update({"out_" + k: v for k, v in st.items()})
+    out["out_time"] = np.float64(R.time)
+    out["out_nactive"] = np.array(nact, np.int32)
+    out["out_last_active_faces"] = faces[-1]
+    np.savez_compressed(os.path.join(HERE, name), **out)
+    print(name, m.ncell, "cells", m.nface, "faces,", int((bnd > 0).sum()), "DIOD cells; active per step", nact)
+
+
 def flux_case(name, nface=256, seed=5):
     rng = np.random.default_rng(seed)
     Wi = np.zeros((nface, 10))
@@ -78,4 +103,5 @@ if __name__ == "__main__":
     run_case("ref_blast7_individual.npz", 7, "blast", False, 14, seed=5, noise=0.2)
     run_case("ref_blast8_individual.npz", 8, "blast", False, 10, seed=12)
     run_case("ref_ot5_shared.npz", 5, "orszag_tang", True, 6, seed=13)
+    disk_case("ref_disk4k_individual.npz", 4096, 12)
     flux_case("ref_flux_kat.npz")

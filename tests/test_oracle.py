@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from common import GOLDEN_STEP_CASES, ORACLE_SO, REF_SO, load_golden, setup_case
+from common import GOLDEN_STEP_CASES, ORACLE_SO, REF_SO, golden_params, load_golden, setup_case
 from oracle.pyoracle import OracleSystem, RefSystem
 
 pytestmark = pytest.mark.skipif(not os.path.exists(ORACLE_SO), reason="oracle not built")
@@ -16,9 +16,9 @@ pytestmark = pytest.mark.skipif(not os.path.exists(ORACLE_SO), reason="oracle no
 @pytest.mark.parametrize("name", GOLDEN_STEP_CASES)
 def test_oracle_matches_golden_bitexact(name):
     m, z = load_golden(name)
-    o = OracleSystem()
+    o = OracleSystem(**golden_params(z))
     o.set_mesh(m)
-    o.init_problem(z["W"])
+    o.init_problem(z["W"], bnd=z.get("bnd"))
     nact = [o.step(shared=bool(z["shared"])) for _ in range(int(z["nsteps"]))]
     assert nact == list(z["out_nactive"])
     st = o.get_state()

@@ -24,6 +24,7 @@ class FvmParams(ctypes.Structure):
         ("iso_GM", c_double),
         ("iso_cfac", c_double),
         ("precision", c_int),
+        ("static_mesh", c_int),
     ]
 
 
@@ -36,6 +37,9 @@ SIGNATURES = {
     "fvm_init_problem": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "fvm_get_state": (c_int, [c_void_p] + [c_void_p] * 8),
     "fvm_set_state": (c_int, [c_void_p] + [c_void_p] * 7 + [c_ull]),
+    "fvm_get_motion": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fvm_clock": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fvm_dump_binary": (c_int, [c_void_p, ctypes.c_char_p, c_void_p, c_void_p]),
     "fvm_begin_step": (c_int, [c_void_p]),
     "fvm_slope_limiter": (c_int, [c_void_p]),
     "fvm_compute_update": (c_int, [c_void_p]),

@@ -16,6 +16,8 @@
 #include "../../include/fvmhd3d_b200.h"
 
 #include <cuda_runtime.h>
+#include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <cstdlib>
@@ -34,9 +36,13 @@ using namespace fvm;
 #ifndef FVM_FLUX_MINB_F
 #define FVM_FLUX_MINB_F 4
 #endif
-#ifndef FVM_CELL_MINB
-#define FVM_CELL_MINB 1
+#ifndef FVM_CELL_MINB_D
+#define FVM_CELL_MINB_D 4
 #endif
+#ifndef FVM_CELL_MINB_F
+#define FVM_CELL_MINB_F 6
+#endif
+#define FVM_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CELL_MINB_F : FVM_CELL_MINB_D)
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
 // cell-kernel mappings: grouped (16 lanes per cell) or two threads per cell
 #ifndef FVM_CELLMAP_GROUPED
@@ -68,6 +74,7 @@ struct Sched {
   int iscal[8];  // [0] rung maximum, [1] active cells, [2] error flags, [3] active faces,
                  // [4] dirty sites of adjust_timesteps, [5] active non-boundary sites
   unsigned long long nactive_total, nfaces_total, steps;
+  unsigned long long tprevU;  // tsysU before the last pull_active_list
 };
 
 struct Dev {
@@ -80,6 +87,8 @@ struct Dev {
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
   // state
   double *pos, *vel, *tlast, *tend, *volp;
+  double *opos, *ovel;  // orig_pos / orig_vel of correct() (generator motion)
+  float *divb;          // divBi of collect_results (float, as the reference keeps it)
   int *rung, *bnd;
   double *U, *dU;
   void *Wrec;  // bulk type (double or float), ncell x 50
@@ -200,7 +209,7 @@ __device__ __forceinline__ void wrap3(const Params &P, double *d) {
 constexpr int KH = 5;  // primitives per thread in the two-threads-per-cell kernels
 
 template <typename R>
-__global__ void __launch_bounds__(128, FVM_CELL_MINB) k_limiter(int n, Params P, const Sched *__restrict__ S,
+__global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params P, const Sched *__restrict__ S,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
@@ -700,7 +709,7 @@ __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched 
     const R *__restrict__ Wrec, const R *__restrict__ tau,
     const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
     double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
-    unsigned long long *__restrict__ counters, const int *__restrict__ perm) {
+    unsigned long long *__restrict__ counters, const int *__restrict__ perm, float *__restrict__ divb) {
   const double t_global = S->t_global;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= n) return;
@@ -743,6 +752,7 @@ __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched 
   const double divB = d0[13] + s[13];
   const double dPsi[3] = {d0[10] + s[10], d0[11] + s[11], d0[12] + s[12]};
   const double dt = t_global - tlast[c];
+  divb[c] = float(dt > 0.0 ? divB / dt / V : divB);  // divBi (MPI/distribute_work.cpp:681)
 #pragma unroll
   for (int k = 0; k < 14; k++) d0[k] = 0.0;  // dU_local = 0 (collect_results)
   if (stepdU) {
@@ -806,7 +816,7 @@ __global__ void __launch_bounds__(256) k_corr_cell_g(int n, Params P, const Sche
     const R *__restrict__ Wrec, const R *__restrict__ tau,
     const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
     double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
-    unsigned long long *__restrict__ counters) {
+    unsigned long long *__restrict__ counters, float *__restrict__ divb) {
   const double t_global = S->t_global;
   const int c = blockIdx.x * (256 / GL) + threadIdx.x / GL, l = threadIdx.x % GL;
   const unsigned char ac = c < n ? act[c] : 0;
@@ -848,6 +858,7 @@ __global__ void __launch_bounds__(256) k_corr_cell_g(int n, Params P, const Sche
   const double divB = d0[13] + s[13];
   const double dPsi[3] = {d0[10] + s[10], d0[11] + s[11], d0[12] + s[12]};
   const double dt = t_global - tlast[c];
+  divb[c] = float(dt > 0.0 ? divB / dt / V : divB);  // divBi (MPI/distribute_work.cpp:681)
 #pragma unroll
   for (int k = 0; k < 14; k++) d0[k] = 0.0;  // dU_local = 0 (collect_results)
   if (stepdU) {
@@ -910,6 +921,11 @@ __global__ void k_pvel(int n, Params P, const unsigned char *__restrict__ act, c
                        const double *__restrict__ pos, double *__restrict__ vel) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n || !(act[i] & A_ACTIVE)) return;
+  if (P.static_mesh) {  // compute_pvel1 hook returning true (MPI/set_problem.cpp:61-72)
+    double *vo = vel + 3 * (size_t)i;
+    vo[0] = vo[1] = vo[2] = 0.0;
+    return;
+  }
   double W[NF];
   to_primitive(U + 10 * (size_t)i, volp[i], W);
   double v[3] = {W[VELX], W[VELY], W[VELZ]};
@@ -1143,7 +1159,8 @@ __global__ void k_rungs(int n, Params P, const Sched *__restrict__ S, int shared
                         const unsigned char *__restrict__ act, const unsigned char *__restrict__ hash,
                         const double *__restrict__ dtl, const double *__restrict__ dmin,
                         int *__restrict__ rung, double *__restrict__ tlast, double *__restrict__ tend,
-                        R *__restrict__ Wrec, int *__restrict__ iscal) {
+                        R *__restrict__ Wrec, int *__restrict__ iscal, const double *__restrict__ vel,
+                        double *__restrict__ opos, double *__restrict__ ovel) {
   const double t_global = S->t_global;
   const int min_rung = S->min_rung;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1153,6 +1170,14 @@ __global__ void k_rungs(int n, Params P, const Sched *__restrict__ S, int shared
   if (a & A_ACTIVE) {
     const int r = shared ? get_rung(P, dmin[0], min_rung) : get_rung(P, fabs(dtl[i]), min_rung);
     rung[i] = r;
+    // correct() (MPI/set_problem.cpp:89-101): generator motion over the step
+    const double dth = 0.5 * (t_global - tlast[i]);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      const double v = vel[3 * (size_t)i + a];
+      opos[3 * (size_t)i + a] = opos[3 * (size_t)i + a] + (v + ovel[3 * (size_t)i + a]) * dth;
+      ovel[3 * (size_t)i + a] = v;
+    }
     tlast[i] = t_global;
     tend[i] = t_global + get_dt(P, r);
     if (r < 0 || r >= RUNGMAX) atomicOr(&iscal[2], 1);
@@ -1374,7 +1399,7 @@ __global__ void __launch_bounds__(256) k_pred_cell_g(int n, Params P, const Sche
 // Two threads per active cell, five primitives each: Voronoi face gradient of
 // the updated primitives, local limiter, density positivity rescale.
 template <typename R>
-__global__ void __launch_bounds__(128, FVM_CELL_MINB) k_recon(int n, Params P,
+__global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
@@ -1501,6 +1526,7 @@ __global__ void k_sched_begin(Params P, Sched *S) {
   S->max_rung = max_rung;
   S->min_rung = min_rung;
   S->flags = flags;
+  S->tprevU = S->tsysU;
   S->tsysU = tnextU;
   S->t_global = P.dt_tick * (double)tnextU;
   S->dtmin = FVM_HUGE;
@@ -1516,7 +1542,7 @@ __global__ void k_sched_end(Sched *S) {
 }
 
 __global__ void k_sched_set(Params P, Sched *S, unsigned long long tsysU, int reset_err) {
-  S->tsysU = tsysU;
+  S->tsysU = S->tprevU = tsysU;
   S->t_global = P.dt_tick * (double)tsysU;
   if (reset_err) {
     S->min_rung = 0;
@@ -1749,6 +1775,7 @@ fvm_ctx *fvm_create(const fvm_params *p, int device) {
   c->P.eos = p->eos;
   c->P.iso_GM = p->iso_GM;
   c->P.iso_cfac = p->iso_cfac;
+  c->P.static_mesh = p->static_mesh ? 1 : 0;
   c->tsysU = 0;
   c->min_rung = 0;
   c->max_rung = RUNGMAX - 1;
@@ -1815,6 +1842,8 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
   if ((ncell + CB - 1) / CB > CB * 16) { c->err = "fvm_set_mesh: more than 16M cells"; return FVM_ERANGE; }
   rc |= dalloc(c, &d.pos, 3 * (size_t)ncell); rc |= dalloc(c, &d.vel, 3 * (size_t)ncell);
+  rc |= dalloc(c, &d.opos, 3 * (size_t)ncell); rc |= dalloc(c, &d.ovel, 3 * (size_t)ncell);
+  rc |= dalloc(c, &d.divb, ncell);
   rc |= dalloc(c, &d.tlast, ncell); rc |= dalloc(c, &d.tend, ncell); rc |= dalloc(c, &d.volp, ncell);
   rc |= dalloc(c, &d.rung, ncell); rc |= dalloc(c, &d.bnd, ncell);
   rc |= dalloc(c, &d.U, 10 * (size_t)ncell); rc |= dalloc(c, &d.dU, 14 * (size_t)ncell);
@@ -1912,6 +1941,9 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   CK(cudaMemsetAsync(d.act, A_ACTIVE, n, c->st));
   k_pvel<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel);
   LAUNCH_CHECK();
+  CK(cudaMemcpyAsync(d.opos, d.pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemcpyAsync(d.ovel, d.vel, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaMemsetAsync(d.divb, 0, sizeof(float) * n, c->st));
   Sched h0;
   memset(&h0, 0, sizeof(h0));
   h0.dtmin = FVM_HUGE;
@@ -2049,12 +2081,12 @@ static int enq_update(fvm_ctx *c) {
   BULK(k_corr_cell_g<R><<<nblk(c->n, 256 / GL), 256, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
                                                           (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
-                                                          d.stepdU, d.counters));
+                                                          d.stepdU, d.counters, d.divb));
 #else
   BULK(k_corr_cell<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
                                                           (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
-                                                          d.stepdU, d.counters, d.perm));
+                                                          d.stepdU, d.counters, d.perm, d.divb));
 #endif
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_CELL);
@@ -2098,7 +2130,8 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
   kt_end(c, KT_TIMESTEP);
   kt_begin(c, KT_RUNGS);
   BULK(k_rungs<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.S, shared, d.act, d.hash, d.dtl, &d.S->dtmin, d.rung,
-                                                   d.tlast, d.tend, (R *)d.Wrec, d.S->iscal));
+                                                   d.tlast, d.tend, (R *)d.Wrec, d.S->iscal, d.vel, d.opos,
+                                                   d.ovel));
   LAUNCH_CHECK();
   kt_end(c, KT_RUNGS);
   return 0;
@@ -2297,6 +2330,106 @@ double fvm_time(const fvm_ctx *c) { return c ? c->t_global : 0.0; }
 
 void *fvm_stream(fvm_ctx *c) { return c ? (void *)c->st : nullptr; }
 
+int fvm_get_motion(fvm_ctx *c, double *orig_pos, double *orig_vel, float *divb) {
+  if (!c || !c->have_mesh) return FVM_ENOMESH;
+  CK(cudaSetDevice(c->device));
+  const size_t n = c->n;
+  if (orig_pos) CK(cudaMemcpyAsync(orig_pos, c->d.opos, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (orig_vel) CK(cudaMemcpyAsync(orig_vel, c->d.ovel, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  if (divb) CK(cudaMemcpyAsync(divb, c->d.divb, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int fvm_clock(fvm_ctx *c, unsigned long long *tsys_ticks, double *dt_global, long long *iteration) {
+  if (!c || !c->have_state) return FVM_ENOMESH;
+  if (c->in_step) { c->err = "fvm_clock: inside a step"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  const int rc = read_sched(c);
+  if (rc) return rc;
+  if (tsys_ticks) *tsys_ticks = c->hS.tsysU;
+  if (dt_global) *dt_global = c->P.dt_tick * (double)(c->hS.tsysU - c->hS.tprevU);
+  if (iteration) *iteration = (long long)c->hS.steps;
+  return 0;
+}
+
+// system::dump_binary (MPI/dump_binary.cpp:5-99) for one rank.  The state is
+// brought to the host and converted there with the same to_primitive and
+// pressure as the device path, in double precision, then rounded to float as
+// the reference's fdump does.
+int fvm_dump_binary(fvm_ctx *c, const char *path, const int *idx, const float *rmax) {
+  if (!c || !path) return FVM_EINVAL;
+  if (!c->have_state) { c->err = "fvm_dump_binary: no state"; return FVM_ENOMESH; }
+  if (c->in_step) { c->err = "fvm_dump_binary: inside a step"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  const size_t n = c->n;
+  std::vector<double> U(10 * n), opos(3 * n), ovel(3 * n), vol(n);
+  std::vector<float> divb(n);
+  std::vector<int> rung(n), bnd(n);
+  CK(cudaMemcpyAsync(U.data(), c->d.U, U.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(opos.data(), c->d.opos, opos.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(ovel.data(), c->d.ovel, ovel.size() * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(vol.data(), c->d.cvol, n * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(divb.data(), c->d.divb, n * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(rung.data(), c->d.rung, n * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(bnd.data(), c->d.bnd, n * sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  const int rc = read_sched(c);  // synchronises the stream
+  if (rc) return rc;
+
+  std::vector<uint32_t> w;
+  w.reserve(22 + 28 * n);
+  auto iw = [&](int v) { uint32_t u; memcpy(&u, &v, 4); w.push_back(u); };
+  auto fw = [&](double v) { const float f = (float)v; uint32_t u; memcpy(&u, &f, 4); w.push_back(u); };
+  const Sched &S = c->hS;
+  iw(20 * 4);
+  iw(0);  // myproc
+  iw(1);  // nproc
+  iw(1);  // nproc
+  w.push_back((uint32_t)(S.tsysU & 0xffffffffULL));
+  w.push_back((uint32_t)(S.tsysU >> 32));
+  iw(c->n);  // global_n
+  iw(c->n);  // local_n
+  iw(3);
+  fw(S.t_global);
+  fw(c->P.dt_tick * (double)(S.tsysU - S.tprevU));  // dt_global
+  iw((int)S.steps);                                   // iteration
+  fw(c->P.courant);
+  fw(c->P.gamma);
+  iw(-1);
+  for (int a = 0; a < 3; a++) fw(0.0);  // periodic domain [0, box)
+  for (int a = 0; a < 3; a++) fw(c->P.box[a]);
+  iw(20 * 4);
+  for (size_t i = 0; i < n; i++) {
+    double W[10];
+    to_primitive<double>(&U[10 * i], vol[i], W);
+    const double L = std::pow(vol[i] * 3.0 / 4.0 / M_PI, 1.0 / 3.0);
+    iw(26 * 4);
+    iw(idx ? idx[i] : (int)i);
+    for (int a = 0; a < 3; a++) fw(opos[3 * i + a]);
+    for (int a = 0; a < 3; a++) fw(ovel[3 * i + a]);
+    fw(W[DENS]);
+    fw(W[ETHM]);
+    fw(pressure<double>(c->P, W));
+    fw(rmax ? (double)rmax[i] : 0.0);
+    iw(bnd[i]);
+    fw(W[VELX]); fw(W[VELY]); fw(W[VELZ]);
+    fw(W[BX]); fw(W[BY]); fw(W[BZ]);
+    fw(get_dt(c->P, rung[i]));
+    fw(vol[i]);
+    fw(W[PSI]);
+    fw(L * (double)divb[i]);
+    fw(W[ENTR]);
+    fw(0.0); fw(0.0); fw(0.0);  // J
+    iw(26 * 4);
+  }
+  FILE *f = fopen(path, "wb");
+  if (!f) { c->err = std::string("fvm_dump_binary: cannot open ") + path; return FVM_EIO; }
+  const size_t put = fwrite(w.data(), sizeof(uint32_t), w.size(), f);
+  const int cl = fclose(f);
+  if (put != w.size() || cl != 0) { c->err = std::string("fvm_dump_binary: short write to ") + path; return FVM_EIO; }
+  return 0;
+}
+
 int fvm_last_step_counts(const fvm_ctx *c, int *ncell_active, int *nface_active) {
   if (!c) return FVM_EINVAL;
   if (ncell_active) *ncell_active = c->hS.iscal[1];
@@ -2414,3 +2547,4 @@ int fvm_compute_flux(fvm_ctx *c, int nface, const double *wij, const double *Wi,
 }
 
 }  // extern "C"
+

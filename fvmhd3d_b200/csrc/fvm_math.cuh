@@ -25,6 +25,7 @@ struct Params {
   double dtmax, dt_tick;
   int eos;              // 0 ideal gas, 1 isothermal disk
   double iso_GM, iso_cfac;
+  int static_mesh;      // 1: compute_pvel1 hook with vel = 0 (static generators)
 };
 
 template <typename T> __host__ __device__ __forceinline__ T sqr(T x) { return x * x; }
@@ -54,7 +55,7 @@ __host__ __device__ __forceinline__ int get_rung(const Params &P, double dt, int
 // ---- EOS hooks (ideal gas MPI/set_problem.cpp:123-137; isothermal disk
 //      MPI/problems/mri_disk3d.cpp:368-389) ------------------------------
 template <typename T>
-__device__ __forceinline__ T pressure(const Params &P, const T *W) {
+__host__ __device__ __forceinline__ T pressure(const Params &P, const T *W) {
   if (P.eos == 0) return P.gamma > 1.0 ? T(P.gamma - 1.0) * W[ETHM] : W[ETHM];
   return W[ETHM];
 }
@@ -76,7 +77,7 @@ __device__ __forceinline__ double ethm_update(const Params &P, const double *W, 
 
 // ---- prim <-> cons (MPI/Fluid.h:55-129) ----------------------------------
 template <typename T>
-__device__ __forceinline__ void to_primitive(const T *U, T V, T *W) {
+__host__ __device__ __forceinline__ void to_primitive(const T *U, T V, T *W) {
   const T iM = T(1.0) / U[MASS];
   const T iV = T(1.0) / V;
   W[DENS] = U[MASS] * iV;

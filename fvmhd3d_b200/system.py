@@ -16,6 +16,7 @@ a failed ``assert``).
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 
@@ -38,7 +39,7 @@ class System:
     """One context on one CUDA device (one rank of the reference)."""
 
     def __init__(self, gamma=5.0 / 3.0, courant=0.4, box=(1.0, 1.0, 1.0), dtmax=1.0 / 64, eos=0,
-                 iso_GM=1.0, iso_cfac=0.05, precision=FVM_PREC_FP64, device=0):
+                 iso_GM=1.0, iso_cfac=0.05, precision=FVM_PREC_FP64, device=0, static_mesh=False):
         self.L = _lib.lib()
         prm = _lib.FvmParams()
         prm.gamma, prm.courant = gamma, courant
@@ -46,6 +47,7 @@ class System:
         for a in range(3):
             prm.box[a] = float(box[a])
         prm.dtmax, prm.eos, prm.iso_GM, prm.iso_cfac, prm.precision = dtmax, eos, iso_GM, iso_cfac, precision
+        prm.static_mesh = 1 if static_mesh else 0
         self.params = prm
         h = self.L.fvm_create(ctypes.byref(prm), int(device))
         if not h:
@@ -158,6 +160,37 @@ class System:
                                                    ("pos", "vel", "tlast", "tend", "rung", "U", "dU", "wrec")]),
                     "fvm_get_state")
         return st
+
+    def get_motion(self) -> dict:
+        """orig_pos, orig_vel (the reference's correct()) and divBi (float32)."""
+        n = self.mesh.ncell
+        out = dict(orig_pos=np.zeros((n, 3)), orig_vel=np.zeros((n, 3)), divb=np.zeros(n, np.float32))
+        self._check(self.L.fvm_get_motion(self.h, _p(out["orig_pos"]), _p(out["orig_vel"]), _p(out["divb"])),
+                    "fvm_get_motion")
+        return out
+
+    def clock(self):
+        """(tsysU, dt_global, iteration): the scheduler clock after the last
+        step (the reference's Scheduler::tsysU, system::dt_global and
+        system::iteration)."""
+        t = ctypes.c_ulonglong(0)
+        dt = ctypes.c_double(0.0)
+        it = ctypes.c_longlong(0)
+        self._check(self.L.fvm_clock(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(it)), "fvm_clock")
+        return t.value, dt.value, it.value
+
+    def dump_binary(self, path, idx=None, rmax=None) -> None:
+        """Writes the current state as the reference's snapshot file
+        (system::dump_binary, MPI/dump_binary.cpp); read it back with
+        :func:`fvmhd3d_b200.snapshot.read_binary`.  idx (int32 particle ids)
+        and rmax (float32 mesh search radii) default to the cell index and 0."""
+        n = self.mesh.ncell
+        i = None if idx is None else np.ascontiguousarray(idx, np.int32)
+        r = None if rmax is None else np.ascontiguousarray(rmax, np.float32)
+        for a in (i, r):
+            if a is not None and a.shape != (n,):
+                raise ValueError(f"expected {n} entries, got {a.shape}")
+        self._check(self.L.fvm_dump_binary(self.h, os.fsencode(path), _p(i), _p(r)), "fvm_dump_binary")
 
     def set_state(self, vel=None, tlast=None, tend=None, rung=None, U=None, dU=None, wrec=None, tsys_ticks=0):
         conv = [None if a is None else np.ascontiguousarray(a, t) for a, t in

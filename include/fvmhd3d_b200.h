@@ -38,7 +38,8 @@ enum {
   FVM_ECUDA = -2,     /* CUDA runtime error */
   FVM_ENOMEM = -3,    /* device allocation failed */
   FVM_ENOMESH = -4,   /* no mesh / state installed yet */
-  FVM_ERANGE = -5     /* a rung left [0, 32) or a size limit was exceeded */
+  FVM_ERANGE = -5,    /* a rung left [0, 32) or a size limit was exceeded */
+  FVM_EIO = -6        /* a snapshot file could not be written */
 };
 
 enum { FVM_PREC_FP64 = 0, FVM_PREC_FP32 = 1 };
@@ -53,6 +54,10 @@ typedef struct fvm_params {
   double iso_GM;    /* disk: cs^2(r) = iso_GM/|r| * iso_cfac^2 */
   double iso_cfac;
   int precision;    /* FVM_PREC_FP64 (plain path) or FVM_PREC_FP32 */
+  int static_mesh;  /* 0: compute_pvel moves generators with the flow
+                       (MPI/compute_pvel.cpp:5-50); 1: static generators, the
+                       compute_pvel1 hook that sets vel = 0 for every active
+                       site (MPI/set_problem.cpp:61-72, acoustic_waves.cpp:6-16) */
 } fvm_params;
 
 typedef struct fvm_ctx fvm_ctx;
@@ -85,6 +90,29 @@ int fvm_get_state(fvm_ctx *c, double *pos, double *vel, double *tlast, double *t
 int fvm_set_state(fvm_ctx *c, const double *vel, const double *tlast, const double *tend,
                   const int *rung, const double *U, const double *dU, const double *wrec,
                   unsigned long long tsys_ticks);
+
+/* Generator motion and divergence diagnostics between steps (any pointer may
+ * be NULL): orig_pos / orig_vel as advanced by the reference's correct()
+ * (MPI/set_problem.cpp:89-101) and divBi, the per-cell divB/dt/V that
+ * collect_results keeps in single precision (MPI/distribute_work.cpp:681).
+ * These feed the host's next mesh build and the snapshot writer. */
+int fvm_get_motion(fvm_ctx *c, double *orig_pos, double *orig_vel, float *divb);
+
+/* The scheduler clock: Scheduler::tsysU, system::dt_global (the interval the
+ * last Scheduler::pull_active_list advanced, MPI/Scheduler.h:138-153) and
+ * system::iteration (steps since fvm_init_problem, MPI/iterate.cpp:117).
+ * Any pointer may be NULL. */
+int fvm_clock(fvm_ctx *c, unsigned long long *tsys_ticks, double *dt_global, long long *iteration);
+
+/* Writes the reference's single-rank snapshot, system::dump_binary
+ * (MPI/dump_binary.cpp:5-99), byte for byte in its layout: a 20-word header
+ * and one 26-word record per cell, each framed by its byte count, native
+ * little-endian int32/float32.  idx (particle ids) and rmax (the mesh
+ * builder's search radius) are host data the fluid path does not hold: NULL
+ * writes idx = cell index and rmax = 0.  Cell volumes are the installed mesh's;
+ * the current-density words are 0 (the hot path computes no J).  Returns
+ * FVM_EIO if the file cannot be written. */
+int fvm_dump_binary(fvm_ctx *c, const char *path, const int *idx, const float *rmax);
 
 /* ---- the reference's step, one entry point per member function ---------- */
 

@@ -49,13 +49,16 @@ struct fvo_ctx {
   int *ids;
   /* scheduler (MPI/Scheduler.h:4-30) */
   double dt_tick;
-  unsigned long long tsysU;
+  unsigned long long tsysU, tprevU;
+  long long iteration;  /* system::iteration (MPI/iterate.cpp:117) */
   int min_rung, max_rung;
   double t_global;
   /* state */
   double *pos, *vel, *tlast, *tend, *volume;
   int *rung, *bnd;
   double *U, *dU, *Wrec;
+  double *opos, *ovel;  /* orig_pos, orig_vel (correct(), MPI/set_problem.cpp:89-101) */
+  float *divb;          /* divBi (MPI/distribute_work.cpp:681) */
   /* per-step work */
   unsigned char *active, *lngb, *hasngb;
   int *alist, nactive;
@@ -364,6 +367,7 @@ static void free_state(fvo_ctx *c) {
   free(c->pos); free(c->vel); free(c->tlast); free(c->tend); free(c->volume);
   free(c->rung); free(c->bnd); free(c->U); free(c->dU); free(c->Wrec);
   free(c->active); free(c->lngb); free(c->hasngb); free(c->alist); free(c->flist);
+  free(c->opos); free(c->ovel); free(c->divb);
 }
 
 void fvo_destroy(fvo_ctx *c) {
@@ -406,6 +410,9 @@ int fvo_set_mesh(fvo_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   c->U = (double *)calloc(10 * n, sizeof(double));
   c->dU = (double *)calloc(14 * n, sizeof(double));
   c->Wrec = (double *)calloc(50 * n, sizeof(double));
+  c->opos = (double *)calloc(3 * n, sizeof(double));
+  c->ovel = (double *)calloc(3 * n, sizeof(double));
+  c->divb = (float *)calloc(n, sizeof(float));
   c->active = (unsigned char *)calloc(n, 1);
   c->lngb = (unsigned char *)calloc(n, 1);
   c->hasngb = (unsigned char *)calloc(n, 1);
@@ -414,8 +421,14 @@ int fvo_set_mesh(fvo_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   return 0;
 }
 
-/* compute_pvel (MPI/compute_pvel.cpp:5-52) for the cells in alist */
+/* compute_pvel (MPI/compute_pvel.cpp:5-52) for the cells in alist; with
+ * static_mesh the compute_pvel1 hook that zeroes the velocity of every active
+ * site and returns true (MPI/set_problem.cpp:61-72). */
 static void compute_pvel(fvo_ctx *c) {
+  if (c->p.static_mesh) {
+    for (int a = 0; a < c->nactive; a++) memset(CELL3(c->vel, c->alist[a]), 0, 3 * sizeof(double));
+    return;
+  }
   for (int a = 0; a < c->nactive; a++) {
     const int i = c->alist[a];
     double W[NF];
@@ -512,12 +525,32 @@ int fvo_init_problem(fvo_ctx *c, const double *W, const double *pos, const int *
   for (int i = 0; i < n; i++) {
     c->rung[i] = rung + rung_offset;
     c->tend[i] = 0.0 + get_dt(c, c->rung[i]);
+    memcpy(CELL3(c->opos, i), CELL3(c->pos, i), 3 * sizeof(double));
+    memcpy(CELL3(c->ovel, i), CELL3(c->vel, i), 3 * sizeof(double));
+    c->divb[i] = 0.0f;
   }
   c->t_global = 0.0;
   return 0;
 }
 
 double fvo_time(const fvo_ctx *c) { return c->t_global; }
+
+/* Scheduler::tsysU, the dt_global that pull_active_list returned
+ * (MPI/Scheduler.h:138,153) and system::iteration. */
+int fvo_clock(const fvo_ctx *c, unsigned long long *tsys, double *dt_global, long long *iteration) {
+  if (tsys) *tsys = c->tsysU;
+  if (dt_global) *dt_global = c->dt_tick * (double)(c->tsysU - c->tprevU);
+  if (iteration) *iteration = c->iteration;
+  return 0;
+}
+
+int fvo_get_motion(const fvo_ctx *c, double *opos, double *ovel, float *divb) {
+  const size_t n = c->ncell;
+  if (opos) memcpy(opos, c->opos, 3 * n * sizeof(double));
+  if (ovel) memcpy(ovel, c->ovel, 3 * n * sizeof(double));
+  if (divb) memcpy(divb, c->divb, n * sizeof(float));
+  return 0;
+}
 
 int fvo_get_state(const fvo_ctx *c, double *pos, double *vel, double *tlast, double *tend, int *rung,
                   double *U, double *dU, double *wrec) {
@@ -544,7 +577,7 @@ int fvo_set_state(fvo_ctx *c, const double *vel, const double *tlast, const doub
   if (U) memcpy(c->U, U, 10 * n * sizeof(double));
   if (dU) memcpy(c->dU, dU, 14 * n * sizeof(double));
   if (wrec) memcpy(c->Wrec, wrec, 50 * n * sizeof(double));
-  c->tsysU = tsys_ticks;
+  c->tsysU = c->tprevU = tsys_ticks;
   c->t_global = c->dt_tick * (double)tsys_ticks;
   return 0;
 }
@@ -567,7 +600,9 @@ int fvo_step(fvo_ctx *c, int shared, fvo_snap *snap) {
   const unsigned long long flags = c->tsysU ^ tnextU;
   for (int b = 0; b < RUNGMAX; b++)
     if (flags & (1ULL << b)) c->min_rung = RUNGMAX - 1 - b;
+  c->tprevU = c->tsysU;
   c->tsysU = tnextU;
+  c->iteration++;
   c->t_global = c->dt_tick * (double)c->tsysU;
   const double t_global = c->t_global;
 
@@ -897,7 +932,14 @@ int fvo_step(fvo_ctx *c, int shared, fvo_snap *snap) {
         c->volume[i] = voli[i];
         memcpy(CELL3(c->vel, i), CELL3(veli, i), 3 * sizeof(double));
         c->tend[i] = tendi[i];
+        c->divb[i] = (float)dUi[14 * (size_t)i + 13];
         /* correct(i), MPI/set_problem.cpp:89-101 */
+        {
+          const double dth = 0.5 * (t_global - c->tlast[i]);
+          double *op = CELL3(c->opos, i), *ov = CELL3(c->ovel, i);
+          const double *v = CELL3(c->vel, i);
+          for (int a = 0; a < 3; a++) { op[a] = op[a] + (v[a] + ov[a]) * dth; ov[a] = v[a]; }
+        }
         c->tlast[i] = c->dt_tick * (double)c->tsysU;
         c->tend[i] = c->dt_tick * (double)c->tsysU + get_dt(c, c->rung[i]);
       } else if (!(c->tlast[i] == t_global)) {

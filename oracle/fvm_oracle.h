@@ -25,6 +25,7 @@ typedef struct fvo_params {
   double dtmax;
   int eos;                 /* 0 ideal gas, 1 isothermal disk */
   double iso_GM, iso_cfac; /* disk: cs^2 = GM/|r| * cfac^2 */
+  int static_mesh;         /* 1: compute_pvel1 hook with vel = 0 (MPI/set_problem.cpp:61-72) */
 } fvo_params;
 
 /* snapshots between stages of one step (any pointer may be NULL) */
@@ -52,6 +53,8 @@ int fvo_set_mesh(fvo_ctx *c, int ncell, int nface, const int *s1, const int *s2,
 int fvo_init_problem(fvo_ctx *c, const double *W, const double *pos, const int *bnd, int rung_offset);
 int fvo_step(fvo_ctx *c, int shared, fvo_snap *snap);
 double fvo_time(const fvo_ctx *c);
+int fvo_clock(const fvo_ctx *c, unsigned long long *tsys, double *dt_global, long long *iteration);
+int fvo_get_motion(const fvo_ctx *c, double *opos, double *ovel, float *divb);
 int fvo_get_state(const fvo_ctx *c, double *pos, double *vel, double *tlast, double *tend,
                   int *rung, double *U, double *dU, double *wrec);
 int fvo_set_state(fvo_ctx *c, const double *vel, const double *tlast, const double *tend,

@@ -13,7 +13,9 @@ baseline leg of ``bench.py`` may use this module.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
+import struct
 import subprocess
 
 import numpy as np
@@ -41,6 +43,7 @@ class _Params(ctypes.Structure):
         ("eos", ctypes.c_int),
         ("iso_GM", ctypes.c_double),
         ("iso_cfac", ctypes.c_double),
+        ("static_mesh", ctypes.c_int),
     ]
 
 
@@ -67,13 +70,31 @@ def _p(a):
     return ctypes.c_void_p(a.ctypes.data) if a is not None else None
 
 
+def _to_primitive(U, V):
+    """FluidBase::to_primitive (MPI/Fluid.h:55-92) in double precision, the
+    reference's operation order."""
+    U = [float(u) for u in U]
+    iM = 1.0 / U[0]
+    iV = 1.0 / V
+    W = [0.0] * 10
+    W[0] = U[0] * iV
+    W[1], W[2], W[3] = U[1] * iM, U[2] * iM, U[3] * iM
+    W[5], W[6], W[7] = U[5] * iV, U[6] * iV, U[7] * iV
+    W[8] = U[8] * iM
+    W[9] = U[9] * iM
+    W[4] = (U[4] * iV - 0.5 * (W[5] * W[5] + W[6] * W[6] + W[7] * W[7])
+            - 0.5 * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]) * W[0])
+    return W
+
+
 def make_params(gamma=5.0 / 3.0, courant=0.4, box=(1.0, 1.0, 1.0), dtmax=1.0 / 64, eos=0,
-                iso_GM=1.0, iso_cfac=0.05) -> _Params:
+                iso_GM=1.0, iso_cfac=0.05, static_mesh=False) -> _Params:
     p = _Params()
     p.gamma, p.courant = gamma, courant
     for a in range(3):
         p.box[a] = box[a]
     p.dtmax, p.eos, p.iso_GM, p.iso_cfac = dtmax, eos, iso_GM, iso_cfac
+    p.static_mesh = 1 if static_mesh else 0
     return p
 
 
@@ -165,6 +186,12 @@ class _Base:
         self._fn("get_state")(self.h, *[_p(st[k]) for k in ("pos", "vel", "tlast", "tend", "rung", "U", "dU", "wrec")])
         return st
 
+    def get_motion(self):
+        n = self.mesh.ncell
+        out = dict(orig_pos=np.zeros((n, 3)), orig_vel=np.zeros((n, 3)), divb=np.zeros(n, np.float32))
+        self._fn("get_motion")(self.h, _p(out["orig_pos"]), _p(out["orig_vel"]), _p(out["divb"]))
+        return out
+
     def compute_flux(self, wij, Wi, Wj, jbnd, normal):
         nf = Wi.shape[0]
         wij, Wi, Wj, normal = (np.ascontiguousarray(a, np.float64) for a in (wij, Wi, Wj, normal))
@@ -181,12 +208,57 @@ class RefSystem(_Base):
     so = REF_SO
     off_dtype = np.int32
 
+    def dump_binary(self, path):
+        """The reference's own snapshot writer (MPI/dump_binary.cpp)."""
+        self._fn("dump_binary")(self.h, ctypes.c_char_p(str(path).encode()))
+
+    @property
+    def tsys_ticks(self):
+        f = self._fn("tsys_ticks")
+        f.restype = ctypes.c_ulonglong
+        return int(f(self.h))
+
 
 class OracleSystem(_Base):
     """The plain-C restatement."""
     prefix = "fvo_"
     so = ORACLE_SO
     off_dtype = np.int64
+
+    def clock(self):
+        """(tsysU, dt_global, iteration) after the last step."""
+        t = ctypes.c_ulonglong(0)
+        dt = ctypes.c_double(0.0)
+        it = ctypes.c_longlong(0)
+        self._fn("clock")(self.h, ctypes.byref(t), ctypes.byref(dt), ctypes.byref(it))
+        return t.value, dt.value, it.value
+
+    def dump_binary_bytes(self, bnd=None, idx=None, rmax=None):
+        """Restatement of system::dump_binary (MPI/dump_binary.cpp:5-99) for
+        one rank over this oracle's state: returns the file's bytes."""
+        p = self.params
+        n = self.mesh.ncell
+        st = self.get_state()
+        mo = self.get_motion()
+        tsys, dt_global, iteration = self.clock()
+        vol = np.asarray(self.mesh.volume, np.float64)
+        bnd = np.zeros(n, np.int32) if bnd is None else np.asarray(bnd, np.int32)
+        out = [struct.pack("<4iQ", 80, 0, 1, 1, tsys),
+               struct.pack("<3i2fi2fi", n, n, 3, self.time, dt_global, iteration, p.courant, p.gamma, -1),
+               struct.pack("<6fi", 0.0, 0.0, 0.0, p.box[0], p.box[1], p.box[2], 80)]
+        dt_tick = p.dtmax / float(1 << 31)
+        for i in range(n):
+            W = _to_primitive(st["U"][i], vol[i])
+            pres = ((p.gamma - 1.0) * W[4] if p.gamma > 1.0 else W[4]) if p.eos == 0 else W[4]
+            L = math.pow(vol[i] * 3.0 / 4.0 / math.pi, 1.0 / 3.0)
+            dt = dt_tick * float(1 << (31 - int(st["rung"][i])))
+            out.append(struct.pack(
+                "<ii3f3f4fi3f3f5f3fi", 104, i if idx is None else int(idx[i]),
+                *mo["orig_pos"][i], *mo["orig_vel"][i], W[0], W[4], pres,
+                0.0 if rmax is None else float(rmax[i]), int(bnd[i]),
+                W[1], W[2], W[3], W[5], W[6], W[7], dt, vol[i], W[8],
+                L * float(mo["divb"][i]), W[9], 0.0, 0.0, 0.0, 104))
+        return b"".join(out)
 
     def set_state(self, vel=None, tlast=None, tend=None, rung=None, U=None, dU=None, wrec=None, tsys_ticks=0):
         f = self._fn("set_state")

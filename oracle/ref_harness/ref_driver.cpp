@@ -39,12 +39,21 @@ namespace {
   int    g_eos = 0;          /* 0: ideal gas, 1: isothermal disk */
   double g_iso_GM = 1.0;     /* disk: cs^2(r) = GM/|r| * c_fac^2 */
   double g_iso_cfac = 0.05;
+  int    g_static_mesh = 0;  /* 1: static generators */
 }
 
 namespace fvmhd3d {
 
   bool system::problem_force_distribute() { return false; }
-  bool system::compute_pvel1() { return false; }
+  /* The reference's default hook returns false (MPI/set_problem.cpp:61-76);
+   * its disabled branch, used here for static generators, zeroes vel of every
+   * active site and returns true. */
+  bool system::compute_pvel1()
+  {
+    if (!g_static_mesh) return false;
+    for (size_t a = 0; a < site_active_list.size(); a++) ptcl_import[site_active_list[a]].vel = 0.0;
+    return true;
+  }
 
   /* MPI/set_problem.cpp:77-87 */
   void system::predict(const int i)
@@ -131,6 +140,7 @@ struct ref_params {
   double dtmax;
   int    eos;
   double iso_GM, iso_cfac;
+  int    static_mesh;
 };
 
 struct ref_snap {
@@ -232,6 +242,7 @@ void *ref_create(const ref_params *p)
   g_eos = p->eos;
   g_iso_GM = p->iso_GM;
   g_iso_cfac = p->iso_cfac;
+  g_static_mesh = p->static_mesh;
   return c;
 }
 
@@ -283,6 +294,8 @@ int ref_init_problem(void *h, const double *W, const double *pos, const int *bnd
   s.dU_local.assign(n, FluidD(0.0));
   s.Wrec_local.resize(n);
   s.divBi.assign(n, 0.0f);
+  s.Wextra_local.resize(n);
+  for (int i = 0; i < n; i++) s.Wextra_local[i].J = vec3(0.0);
   s.ngb_list.assign(n, Neighbours<Ngb>());
   for (int i = 0; i < n; i++)
   {
@@ -295,6 +308,7 @@ int ref_init_problem(void *h, const double *W, const double *pos, const int *bnd
     p.rung = 0;
     p.boundary = bnd ? bnd[i] : 0;
     p.idx = i;
+    p.rmax = 0.0f;
     p.local_id = i;
     p.volume = p.volume_new = c->cells[i].Volume;
     Fluid m;
@@ -423,6 +437,29 @@ int ref_step(void *h, int shared, ref_snap *snap)
 }
 
 double ref_time(void *h) { return ((RefCtx *)h)->s->t_global; }
+
+/* orig_pos / orig_vel of the particles and divBi (after a step). */
+int ref_get_motion(void *h, double *opos, double *ovel, float *divb)
+{
+  RefCtx *c = (RefCtx *)h;
+  fsys &s = *c->s;
+  for (int i = 0; i < c->ncell; i++)
+  {
+    const Particle &p = s.ptcl_local[i];
+    if (opos) { opos[3*i] = p.orig_pos.x; opos[3*i+1] = p.orig_pos.y; opos[3*i+2] = p.orig_pos.z; }
+    if (ovel) { ovel[3*i] = p.orig_vel.x; ovel[3*i+1] = p.orig_vel.y; ovel[3*i+2] = p.orig_vel.z; }
+    if (divb) divb[i] = s.divBi[i];
+  }
+  return 0;
+}
+
+/* The reference's snapshot writer, system::dump_binary (MPI/dump_binary.cpp). */
+int ref_dump_binary(void *h, const char *path)
+{
+  RefCtx *c = (RefCtx *)h;
+  c->s->dump_binary(path);
+  return 0;
+}
 double ref_dt_tick(void *h) { return ((RefCtx *)h)->s->scheduler.dt_tick; }
 unsigned long long ref_tsys_ticks(void *h) { return ((RefCtx *)h)->s->scheduler.tsysU; }
 

@@ -38,17 +38,22 @@ def setup_case(nside=8, problem="alfven", seed=1, noise=0.05, gamma=5.0 / 3.0):
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 GOLDEN_STEP_CASES = ["ref_alfven4_shared.npz", "ref_ot5_shared.npz", "ref_blast7_individual.npz",
-                     "ref_blast8_individual.npz", "ref_disk4k_individual.npz"]
+                     "ref_blast8_individual.npz", "ref_disk4k_individual.npz",
+                     "ref_disk4k_static_individual.npz"]
 
 
 def golden_params(z):
     """System parameters of a fixture (ideal gas, unit box by default; the
-    disk fixture stores gamma, courant, box, dtmax, eos, GM, cfac)."""
+    disk fixtures store gamma, courant, box, dtmax, eos, GM, cfac and, in
+    the static-generator one, static_mesh)."""
     if "params" not in z:
         return {}
     p = z["params"]
-    return dict(gamma=float(p[0]), courant=float(p[1]), box=(float(p[2]), float(p[3]), float(p[4])),
-                dtmax=float(p[5]), eos=int(p[6]), iso_GM=float(p[7]), iso_cfac=float(p[8]))
+    out = dict(gamma=float(p[0]), courant=float(p[1]), box=(float(p[2]), float(p[3]), float(p[4])),
+               dtmax=float(p[5]), eos=int(p[6]), iso_GM=float(p[7]), iso_cfac=float(p[8]))
+    if p.shape[0] > 9:
+        out["static_mesh"] = bool(p[9])
+    return out
 
 
 def load_golden(name):

@@ -26,6 +26,25 @@ def mesh_arrays(m):
                 cell_centroid=m.cell_centroid, cell_face_off=m.cell_face_off, cell_face_ids=m.cell_face_ids)
 
 
+def finish(R, out, nact, faces, path):
+    """Final state, generator motion, clock and the reference's own snapshot
+    file (system::dump_binary) after the last step."""
+    st = R.get_state()
+    out.update({"out_" + k: v for k, v in st.items()})
+    mo = R.get_motion()
+    out.update({"out_" + k: v for k, v in mo.items()})
+    out["out_time"] = np.float64(R.time)
+    out["out_tsys"] = np.uint64(R.tsys_ticks)
+    out["out_nactive"] = np.array(nact, np.int32)
+    out["out_last_active_faces"] = faces[-1]
+    tmp = path + ".dump.tmp"
+    R.dump_binary(tmp)
+    with open(tmp, "rb") as f:
+        out["out_dump_binary"] = np.frombuffer(f.read(), np.uint8)
+    os.unlink(tmp)
+    np.savez_compressed(path, **out)
+
+
 def run_case(name, nside, problem, shared, nsteps, seed, noise=0.05):
     m = F.build_periodic(F.jittered_lattice(nside, 0.1, seed=seed), 1.0)
     W = F.problems.perturbed(getattr(F.problems, problem)(m.pos), noise, seed=seed + 1)
@@ -38,37 +57,30 @@ def run_case(name, nside, problem, shared, nsteps, seed, noise=0.05):
         s = R.step(shared=bool(shared), snap=True)
         nact.append(s["nactive"])
         faces.append(s["active_faces"])
-    st = R.get_state()
-    out.update({"out_" + k: v for k, v in st.items()})
-    out["out_time"] = np.float64(R.time)
-    out["out_nactive"] = np.array(nact, np.int32)
-    out["out_last_active_faces"] = faces[-1]
-    np.savez_compressed(os.path.join(HERE, name), **out)
+    finish(R, out, nact, faces, os.path.join(HERE, name))
     print(name, m.ncell, "cells", m.nface, "faces; active per step", nact)
 
 
-def disk_case(name, n, nsteps, seed=3):
-    """Keplerian disk, isothermal EOS, individual timesteps, with a DIOD sink."""
+def disk_case(name, n, nsteps, seed=3, static_mesh=False):
+    """Keplerian disk, isothermal EOS, individual timesteps, with a DIOD sink;
+    generators moving with the flow, or static (compute_pvel1 hook)."""
     pos, box = F.problems.disk_generators(n, seed=seed)
     m = F.build_periodic(pos, box)
     W, bnd = F.problems.disk(pos, box, r_sink=0.55)
-    prm = dict(gamma=1.0, courant=0.4, box=tuple(box), dtmax=1.0 / 16, eos=1, iso_GM=1.0, iso_cfac=0.05)
+    prm = dict(gamma=1.0, courant=0.4, box=tuple(box), dtmax=1.0 / 16, eos=1, iso_GM=1.0, iso_cfac=0.05,
+               static_mesh=static_mesh)
     R = RefSystem(**prm)
     R.set_mesh(m)
     R.init_problem(W, bnd=bnd)
     out = dict(mesh_arrays(m), W=W, bnd=bnd, shared=np.int32(0), nsteps=np.int32(nsteps),
-               params=np.array([prm["gamma"], prm["courant"], box[0], box[1], box[2], prm["dtmax"], 1.0, 1.0, 0.05]))
+               params=np.array([prm["gamma"], prm["courant"], box[0], box[1], box[2], prm["dtmax"], 1.0, 1.0, 0.05,
+                                float(static_mesh)]))
     nact, faces = [], []
     for _ in range(nsteps):
         s = R.step(shared=False, snap=True)
         nact.append(s["nactive"])
         faces.append(s["active_faces"])
-    st = R.get_state()
-    out.update({"out_" + k: v for k, v in st.items()})
-    out["out_time"] = np.float64(R.time)
-    out["out_nactive"] = np.array(nact, np.int32)
-    out["out_last_active_faces"] = faces[-1]
-    np.savez_compressed(os.path.join(HERE, name), **out)
+    finish(R, out, nact, faces, os.path.join(HERE, name))
     print(name, m.ncell, "cells", m.nface, "faces,", int((bnd > 0).sum()), "DIOD cells; active per step", nact)
 
 
@@ -104,4 +116,5 @@ if __name__ == "__main__":
     run_case("ref_blast8_individual.npz", 8, "blast", False, 10, seed=12)
     run_case("ref_ot5_shared.npz", 5, "orszag_tang", True, 6, seed=13)
     disk_case("ref_disk4k_individual.npz", 4096, 12)
+    disk_case("ref_disk4k_static_individual.npz", 4096, 16, seed=8, static_mesh=True)
     flux_case("ref_flux_kat.npz")

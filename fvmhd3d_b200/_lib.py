@@ -59,6 +59,7 @@ SIGNATURES = {
     "fvm_get_dt_list": (c_int, [c_void_p, c_void_p]),
     "fvm_get_counters": (c_int, [c_void_p, c_void_p]),
     "fvm_compute_flux": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
+    "fvm_compute_flux_static": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_last_step_ms": (c_float, [c_void_p]),
     "fvm_stream": (c_void_p, [c_void_p]),
     "fvm_last_step_counts": (c_int, [c_void_p, c_void_p, c_void_p]),

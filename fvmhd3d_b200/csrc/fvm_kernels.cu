@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <cstdlib>
@@ -2548,3 +2549,96 @@ int fvm_compute_flux(fvm_ctx *c, int nface, const double *wij, const double *Wi,
 
 }  // extern "C"
 
+// ==================== fvm_compute_flux_static (no allocation) ====================
+//
+// fvm_compute_flux stages its face batch in a device buffer it cudaMallocs and
+// cudaFrees on every call.  Some callers cannot do that while they run: a host
+// integrator that solves boundary or sub-grid face batches between steps of a
+// GPU pipeline whose other streams stay busy (cudaFree waits for the whole
+// device, stalling them), and a run that holds most of HBM for its mesh, where
+// a per-call cudaMalloc can fail half way through.  fvm_compute_flux_static
+// runs the same kernel (k_flux_kat) on the same inputs with its staging in the
+// file-scope array below instead, and calls no allocating routine.
+//
+// Capacity: FVM_FLUX_STATIC_MAX_FACES faces per call (308 bytes a face, about
+// 5 MB, held by every process that loads this library on each device it uses).
+// Layout, in doubles unless noted, each region sized for the capacity:
+//   wij 3, Wi 10, Wj 10, normal 3, psi 1, Bn 1, flux 10, boundary flags 1 (int)
+// The capacity is a multiple of 32, so every region starts 256-byte aligned.
+// Only the boundary-flag region must start at zero, and only when the caller
+// passes no flags: it is cleared on the stream before the kernel.  Every call
+// on a device shares this one array, so calls whose GPU work overlaps (from
+// several host threads, or several contexts on one device, at once) race;
+// each call returns only after its stream has synchronised, so calls made one
+// after another do not overlap.
+
+static_assert(FVM_FLUX_STATIC_MAX_FACES % 32 == 0, "regions of the staging array must stay 256-byte aligned");
+#define FLUX_STAGE_DOUBLES_PER_FACE 38
+static __device__ __align__(256) double g_flux_stage[(size_t)FVM_FLUX_STATIC_MAX_FACES * FLUX_STAGE_DOUBLES_PER_FACE +
+                                                     FVM_FLUX_STATIC_MAX_FACES / 2];
+
+namespace {
+constexpr int kStageDevices = 64;
+std::mutex g_flux_stage_mu;
+double *g_flux_stage_ptr[kStageDevices];  // device address of g_flux_stage, per device
+
+// Device address of the staging array on the current device (looked up once
+// per device).  The caller has made c->device current.
+int flux_stage_address(fvm_ctx *c, double **out) {
+  if (c->device < 0 || c->device >= kStageDevices) {
+    c->err = "fvm_compute_flux_static: device index out of range";
+    return FVM_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(g_flux_stage_mu);
+  if (!g_flux_stage_ptr[c->device]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_flux_stage);
+    if (e != cudaSuccess || !p) {
+      c->err = std::string("fvm_compute_flux_static: cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+      return FVM_ECUDA;
+    }
+    g_flux_stage_ptr[c->device] = (double *)p;
+  }
+  *out = g_flux_stage_ptr[c->device];
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const double *Wi, const double *Wj,
+                            const int *jbnd, const double *normal, double *psi, double *Bn, double *flux) {
+  if (!c || nface < 0 || !wij || !Wi || !Wj || !normal || !psi || !Bn || !flux) return FVM_EINVAL;
+  if (nface > FVM_FLUX_STATIC_MAX_FACES) {
+    c->err = "fvm_compute_flux_static: nface " + std::to_string(nface) + " exceeds the static staging capacity of " +
+             std::to_string(FVM_FLUX_STATIC_MAX_FACES) + " faces; split the batch or use fvm_compute_flux";
+    return FVM_ERANGE;
+  }
+  if (nface == 0) return 0;
+  CK(cudaSetDevice(c->device));
+  double *base = nullptr;
+  const int rc = flux_stage_address(c, &base);
+  if (rc) return rc;
+  const size_t M = FVM_FLUX_STATIC_MAX_FACES, nf = nface;
+  double *dw = base, *da = dw + 3 * M, *db = da + 10 * M, *dn = db + 10 * M, *dp = dn + 3 * M, *dB = dp + M,
+         *dF = dB + M;
+  int *dj = (int *)(dF + 10 * M);
+  CK(cudaMemcpyAsync(dw, wij, sizeof(double) * 3 * nf, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(da, Wi, sizeof(double) * 10 * nf, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(db, Wj, sizeof(double) * 10 * nf, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dn, normal, sizeof(double) * 3 * nf, cudaMemcpyHostToDevice, c->st));
+  if (jbnd)
+    CK(cudaMemcpyAsync(dj, jbnd, sizeof(int) * nf, cudaMemcpyHostToDevice, c->st));
+  else
+    CK(cudaMemsetAsync(dj, 0, sizeof(int) * nf, c->st));
+  k_flux_kat<<<nblk(nface, 128), 128, 0, c->st>>>(nface, c->P, dw, da, db, dj, dn, dp, dB, dF);
+  CK(cudaGetLastError());
+  c->launches++;
+  CK(cudaMemcpyAsync(psi, dp, sizeof(double) * nf, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(Bn, dB, sizeof(double) * nf, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(flux, dF, sizeof(double) * 10 * nf, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+}  // extern "C"

@@ -178,6 +178,22 @@ int fvm_get_counters(fvm_ctx *c, long long *out2);
 int fvm_compute_flux(fvm_ctx *c, int nface, const double *wij, const double *Wi, const double *Wj,
                      const int *jbnd, const double *normal, double *psi, double *Bn, double *flux);
 
+/* No counterpart in the reference.  fvm_compute_flux without device
+ * allocation, for callers that must not allocate while they run: a host
+ * integrator solving boundary or sub-grid face batches between steps while
+ * other streams keep the GPU busy (fvm_compute_flux's per-call cudaFree waits
+ * for the whole device), or a run holding most of HBM for its mesh, where a
+ * per-call cudaMalloc can fail mid-run.  Same arguments and results as
+ * fvm_compute_flux; the batch is staged in one fixed device array of
+ * FVM_FLUX_STATIC_MAX_FACES faces (about 5 MB) that every call on a device
+ * shares.  nface above the capacity returns FVM_ERANGE and does nothing.
+ * Calls whose GPU work overlaps (several host threads, or several contexts on
+ * one device, at once) race on that array; each call returns after its work
+ * has finished, so calls made one after another are safe. */
+#define FVM_FLUX_STATIC_MAX_FACES 16384
+int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const double *Wi, const double *Wj,
+                            const int *jbnd, const double *normal, double *psi, double *Bn, double *flux);
+
 /* Timing helper: CUDA-event time in ms of the last fvm_step's kernels. */
 float fvm_last_step_ms(const fvm_ctx *c);
 /* The context's CUDA stream (a cudaStream_t), for callers that order their

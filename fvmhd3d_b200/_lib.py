@@ -63,6 +63,7 @@ SIGNATURES = {
     "fvm_last_step_ms": (c_float, [c_void_p]),
     "fvm_stream": (c_void_p, [c_void_p]),
     "fvm_last_step_counts": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "fvm_last_adjust_stats": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "fvm_launch_count": (c_ll, [c_void_p]),
     "fvm_set_profiling": (c_int, [c_void_p, c_int]),
     "fvm_kernel_times": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(c_double),

@@ -46,6 +46,9 @@ using namespace fvm;
 #define FVM_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CELL_MINB_F : FVM_CELL_MINB_D)
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
 // cell-kernel mappings: grouped (16 lanes per cell) or two threads per cell
+#ifndef FVM_ADJUST_REPLAY
+#define FVM_ADJUST_REPLAY 1  // adjust_timesteps by parallel replay (sequential sweep as fallback)
+#endif
 #ifndef FVM_CELLMAP_GROUPED
 #define FVM_CELLMAP_GROUPED 0
 #endif
@@ -73,7 +76,8 @@ struct Sched {
   double t_global, dtmin;
   int min_rung, max_rung;
   int iscal[8];  // [0] rung maximum, [1] active cells, [2] error flags, [3] active faces,
-                 // [4] dirty sites of adjust_timesteps, [5] active non-boundary sites
+                 // [4] dirty sites of adjust_timesteps, [5] active non-boundary sites,
+                 // [6] adjust_timesteps replays, [7] 1 if the sequential sweep ran
   unsigned long long nactive_total, nfaces_total, steps;
   unsigned long long tprevU;  // tsysU before the last pull_active_list
 };
@@ -86,6 +90,10 @@ struct Dev {
   int *off, *lnk;
   int *perm;  // thread slot -> cell (face-count order inside windows of CPW cells)
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
+  int2 *lfj;            // per link: face id, neighbour (~j when the cell is s2)
+  int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
+  double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
+  int *aflag;               // adjust_timesteps replay flags
   // state
   double *pos, *vel, *tlast, *tend, *volp;
   double *opos, *ovel;  // orig_pos / orig_vel of correct() (generator motion)
@@ -1134,7 +1142,7 @@ __global__ void k_adjust_seq(const int *__restrict__ off, const int *__restrict_
                              const int *__restrict__ nsite, const int *__restrict__ ndirty,
                              double *__restrict__ dtl) {
   if (blockIdx.x != 0 || threadIdx.x != 0) return;
-  if (*ndirty == 0) return;
+  if (*ndirty == 0) return;  // nonzero when the sweep must run
   const int m = *nsite;
   for (int a = 0; a < m; a++) {
     const int i = alist[a];
@@ -1150,6 +1158,105 @@ __global__ void k_adjust_seq(const int *__restrict__ off, const int *__restrict_
       dtl[i] = di;
     }
   }
+}
+
+// ---- adjust_timesteps in parallel, bit for bit ----------------------------
+// The sequential sweep above visits the active non-boundary sites in
+// ascending order; at site i, for each face slot in order with a non-boundary
+// neighbour j, it sets dt_i = min(dt_i, 2 dt_j) and then
+// dt_j = min(dt_j, 2 dt_i).  min and doubling are exact, so every value the
+// sweep produces is 2^k dt0_y for a chain of such updates that runs forward in
+// sweep order, and each final dt is the minimum over the chains that end at
+// it.  The kernels below compute that minimum as a fixed point.  Per link q
+// (cell u, face slot s, neighbour v) they keep
+//   rdv[q]: dt of v when the sweep reaches u's slot s (what u reads there),
+//   wrv[q]: dt of u just after its own update at slot s (what v then reads).
+// Each replay lets every involved site walk its own timeline: the slots of
+// its active neighbours at their positions in the order (the sweep reads the
+// site's dt, then lowers it) and, for an active site, its own slots at its
+// own position.  It reads the neighbours' entries, writes its own, and keeps
+// the result in dtl.  Entries only decrease and start at the initial dt, an
+// upper bound, so replays converge; a replay that changes nothing leaves the
+// exact result.  Replays after convergence return at once.  If ADJ_ITERS
+// replays have not settled, the sequential sweep runs from the initial dt.
+// aflag[0..2]: changed flags of replays k % 3; [3] replays run; [4] fallback;
+// [5] settled (or nothing to do).
+constexpr int ADJ_ITERS = 24;
+
+__device__ __forceinline__ int lfj_nb(int2 fj) { return fj.y >= 0 ? fj.y : ~fj.y; }
+
+__global__ void k_adjust_init(int n, const int *__restrict__ off, const int2 *__restrict__ lfj,
+                              const unsigned char *__restrict__ act, const int *__restrict__ ndirty,
+                              const double *__restrict__ dtl, double *__restrict__ dt0, double *__restrict__ rdv,
+                              double *__restrict__ wrv, int *__restrict__ aflag) {
+  if (*ndirty == 0) return;  // every pair is within a factor 2: nothing changes
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u == 0) aflag[2] = 1;  // replay 0 runs
+  if (u >= n || !(act[u] & (A_ACTIVE | A_LNGB))) return;
+  const double du = dtl[u];
+  dt0[u] = du;
+  for (int q = off[u]; q < off[u + 1]; q++) {
+    const int v = lfj_nb(lfj[q]);
+    rdv[q] = (act[v] & (A_ACTIVE | A_LNGB)) ? dtl[v] : du;
+    wrv[q] = du;
+  }
+}
+
+__global__ void k_adjust_replay(int n, int k, const int *__restrict__ off, const int2 *__restrict__ lfj,
+                                const int *__restrict__ lsort, const int *__restrict__ lpart,
+                                const unsigned char *__restrict__ act, const double *__restrict__ dt0,
+                                double *__restrict__ rdv, double *__restrict__ wrv, double *__restrict__ dtl,
+                                int *__restrict__ aflag) {
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if (aflag[5]) return;
+  if (aflag[(k + 2) % 3] == 0) {  // the previous replay changed nothing (or none was needed)
+    if (t0 == 0) aflag[5] = 1;
+    return;
+  }
+  if (t0 == 0) { aflag[(k + 1) % 3] = 0; aflag[3] += 1; }
+  bool changed = false;
+  for (int u = t0; u < n; u += gridDim.x * blockDim.x) {  // grid-stride: a settled replay costs one launch
+    const unsigned char a = act[u];
+    if (!(a & (A_ACTIVE | A_LNGB))) continue;
+    const double d0 = dt0[u];
+    if (d0 < 0.0) continue;  // boundary: neither swept nor relaxed
+    const bool swept = (a & A_ACTIVE) != 0;
+    const int q0 = off[u], q1 = off[u + 1];
+    double cur = d0;
+    bool own_done = !swept;
+    auto own_slots = [&]() {  // the sweep at u's own position
+      for (int q = q0; q < q1; q++) {
+        if (dt0[lfj_nb(lfj[q])] < 0.0) continue;
+        cur = smin(cur, 2.0 * rdv[q]);
+        if (cur < wrv[q]) { wrv[q] = cur; changed = true; }
+      }
+    };
+    for (int t = q0; t < q1; t++) {  // neighbours in ascending index = sweep order
+      const int q = lsort[t];
+      const int v = lfj_nb(lfj[q]);
+      if (!own_done && v > u) { own_slots(); own_done = true; }
+      if ((act[v] & A_ACTIVE) && dt0[v] >= 0.0) {  // the sweep at v's position, v's slot for this face
+        const int p = lpart[q];
+        if (cur < rdv[p]) { rdv[p] = cur; changed = true; }
+        cur = smin(cur, 2.0 * wrv[p]);
+      }
+    }
+    if (!own_done) own_slots();
+    dtl[u] = cur;
+  }
+  if (changed) aflag[k % 3] = 1;
+}
+
+// Not settled after ADJ_ITERS replays: restore the initial dt for the
+// sequential sweep.
+__global__ void k_adjust_restore(int n, const unsigned char *__restrict__ act, const double *__restrict__ dt0,
+                                 double *__restrict__ dtl, int *__restrict__ aflag, int *__restrict__ stats) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool fallback = !aflag[5] && aflag[(ADJ_ITERS - 1) % 3] != 0;
+  if (u == 0) { stats[0] = aflag[3]; stats[1] = fallback ? 1 : 0; }
+  if (!fallback) return;
+  if (u == 0) aflag[4] = 1;
+  if (u < n && (act[u] & (A_ACTIVE | A_LNGB))) dtl[u] = dt0[u];
 }
 
 // rung assignment and inactive-neighbour promotion (MPI/compute_timestep.cpp
@@ -1500,6 +1607,20 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
   for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = Wx[k]; r[20 + k] = Wy[k]; r[30 + k] = Wz[k]; r[40 + k] = tt[k]; }
 }
 
+// Per link (a cell's entry in its face list, i.e. one side of a face), in the
+// order the cell walks its faces: the face id and the neighbour j, stored as
+// ~j when the cell is s2.  The mesh is fixed while it is installed.
+__global__ void k_link_tables(int n, const int *__restrict__ off, const int *__restrict__ lnk,
+                              const int2 *__restrict__ s12, int2 *__restrict__ lfj) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (int q = off[c]; q < off[c + 1]; q++) {
+    const int f = lnk[q];
+    const int2 e = s12[f];
+    lfj[q] = make_int2(f, e.x == c ? e.y : ~e.x);
+  }
+}
+
 __global__ void k_shared_sync(int n, Params P, const Sched *__restrict__ S, const unsigned char *__restrict__ act,
                               const int *__restrict__ iscal, int *__restrict__ rung, double *__restrict__ tend) {
   const double t_global = S->t_global;
@@ -1840,6 +1961,10 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc_bytes(c, &d.fst, 20 * c->rb * (size_t)nface);
   rc |= dalloc(c, &d.cvol, ncell); rc |= dalloc(c, &d.ccen, 3 * (size_t)ncell);
   rc |= dalloc(c, &d.off, ncell + 1); rc |= dalloc(c, &d.lnk, nl); rc |= dalloc(c, &d.perm, ncell);
+  rc |= dalloc(c, &d.lfj, nl);
+  rc |= dalloc(c, &d.lsort, nl); rc |= dalloc(c, &d.lpart, nl);
+  rc |= dalloc(c, &d.rdv, nl); rc |= dalloc(c, &d.wrv, nl); rc |= dalloc(c, &d.dt0, ncell);
+  rc |= dalloc(c, &d.aflag, 8);
   rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
   if ((ncell + CB - 1) / CB > CB * 16) { c->err = "fvm_set_mesh: more than 16M cells"; return FVM_ERANGE; }
   rc |= dalloc(c, &d.pos, 3 * (size_t)ncell); rc |= dalloc(c, &d.vel, 3 * (size_t)ncell);
@@ -1881,6 +2006,41 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   CK(cudaMemcpy(d.ccen, cell_centroid, sizeof(double) * 3 * ncell, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d.off, hoff.data(), sizeof(int) * (ncell + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(d.lnk, ids, sizeof(int) * nl, cudaMemcpyHostToDevice));
+  {
+    // every face must be listed once by each of its two cells: the link of
+    // the other side, and each cell's links ordered by neighbour index
+    std::vector<int> flink(2 * (size_t)nface, -1), part(nl), srt(nl);
+    for (int c0 = 0; c0 < ncell; c0++)
+      for (long long q = off[c0]; q < off[c0 + 1]; q++) {
+        const int f = ids[q];
+        const int side = s1[f] == c0 ? 0 : (s2[f] == c0 ? 1 : -1);
+        if (side < 0 || flink[2 * (size_t)f + side] >= 0) {
+          c->err = "fvm_set_mesh: face " + std::to_string(f) + " listed by a cell that is not its side, or twice";
+          return FVM_EINVAL;
+        }
+        flink[2 * (size_t)f + side] = (int)q;
+      }
+    for (int f = 0; f < nface; f++) {
+      const int a = flink[2 * (size_t)f], b = flink[2 * (size_t)f + 1];
+      if (a < 0 || b < 0) {
+        c->err = "fvm_set_mesh: face " + std::to_string(f) + " missing from a cell's face list";
+        return FVM_EINVAL;
+      }
+      part[a] = b;
+      part[b] = a;
+    }
+    for (int c0 = 0; c0 < ncell; c0++) {
+      const long long q0 = off[c0], q1 = off[c0 + 1];
+      for (long long q = q0; q < q1; q++) srt[q] = (int)q;
+      auto nb = [&](int q) { const int f = ids[q]; return s1[f] == c0 ? s2[f] : s1[f]; };
+      std::sort(srt.begin() + q0, srt.begin() + q1, [&](int x, int y) { return nb(x) < nb(y); });
+    }
+    CK(cudaMemcpy(d.lpart, part.data(), sizeof(int) * nl, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d.lsort, srt.data(), sizeof(int) * nl, cudaMemcpyHostToDevice));
+    k_link_tables<<<nblk(ncell, 256), 256, 0, c->st>>>(ncell, d.off, d.lnk, d.s12, d.lfj);
+    LAUNCH_CHECK();
+    CK(cudaStreamSynchronize(c->st));
+  }
   {
     std::vector<int> perm(ncell);
     for (int i = 0; i < ncell; i++) perm[i] = i;
@@ -1936,6 +2096,7 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   CK(cudaMemsetAsync(d.tlast, 0, sizeof(double) * n, c->st));
   k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
   LAUNCH_CHECK();
+
   BULK(k_init_state<R><<<nblk(n, 128), 128, 0, c->st>>>(n, dW, d.cvol, d.U, d.dU, (R *)d.Wrec, d.volp));
   LAUNCH_CHECK();
   // compute_pvel on all cells, then the shared timestep
@@ -2114,7 +2275,7 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     k_halve<<<nblk(n, 256), 256, 0, c->st>>>(n, d.act, &d.S->dtmin, d.dtl);
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(d.hash, 0, n, c->st));
-    CK(cudaMemsetAsync(&d.S->iscal[4], 0, 2 * sizeof(int), c->st));
+    CK(cudaMemsetAsync(&d.S->iscal[4], 0, 4 * sizeof(int), c->st));
     k_adjust_mark<<<nblk(n, 128), 128, 0, c->st>>>(n, d.off, d.lnk, d.s12, d.act, d.bnd, d.dtl, d.hash,
                                                    &d.S->iscal[4], d.act0);
     LAUNCH_CHECK();
@@ -2125,7 +2286,22 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     LAUNCH_CHECK();
     k_place_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount, d.alist);
     LAUNCH_CHECK();
+#if FVM_ADJUST_REPLAY
+    CK(cudaMemsetAsync(d.aflag, 0, 8 * sizeof(int), c->st));
+    k_adjust_init<<<nblk(n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.act, &d.S->iscal[4], d.dtl, d.dt0, d.rdv,
+                                                   d.wrv, d.aflag);
+    LAUNCH_CHECK();
+    for (int k = 0; k < ADJ_ITERS; k++) {
+      k_adjust_replay<<<smin(nblk(n, 128), 148 * 16), 128, 0, c->st>>>(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv,
+                                                       d.wrv, d.dtl, d.aflag);
+      LAUNCH_CHECK();
+    }
+    k_adjust_restore<<<nblk(n, 256), 256, 0, c->st>>>(n, d.act, d.dt0, d.dtl, d.aflag, &d.S->iscal[6]);
+    LAUNCH_CHECK();
+    k_adjust_seq<<<1, 32, 0, c->st>>>(d.off, d.lnk, d.s12, d.alist, &d.S->iscal[5], &d.aflag[4], d.dtl);
+#else
     k_adjust_seq<<<1, 32, 0, c->st>>>(d.off, d.lnk, d.s12, d.alist, &d.S->iscal[5], &d.S->iscal[4], d.dtl);
+#endif
     LAUNCH_CHECK();
   }
   kt_end(c, KT_TIMESTEP);
@@ -2428,6 +2604,14 @@ int fvm_dump_binary(fvm_ctx *c, const char *path, const int *idx, const float *r
   const size_t put = fwrite(w.data(), sizeof(uint32_t), w.size(), f);
   const int cl = fclose(f);
   if (put != w.size() || cl != 0) { c->err = std::string("fvm_dump_binary: short write to ") + path; return FVM_EIO; }
+  return 0;
+}
+
+int fvm_last_adjust_stats(const fvm_ctx *c, int *dirty_sites, int *replays, int *sequential) {
+  if (!c) return FVM_EINVAL;
+  if (dirty_sites) *dirty_sites = c->hS.iscal[4];
+  if (replays) *replays = c->hS.iscal[6];
+  if (sequential) *sequential = c->hS.iscal[7];
   return 0;
 }
 

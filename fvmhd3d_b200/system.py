@@ -169,6 +169,13 @@ class System:
                     "fvm_get_motion")
         return out
 
+    def adjust_stats(self):
+        """(dirty sites, parallel replays, sequential sweep ran) of the last
+        individual-timestep step's adjust_timesteps."""
+        v = [ctypes.c_int(0) for _ in range(3)]
+        self._check(self.L.fvm_last_adjust_stats(self.h, *[ctypes.byref(x) for x in v]), "fvm_last_adjust_stats")
+        return tuple(x.value for x in v)
+
     def clock(self):
         """(tsysU, dt_global, iteration): the scheduler clock after the last
         step (the reference's Scheduler::tsysU, system::dt_global and

@@ -201,6 +201,11 @@ float fvm_last_step_ms(const fvm_ctx *c);
 void *fvm_stream(fvm_ctx *c);
 /* Active cells and active faces of the last completed step. */
 int fvm_last_step_counts(const fvm_ctx *c, int *ncell_active, int *nface_active);
+
+/* adjust_timesteps diagnostics of the last individual-timestep step: sites
+ * with a neighbour outside a factor 2, parallel replays run, and 1 if the
+ * sequential sweep had to run instead (any pointer may be NULL). */
+int fvm_last_adjust_stats(const fvm_ctx *c, int *dirty_sites, int *replays, int *sequential);
 /* Number of kernels this context has launched so far. */
 long long fvm_launch_count(const fvm_ctx *c);
 /* Per-kernel CUDA-event timing: on != 0 enables it and clears the totals. */

@@ -170,3 +170,36 @@ def test_graph_replay_matches_eager_steps(shared):
     sa, sb = a.get_state(), b.get_state()
     for k in sa:
         assert np.array_equal(sa[k], sb[k]), k
+
+
+def test_adjust_timesteps_replay_vs_oracle():
+    """adjust_timesteps (the order-dependent neighbour relaxation) on a blast
+    with a 1e6 pressure contrast, individual timesteps: the relaxed dt list,
+    rungs and promotions match the oracle's sequential sweep after every
+    step, and the parallel replay settles without the sequential fallback."""
+    from oracle.pyoracle import OracleSystem
+    m, W = setup_case(12, "blast", seed=9, noise=0.02)
+    W = W.copy()
+    r = np.linalg.norm(m.pos - 0.5, axis=1)
+    W[r < 0.12, 4] *= 1e4  # ETHM: pressure 1e6 x the ambient value
+    s = gpu_system(m, W)
+    o = OracleSystem()
+    o.set_mesh(m)
+    o.init_problem(W)
+    dirty_steps = 0
+    for _ in range(14):
+        snap = o.step(shared=False, snap=True)
+        assert s.step(shared=False) == snap["nactive"]
+        dirty, replays, sequential = s.adjust_stats()
+        assert sequential == 0
+        if dirty:
+            dirty_steps += 1
+            assert replays >= 1
+        ref = snap["dt_after_timestep"]
+        mask = ref < 3.0e38  # cells of this step's sweep (the others keep HUGE)
+        got = s.dt_list()
+        assert np.abs(got[mask] - ref[mask]).max() <= RTOL_FP64 * np.abs(ref[mask]).max()
+        st, so = s.get_state(), o.get_state()
+        for k in ("rung", "tend", "tlast"):
+            assert np.array_equal(st[k], so[k]), k
+    assert dirty_steps >= 3

@@ -43,16 +43,17 @@ UNIT = "face-updates/s"
 def kernel_bytes(name, N, F, prec_bytes=8):
     w = prec_bytes
     table = {
-        # reads Wrec (50 w) + pos/tlast/flags per cell, face records; writes tau (10 w)
-        "limiter": N * (50 * w + 24 + 8 + 1) + F * 56 + N * 10 * w,
-        # reads Wrec + tau + pos + vel + tlast per cell, face records; writes the
+        # reads Wrec (50 w) + tlast/flags per cell, face records; writes tau (10 w)
+        # and the two extrapolated face states (20 w per face)
+        "limiter": N * (50 * w + 8 + 1) + F * 56 + N * 10 * w + F * 20 * w,
+        # reads the face states, face records, vel + tlast per cell; writes the
         # face contribution (14 w) and code
-        "corr_flux": N * (50 * w + 10 * w + 24 + 24 + 8) + F * 56 + F * (14 * 8 + 1),
-        # reads face contributions (each face by its two cells), U, dU, Wrec w,t, tau; writes U, dU
-        "corr_cell": F * (14 * 8 + 1) + N * (80 + 112 + 20 * w + 10 * w) + N * (80 + 112),
-        "pred_flux": N * (10 * w + 24 + 24) + F * 56 + F * (14 * 8 + 1),
+        "corr_flux": F * 20 * w + F * 56 + N * (24 + 8) + F * (14 * w + 1),
+        # reads face contributions, U, dU, Wrec w,t, tau; writes U, dU
+        "corr_cell": F * (14 * w + 1) + N * (80 + 112 + 20 * w + 10 * w) + N * (80 + 112),
+        "pred_flux": N * (10 * w + 24) + F * 56 + F * (14 * w + 1),
         # reads face contributions and U; writes Wrec t, rung, tend
-        "pred_cell": F * (14 * 8 + 1) + N * 80 + N * (10 * w + 12),
+        "pred_cell": F * (14 * w + 1) + N * 80 + N * (10 * w + 12),
         # reads Wst (neighbours), face records, Wrec t; writes Wrec
         "recon": F * 56 + N * (10 * w + 24 + 10 * w) + N * 50 * w,
         "timestep": N * (80 + 24 + 8 + 8) + F * 8 + N * 8,
@@ -63,6 +64,19 @@ def kernel_bytes(name, N, F, prec_bytes=8):
         "sync": N * 12,
     }
     return table.get(name)
+
+
+# DRAM bytes (read + write) per launch measured by ncu on the 64^3 blast
+# (262144 cells, 2085347 faces; profiles/cell_and_face_kernels_blast64_*_full.md),
+# per face; a launch on another mesh of the same kind moves these bytes times
+# its face count.
+NCU_FACES_64 = 2085347
+NCU_TRAFFIC_64 = {
+    ("limiter", 8): 307.860224e6 + 325.812992e6, ("limiter", 4): 269.500416e6 + 175.986176e6,
+    ("corr_flux", 8): 494.430720e6 + 206.727424e6, ("corr_flux", 4): 327.601152e6 + 95.878400e6,
+    ("corr_cell", 8): 658.710784e6 + 32.781312e6, ("corr_cell", 4): 274.513664e6 + 38.860288e6,
+    ("recon", 8): 316.076288e6 + 80.746496e6, ("recon", 4): 297.897216e6 + 39.122176e6,
+}
 
 
 def step_bytes(N, F, prec_bytes=8):
@@ -223,9 +237,13 @@ def run_gpu(args):
         sysargs = {}
         shared = True
     mesh_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(local)[0]
     S = F.System(precision=prec, device=local, **sysargs)
     S.set_mesh(m)
     S.init_problem(W, bnd=bnd)
+    torch.cuda.synchronize()
+    footprint = free0 - torch.cuda.mem_get_info(local)[0]
     stream = torch.cuda.ExternalStream(S.stream_ptr, device=local)
 
     for _ in range(args.warmup):
@@ -310,7 +328,10 @@ def run_gpu(args):
         ach = alg / per_launch_s / 1e9
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(ach / peak, 4), "peak_source": peak_kind,
-                    "algorithmic_bytes_per_launch": int(alg), "traffic": None,
+                    "algorithmic_bytes_per_launch": int(alg),
+                    "traffic": (int(NCU_TRAFFIC_64[(dom, pb)] * Fc / NCU_FACES_64)
+                                if (dom, pb) in NCU_TRAFFIC_64 and shared else None),
+                    "traffic_source": "ncu dram bytes of the 64^3 blast launch, scaled by face count",
                     "step_bytes_per_face_update": round(step_bytes(N, Fc, pb), 1),
                     "step_frac": round(value / ws * step_bytes(N, Fc, pb) / 1e9 / peak, 4)}
     breakdown = {k: {"ms_per_launch": round(v[0] / max(v[1], 1), 4), "share": round(v[0] / max(1e-9, sum(
@@ -326,7 +347,7 @@ def run_gpu(args):
                    "steps_mean_active_faces": round(faces / max(args.steps, 1), 1),
                    "ncell": N, "nface_per_step": Fc, "faces_per_cell": round(Fc / N, 3),
                    "l2": "inputs larger than L2 (state > 2 GB), no flush", "parallelism": f"replicas x{ws}",
-                   "mesh_build_s": round(mesh_s, 2)},
+                   "mesh_build_s": round(mesh_s, 2), "device_bytes": int(footprint)},
         "roofline": roofline, "kernels": breakdown, "gpu_launches": launches, "e2e": e2e, "clocks": clocks,
         "timing": "value: CUDA events around K graph-replayed steps on the context stream; kernels/roofline: "
                   "CUDA events around each kernel of a separate profiled pass of eager steps",

@@ -1,0 +1,282 @@
+// Learned face flux: a 16 -> 128 -> 128 -> 128 -> 8 GELU network that stands
+// in for riemann_solver (MPI/compute_update.cpp:1109-1341) on smooth faces.
+//
+// Inference runs on the 5th-generation tensor cores: one CTA takes tiles of
+// 128 faces; the weights sit in shared memory as BF16 in the K-major
+// no-swizzle core-matrix layout the tcgen05 shared-memory descriptors
+// describe; one elected thread issues tcgen05.mma (kind::f16, BF16 inputs,
+// FP32 accumulation in tensor memory); after each layer four warps read their
+// 32 rows back with tcgen05.ld, add the bias, apply GELU, round to BF16 and
+// write the next layer's A operand.  Tensor-memory columns [0,128) and
+// [128,256) alternate between layers.
+//
+// Included by fvm_kernels.cu (it uses the context and its error macros).
+
+#include <cuda_bf16.h>
+
+namespace mlp {
+
+constexpr int NIN = 16, NH = 128, NOUT = 8, NOUTP = 16, TILE = 128;
+constexpr int NPARAM = NH * NIN + NH + NH * NH + NH + NH * NH + NH + NOUT * NH + NOUT;
+static_assert(NPARAM == 36232, "parameter count");
+
+// byte offsets of the shared-memory image (each region 1024-byte aligned)
+constexpr int OFF_W1 = 0;                          // [NH x NIN]   4096 B
+constexpr int OFF_W2 = OFF_W1 + NH * NIN * 2;      // [NH x NH]   32768 B
+constexpr int OFF_W3 = OFF_W2 + NH * NH * 2;       // [NH x NH]   32768 B
+constexpr int OFF_W4 = OFF_W3 + NH * NH * 2;       // [NOUTP x NH] 4096 B
+constexpr int IMG_BYTES = OFF_W4 + NOUTP * NH * 2;  // weights image copied from global
+constexpr int OFF_A = IMG_BYTES;                   // [TILE x NH]  32768 B activations
+constexpr int OFF_BIAS = OFF_A + TILE * NH * 2;    // f32 b1, b2, b3 (3 x NH), b4 (NOUTP)
+constexpr int NBIAS = 3 * NH + NOUTP;
+constexpr int OFF_BAR = OFF_BIAS + NBIAS * 4;      // mbarrier (8 B) + tensor-memory address (4 B)
+constexpr int SMEM_BYTES = OFF_BAR + 16;
+constexpr int TMEM_COLS = 256;
+static_assert(OFF_W2 % 1024 == 0 && OFF_W3 % 1024 == 0 && OFF_W4 % 1024 == 0 && OFF_A % 1024 == 0, "align");
+
+// Element (row, k) of a K-major no-swizzle operand with `rows` rows: core
+// matrices of 8 rows x 16 bytes, 8-row groups 128 B apart (stride byte
+// offset), 8-element K chunks rows/8 * 128 B apart (leading byte offset).
+__host__ __device__ constexpr int kmajor_off(int row, int k, int rows) {
+  return ((k >> 3) * (rows >> 3) + (row >> 3)) * 128 + (row & 7) * 16 + (k & 7) * 2;
+}
+
+// tcgen05 shared-memory matrix descriptor, K-major, no swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// Instruction descriptor of kind::f16: BF16 A and B, FP32 D, both K-major.
+__host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0), "r"(0), "r"(0), "r"(0));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// Waits for the mbarrier phase `parity` to complete; gives up after a bounded
+// number of polls and returns false.
+__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
+  for (int it = 0; it < (1 << 22); it++) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
+}
+
+// The hardware tanh approximation (one MUFU instruction).
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// GELU, tanh form: 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the
+// hardware tanh in inference and training alike.
+__device__ __forceinline__ float gelu(float x) {
+  const float u = 0.7978845608028654f * (x + 0.044715f * x * x * x);
+  return 0.5f * x * (1.0f + tanh_hw(u));
+}
+
+__device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
+  const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
+
+// Hidden-layer epilogue: warp w takes rows 32 (w % 4) .. +31 (its
+// tensor-memory lane quarter) and columns 64 (w / 4) .. +63 of the
+// accumulator at col0; bias, GELU, BF16, into the A operand.
+__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, int col0, const float *bias, unsigned char *A,
+                                                int warp, int lane) {
+  const int q = warp & 3, h = warp >> 2, r = 32 * q + lane;
+#pragma unroll 1
+  for (int c = 2 * h; c < 2 * h + 2; c++) {
+    float v[32];
+    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(col0 + 32 * c), v);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      uint4 w;
+      const int k = 32 * c + 8 * q;
+      w.x = pack_bf16(gelu(v[8 * q + 0] + bias[k + 0]), gelu(v[8 * q + 1] + bias[k + 1]));
+      w.y = pack_bf16(gelu(v[8 * q + 2] + bias[k + 2]), gelu(v[8 * q + 3] + bias[k + 3]));
+      w.z = pack_bf16(gelu(v[8 * q + 4] + bias[k + 4]), gelu(v[8 * q + 5] + bias[k + 5]));
+      w.w = pack_bf16(gelu(v[8 * q + 6] + bias[k + 6]), gelu(v[8 * q + 7] + bias[k + 7]));
+      *reinterpret_cast<uint4 *>(A + kmajor_off(r, k, TILE)) = w;
+    }
+  }
+}
+
+// Y[n x 8] = MLP(X[n x 16]) (n read from n_dev when given); X in BF16, Y in
+// FP32.  256 threads per CTA: the eight warps share each epilogue (a
+// tensor-memory lane quarter and half the columns each).  err bit 1: an
+// mbarrier wait gave up.
+constexpr int THREADS = 256;
+__global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__restrict__ n_dev,
+                                                      const __nv_bfloat16 *__restrict__ X, float *__restrict__ Y,
+                                                      const uint4 *__restrict__ wimg, const float *__restrict__ bias_g,
+                                                      int *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  if (n_dev) n = *n_dev;  // row count produced on the device
+  const int t = threadIdx.x, warp = t >> 5;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + 8);
+  float *bias = reinterpret_cast<float *>(sm + OFF_BIAS);
+  unsigned char *A = sm + OFF_A;
+  for (int i = t; i < IMG_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4 *>(sm)[i] = wimg[i];
+  for (int i = t; i < NBIAS; i += blockDim.x) bias[i] = bias_g[i];
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (t == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t bar_a = smem_u32(bar);
+  const uint32_t a_addr = smem_u32(A);
+  const uint32_t w_addr = smem_u32(sm);
+  const uint32_t id_h = instr_desc(TILE, NH), id_o = instr_desc(TILE, NOUTP);
+  const uint32_t LBO_128 = (128 / 8) * 128, LBO_OUT = (NOUTP / 8) * 128, SBO = 128;
+  uint32_t parity = 0;
+  bool ok = true;
+  const int ntiles = (n + TILE - 1) / TILE;
+  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    // layer-1 input: thread t loads half a row of X (8 BF16, 16 bytes)
+    {
+      const int r = t & (TILE - 1), half = t >> 7, row = tile * TILE + r;
+      uint4 x = make_uint4(0, 0, 0, 0);
+      if (row < n) x = reinterpret_cast<const uint4 *>(X + (size_t)row * NIN)[half];
+      *reinterpret_cast<uint4 *>(A + kmajor_off(r, 8 * half, TILE)) = x;
+    }
+    // four layers; layer L reads A (and weights), writes tensor-memory columns dcol
+#pragma unroll 1
+    for (int L = 0; L < 4 && ok; L++) {
+      fence_async_smem();
+      fence_before();
+      __syncthreads();
+      if (t == 0) {
+        fence_after();
+        const uint32_t dcol = (L & 1) ? 128u : 0u;
+        if (L == 0) {
+          mma_bf16(tmem + dcol, smem_desc(a_addr, LBO_128, SBO), smem_desc(w_addr + OFF_W1, LBO_128, SBO), id_h, 0);
+        } else {
+          const uint32_t wb = w_addr + (L == 1 ? OFF_W2 : L == 2 ? OFF_W3 : OFF_W4);
+          const uint32_t lbo_b = L == 3 ? LBO_OUT : LBO_128;
+#pragma unroll 1
+          for (int kk = 0; kk < NH / 16; kk++)
+            mma_bf16(tmem + dcol, smem_desc(a_addr + 2 * kk * LBO_128, LBO_128, SBO),
+                     smem_desc(wb + 2 * kk * lbo_b, lbo_b, SBO), L == 3 ? id_o : id_h, kk > 0 ? 1u : 0u);
+        }
+        mma_commit(bar_a);
+      }
+      const bool waited = bar_wait(bar_a, parity);
+      if (!__syncthreads_and(waited)) {  // every thread leaves together
+        if (t == 0) atomicOr(err, 1);
+        ok = false;
+        break;
+      }
+      parity ^= 1;
+      fence_after();
+      if (L < 3) {
+        epilogue_hidden(tmem, (L & 1) ? 128 : 0, bias + NH * L, A, warp, t & 31);
+      } else if (warp < 4) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 128u, v);
+        const int row = tile * TILE + t;
+        if (row < n) {
+          float4 *yo = reinterpret_cast<float4 *>(Y + (size_t)row * NOUT);
+          const float *b4 = bias + 3 * NH;
+          yo[0] = make_float4(v[0] + b4[0], v[1] + b4[1], v[2] + b4[2], v[3] + b4[3]);
+          yo[1] = make_float4(v[4] + b4[4], v[5] + b4[5], v[6] + b4[6], v[7] + b4[7]);
+        }
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+__global__ void k_f32_to_bf16(long long n, const float *__restrict__ x, __nv_bfloat16 *__restrict__ y) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = __float2bfloat16_rn(x[i]);
+}
+
+// Parameters (W1[NH x NIN], b1, W2[NH x NH], b2, W3, b3, W4[NOUT x NH], b4)
+// -> shared-memory image of the BF16 weights (W4 padded to NOUTP rows with
+// zeros) and the FP32 biases (b4 padded likewise).
+__global__ void k_mlp_pack(const float *__restrict__ p, unsigned char *__restrict__ img, float *__restrict__ bias) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const float *W1 = p, *b1 = W1 + NH * NIN, *W2 = b1 + NH, *b2 = W2 + NH * NH, *W3 = b2 + NH, *b3 = W3 + NH * NH,
+              *W4 = b3 + NH, *b4 = W4 + NOUT * NH;
+  if (i < NH * NIN) {
+    const int r = i / NIN, k = i % NIN;
+    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W1 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(W1[i]);
+  }
+  if (i < NH * NH) {
+    const int r = i / NH, k = i % NH;
+    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W2 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(W2[i]);
+    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W3 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(W3[i]);
+  }
+  if (i < NOUTP * NH) {
+    const int r = i / NH, k = i % NH;
+    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W4 + kmajor_off(r, k, NOUTP)) =
+        __float2bfloat16_rn(r < NOUT ? W4[r * NH + k] : 0.0f);
+  }
+  if (i < NH) {
+    bias[i] = b1[i];
+    bias[NH + i] = b2[i];
+    bias[2 * NH + i] = b3[i];
+  }
+  if (i < NOUTP) bias[3 * NH + i] = i < NOUT ? b4[i] : 0.0f;
+}
+
+}  // namespace mlp

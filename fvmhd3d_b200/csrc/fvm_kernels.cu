@@ -13,6 +13,9 @@
 // same bits.  Each face flux is evaluated once by a face-parallel kernel that
 // stores the face's contribution; the owning cells then gather it.
 #include "fvm_math.cuh"
+#include "flux_mlp.cuh"
+#include "mlp_train.cuh"
+#include "flux_learn.cuh"
 #include "../../include/fvmhd3d_b200.h"
 
 #include <cuda_runtime.h>
@@ -94,6 +97,8 @@ struct Dev {
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
   double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
   int *aflag;               // adjust_timesteps replay flags
+  // learned-flux buffers (fvm_set_flux_mode)
+  void *lX, *lY, *lface, *lcount, *lstats, *lhx, *lhy, *lhcount, *lnorm;
   // state
   double *pos, *vel, *tlast, *tend, *volp;
   double *opos, *ovel;  // orig_pos / orig_vel of correct() (generator motion)
@@ -582,15 +587,66 @@ __global__ void __launch_bounds__(GTB) k_recon_g(int n, Params P, const Sched *_
 // One thread per face: half-step extrapolated face states, face velocity,
 // rotated-frame HLLD flux.  Stores flux*dt*area, gradPsi and divB
 // contributions (in the bulk type) for the owning cells to gather.
-template <typename R>
+// Face flux of one pass under the learned-flux mode MODE: exact (LM_EXACT),
+// exact with harvesting (LM_HARVEST), gate and defer to the network
+// (LM_DEFER: returns false for a deferred face), or the deferred face's flux
+// from the network output (LM_FINISH), falling back to the exact solver when
+// the face would move more than half of either cell's mass within its step
+// (tdt_i, tdt_j: area times each side's step) or the result is not finite.
+enum { LM_EXACT = 0, LM_HARVEST = 1, LM_DEFER = 2, LM_FINISH = 3 };
+
+template <typename R, int MODE>
+__device__ __forceinline__ bool learned_flux(const Params &P, const Sched *S, const LearnBuf &lb, int f, int slot,
+                                             int pass, const R *wij, const R *Wi, const R *Wj, int jb, const R *nr,
+                                             R &psi, R &Bn, R *flux, double tdt_i, double tdt_j, int i, int j) {
+  if (MODE == LM_EXACT) {
+    compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
+    return true;
+  }
+  const unsigned salt = (unsigned)(S->steps * 2 + pass);
+  if (MODE == LM_HARVEST) {
+    HarvestSolver h{P, lb, (unsigned)f, salt};
+    compute_flux_with<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux, h);
+    return true;
+  }
+  if (MODE == LM_DEFER) {
+    DeferSolver h{P, lb, f};
+    return compute_flux_with<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux, h);
+  }
+  if (slot == 0) atomicAdd(&lb.stats[LSTAT_DEFERRED], (double)*lb.count);  // once per pass
+  float y[8];
+  const float4 *yp = reinterpret_cast<const float4 *>(lb.Y + 8 * (size_t)slot);
+  const float4 y0 = yp[0], y1 = yp[1];
+  y[0] = y0.x; y[1] = y0.y; y[2] = y0.z; y[3] = y0.w; y[4] = y1.x; y[5] = y1.y; y[6] = y1.z; y[7] = y1.w;
+  LearnedSolver h{lb, y, lb.judge != 0 && face_hash((unsigned)f, salt) % lb.judge == 0};
+  compute_flux_with<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux, h);
+  const double dm = fabs(double(flux[MASS]));
+  bool ok = dm * tdt_i <= 0.5 * lb.U[10 * (size_t)i + MASS] && dm * tdt_j <= 0.5 * lb.U[10 * (size_t)j + MASS];
+#pragma unroll
+  for (int k = 0; k < NF; k++) ok = ok && isfinite(double(flux[k]));
+  if (!ok) {
+    compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
+    atomicAdd(&lb.stats[LSTAT_FALLBACK], 1.0);
+  }
+  return true;
+}
+
+template <typename R, int MODE>
 __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Params P, const Sched *__restrict__ S,
     const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
     const unsigned char *__restrict__ fflag, const int *__restrict__ bnd, const double *__restrict__ vel,
     const double *__restrict__ tlast, const R *__restrict__ Wrec, const R *__restrict__ fst,
-    R *__restrict__ fcon, unsigned char *__restrict__ fcode) {
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode, LearnBuf lb) {
   const double t_global = S->t_global;
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nf) return;
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  int slot = -1;
+  if (MODE == LM_FINISH) {  // one deferred face per thread
+    if (f >= *lb.count) return;
+    slot = f;
+    f = lb.gface[slot];
+  } else if (f >= nf) {
+    return;
+  }
   const unsigned char ff = fflag[f];
   if (!(ff & FF_ACTIVE)) { fcode[f] = F_OFF; return; }
   const int2 e = s12[f];
@@ -630,7 +686,10 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Par
   const R nr[3] = {R(nrm[0]), R(nrm[1]), R(nrm[2])};
   R psi, Bn, flux[NF];
   const int jb = jbnd ? bnd[j] : NO_BOUNDARY;
-  compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
+  if (!learned_flux<R, MODE>(P, S, lb, f, slot, 0, wij, Wi, Wj, jb, nr, psi, Bn, flux, dt * area, dt * area, i, j)) {
+    fcode[f] = code;  // deferred to the network; the contribution is written by the finishing pass
+    return;
+  }
   const double tarea = dt * area;
   R *o = fcon + 14 * (size_t)f;
 #pragma unroll
@@ -1330,14 +1389,22 @@ __global__ void k_wst(int n, const unsigned char *__restrict__ act, const double
 }
 
 // ---- compute_update0 face pass (MPI/compute_update.cpp:713-810) ----------
-template <typename R>
+template <typename R, int MODE>
 __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Params P,
     const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
     const unsigned char *__restrict__ fflag, const int *__restrict__ bnd,
     const double *__restrict__ vel, const R *__restrict__ Wst,
-    R *__restrict__ fcon, unsigned char *__restrict__ fcode) {
-  const int f = blockIdx.x * blockDim.x + threadIdx.x;
-  if (f >= nf) return;
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode, const Sched *__restrict__ S, const int *__restrict__ rung,
+    LearnBuf lb) {
+  int f = blockIdx.x * blockDim.x + threadIdx.x;
+  int slot = -1;
+  if (MODE == LM_FINISH) {
+    if (f >= *lb.count) return;
+    slot = f;
+    f = lb.gface[slot];
+  } else if (f >= nf) {
+    return;
+  }
   const unsigned char ff = fflag[f];
   if (!(ff & FF_ACTIVE)) { fcode[f] = F_OFF; return; }
   const int2 e = s12[f];
@@ -1370,7 +1437,15 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Par
                     R((vj[2] + vi[2]) * 0.5 + dri[2] * ids2)};
   const R nr[3] = {R(nrm[0]), R(nrm[1]), R(nrm[2])};
   R psi, Bn, flux[NF];
-  compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
+  {
+    // positivity horizon of each side: its own step dt(rung)
+    const double ai = MODE == LM_FINISH ? area * get_dt(P, rung[i]) : 0.0;
+    const double aj = MODE == LM_FINISH ? area * get_dt(P, rung[j]) : 0.0;
+    if (!learned_flux<R, MODE>(P, S, lb, f, slot, 1, wij, Wi, Wj, jb, nr, psi, Bn, flux, ai, aj, i, j)) {
+      fcode[f] = code;
+      return;
+    }
+  }
   R *o = fcon + 14 * (size_t)f;
 #pragma unroll
   for (int k = 0; k < NF; k++) o[k] = R(double(flux[k]) * area);
@@ -1785,6 +1860,15 @@ struct fvm_ctx {
   // one captured step per mode (shared / individual), replayed by fvm_run
   cudaGraphExec_t graph[2];
   Sched hS;  // host copy of the device scheduler, refreshed after synchronisation
+  // learned flux network: BF16 weight image and FP32 biases
+  unsigned char *mlp_img = nullptr;
+  float *mlp_bias = nullptr;
+  int *mlp_err = nullptr;
+  float *mlp_param = nullptr;  // FP32 master parameters
+  // learned-flux mode: 0 exact, 1 network on gated faces, 2 exact + harvest
+  int learn_mode = 0;
+  LearnBuf lb{};
+  float h_norm[48];  // standardisation of the network's inputs and outputs (fvm_mlp_set_norm)
   std::string err;
 };
 
@@ -1887,6 +1971,8 @@ fvm_ctx *fvm_create(const fvm_params *p, int device) {
   if (!p) return nullptr;
   fvm_ctx *c = new fvm_ctx();
   c->device = device;
+  for (int k = 0; k < 48; k++)  // identity standardisation until fvm_mlp_set_norm
+    c->h_norm[k] = (k < 16 || (k >= 32 && k < 40)) ? 0.0f : 1.0f;
   c->prm = *p;
   memset(&c->d, 0, sizeof(Dev));
   c->P.gamma = p->gamma;
@@ -1921,6 +2007,10 @@ void fvm_destroy(fvm_ctx *c) {
   cudaStreamSynchronize(c->st);
   drop_graphs(c);
   free_all(c);
+  if (c->mlp_img) cudaFree(c->mlp_img);
+  if (c->mlp_bias) cudaFree(c->mlp_bias);
+  if (c->mlp_err) cudaFree(c->mlp_err);
+  if (c->mlp_param) cudaFree(c->mlp_param);
   for (int k = 0; k < 2 * KT_COUNT; k++) cudaEventDestroy(c->kev[k]);
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
@@ -1951,6 +2041,8 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   CK(cudaSetDevice(c->device));
   drop_graphs(c);
   free_all(c);
+  c->learn_mode = 0;
+  c->lb = LearnBuf{};
   c->n = ncell;
   c->nf = nface;
   c->nl = nl;
@@ -2230,12 +2322,29 @@ static int enq_limiter(fvm_ctx *c) {
   return 0;
 }
 
+static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfloat16 *X, float *Y);
+
 static int enq_update(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_CORR_FLUX);
-  BULK(k_corr_flux<R><<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd,
-                                                           d.vel, d.tlast, (const R *)d.Wrec, (const R *)d.fst,
-                                                           (R *)d.fcon, d.fcode));
+  const LearnBuf &lb = c->lb;
+#define CORR_FLUX(MODE, GRID)                                                                                   \
+  BULK(k_corr_flux<R, MODE><<<GRID, 128, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, \
+                                                     d.tlast, (const R *)d.Wrec, (const R *)d.fst, (R *)d.fcon,   \
+                                                     d.fcode, lb))
+  if (c->learn_mode == 1) {
+    CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
+    CORR_FLUX(LM_DEFER, nblk(c->nf, 128));
+    LAUNCH_CHECK();
+    int rc = mlp_launch_dev(c, c->nf, lb.count, lb.X, lb.Y);
+    if (rc) return rc;
+    CORR_FLUX(LM_FINISH, nblk(c->nf, 128));
+  } else if (c->learn_mode == 2) {
+    CORR_FLUX(LM_HARVEST, nblk(c->nf, 128));
+  } else {
+    CORR_FLUX(LM_EXACT, nblk(c->nf, 128));
+  }
+#undef CORR_FLUX
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_FLUX);
   kt_begin(c, KT_CORR_CELL);
@@ -2326,8 +2435,24 @@ static int enq_collect(fvm_ctx *c) {
 static int enq_update0(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_FLUX);
-  BULK(k_pred_flux<R><<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd,
-                                                           d.vel, (const R *)d.Wst, (R *)d.fcon2, d.fcode2));
+  const LearnBuf &lb = c->lb;
+#define PRED_FLUX(MODE)                                                                                       \
+  BULK(k_pred_flux<R, MODE><<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
+                                                                 d.vel, (const R *)d.Wst, (R *)d.fcon2, d.fcode2, \
+                                                                 d.S, d.rung, lb))
+  if (c->learn_mode == 1) {
+    CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
+    PRED_FLUX(LM_DEFER);
+    LAUNCH_CHECK();
+    int rc = mlp_launch_dev(c, c->nf, lb.count, lb.X, lb.Y);
+    if (rc) return rc;
+    PRED_FLUX(LM_FINISH);
+  } else if (c->learn_mode == 2) {
+    PRED_FLUX(LM_HARVEST);
+  } else {
+    PRED_FLUX(LM_EXACT);
+  }
+#undef PRED_FLUX
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_FLUX);
   return 0;
@@ -2821,6 +2946,327 @@ int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const doub
   CK(cudaMemcpyAsync(psi, dp, sizeof(double) * nf, cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(Bn, dB, sizeof(double) * nf, cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(flux, dF, sizeof(double) * 10 * nf, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+}  // extern "C"
+
+// ============================ learned flux network ============================
+
+// The network on n rows (or on *n_dev rows, at most nmax, counted on the
+// device): persistent CTAs, two per SM (shared memory allows two).
+static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfloat16 *X, float *Y) {
+  if (nmax <= 0) return 0;
+  static bool attr_set = false;
+  if (!attr_set) {
+    CK(cudaFuncSetAttribute(mlp::k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SMEM_BYTES));
+    attr_set = true;
+  }
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
+  const int ntiles = (nmax + mlp::TILE - 1) / mlp::TILE;
+  const int grid = ntiles < 2 * nsm ? ntiles : 2 * nsm;
+  mlp::k_mlp_infer<<<grid, mlp::THREADS, mlp::SMEM_BYTES, c->st>>>(nmax, n_dev, X, Y, (const uint4 *)c->mlp_img,
+                                                          c->mlp_bias, c->mlp_err);
+  LAUNCH_CHECK();
+  return 0;
+}
+
+static int mlp_launch(fvm_ctx *c, int n, const __nv_bfloat16 *X, float *Y) {
+  return mlp_launch_dev(c, n, nullptr, X, Y);
+}
+
+extern "C" {
+
+int fvm_mlp_set_weights(fvm_ctx *c, const float *params) {
+  if (!c || !params) return FVM_EINVAL;
+  CK(cudaSetDevice(c->device));
+  if (!c->mlp_img) {
+    CK(cudaMalloc(&c->mlp_img, mlp::IMG_BYTES));
+    CK(cudaMalloc(&c->mlp_bias, mlp::NBIAS * sizeof(float)));
+    CK(cudaMalloc(&c->mlp_err, sizeof(int)));
+    CK(cudaMalloc(&c->mlp_param, mlp::NPARAM * sizeof(float)));
+    CK(cudaMemsetAsync(c->mlp_err, 0, sizeof(int), c->st));
+  }
+  CK(cudaMemcpyAsync(c->mlp_param, params, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  mlp::k_mlp_pack<<<(mlp::NH * mlp::NH + 255) / 256, 256, 0, c->st>>>(c->mlp_param, c->mlp_img, c->mlp_bias);
+  LAUNCH_CHECK();
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int fvm_mlp_get_weights(fvm_ctx *c, float *params) {
+  if (!c || !params) return FVM_EINVAL;
+  if (!c->mlp_param) { c->err = "fvm_mlp_get_weights: no weights"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(params, c->mlp_param, mlp::NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// ---- training: forward + backward of one batch of `rows` rows ---------------
+struct MlpWork {
+  int rows = 0;
+  float *X, *T, *Z1, *Z2, *Z3, *Z4, *A1, *A2, *A3, *G, *dA, *dB, *grad, *loss, *wt, *m, *v;
+  void *base = nullptr;
+};
+
+static int mlp_work(fvm_ctx *c, MlpWork &w, int rows) {
+  using namespace mlp;
+  const size_t nf = (size_t)rows * (NIN + NOUT + 3 * NH + NOUT + 3 * NH + NOUT + 2 * NH) + 3 * (size_t)NPARAM + 1 + NOUT;
+  CK(cudaMallocAsync(&w.base, nf * sizeof(float), c->st));
+  CK(cudaMemsetAsync(w.base, 0, nf * sizeof(float), c->st));
+  float *p = (float *)w.base;
+  auto take = [&](size_t k) { float *q = p; p += k; return q; };
+  w.rows = rows;
+  w.X = take((size_t)rows * NIN); w.T = take((size_t)rows * NOUT);
+  w.Z1 = take((size_t)rows * NH); w.Z2 = take((size_t)rows * NH); w.Z3 = take((size_t)rows * NH);
+  w.Z4 = take((size_t)rows * NOUT);
+  w.A1 = take((size_t)rows * NH); w.A2 = take((size_t)rows * NH); w.A3 = take((size_t)rows * NH);
+  w.G = take((size_t)rows * NOUT); w.dA = take((size_t)rows * NH); w.dB = take((size_t)rows * NH);
+  w.grad = take(NPARAM); w.m = take(NPARAM); w.v = take(NPARAM); w.loss = take(1); w.wt = take(NOUT);
+  return 0;
+}
+
+static void gemm(cudaStream_t s, int M, int N, int K, const float *A, long long sam, long long sak, const float *B,
+                 long long sbk, long long sbn, float *C, int ldc) {
+  dim3 grid((N + mlpt::GT - 1) / mlpt::GT, (M + mlpt::GT - 1) / mlpt::GT);
+  mlpt::k_gemm<<<grid, 128, 0, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, 0);
+}
+
+// Loss (added to *w.loss) and gradient (w.grad) of the batch in w.X / w.T at
+// the parameters P.
+static int mlp_fwd_bwd(fvm_ctx *c, MlpWork &w, const float *P) {
+  using namespace mlp;
+  const int B = w.rows;
+  cudaStream_t s = c->st;
+  const float *W1 = P, *b1 = W1 + NH * NIN, *W2 = b1 + NH, *b2 = W2 + NH * NH, *W3 = b2 + NH, *b3 = W3 + NH * NH,
+              *W4 = b3 + NH, *b4 = W4 + NOUT * NH;
+  float *g = w.grad;
+  float *gW1 = g, *gb1 = gW1 + NH * NIN, *gW2 = gb1 + NH, *gb2 = gW2 + NH * NH, *gW3 = gb2 + NH,
+        *gb3 = gW3 + NH * NH, *gW4 = gb3 + NH, *gb4 = gW4 + NOUT * NH;
+  const long long nh = (long long)B * NH;
+  const unsigned eb = (unsigned)((nh + 255) / 256);
+  // forward
+  gemm(s, B, NH, NIN, w.X, NIN, 1, W1, 1, NIN, w.Z1, NH);
+  mlpt::k_bias_gelu<<<eb, 256, 0, s>>>(B, NH, w.Z1, b1, w.A1);
+  gemm(s, B, NH, NH, w.A1, NH, 1, W2, 1, NH, w.Z2, NH);
+  mlpt::k_bias_gelu<<<eb, 256, 0, s>>>(B, NH, w.Z2, b2, w.A2);
+  gemm(s, B, NH, NH, w.A2, NH, 1, W3, 1, NH, w.Z3, NH);
+  mlpt::k_bias_gelu<<<eb, 256, 0, s>>>(B, NH, w.Z3, b3, w.A3);
+  gemm(s, B, NOUT, NH, w.A3, NH, 1, W4, 1, NH, w.Z4, NOUT);
+  mlpt::k_out_loss<<<(B * NOUT + 255) / 256, 256, 0, s>>>(B, w.Z4, b4, w.T, w.wt, w.G, w.loss);
+  // backward
+  gemm(s, NOUT, NH, B, w.G, 1, NOUT, w.A3, NH, 1, gW4, NH);
+  mlpt::k_colsum<<<1, 32, 0, s>>>(B, NOUT, w.G, gb4);
+  gemm(s, B, NH, NOUT, w.G, NOUT, 1, W4, NH, 1, w.dA, NH);
+  mlpt::k_gelu_back<<<eb, 256, 0, s>>>(nh, w.dA, w.Z3);
+  gemm(s, NH, NH, B, w.dA, 1, NH, w.A2, NH, 1, gW3, NH);
+  mlpt::k_colsum<<<1, NH, 0, s>>>(B, NH, w.dA, gb3);
+  gemm(s, B, NH, NH, w.dA, NH, 1, W3, NH, 1, w.dB, NH);
+  mlpt::k_gelu_back<<<eb, 256, 0, s>>>(nh, w.dB, w.Z2);
+  gemm(s, NH, NH, B, w.dB, 1, NH, w.A1, NH, 1, gW2, NH);
+  mlpt::k_colsum<<<1, NH, 0, s>>>(B, NH, w.dB, gb2);
+  gemm(s, B, NH, NH, w.dB, NH, 1, W2, NH, 1, w.dA, NH);
+  mlpt::k_gelu_back<<<eb, 256, 0, s>>>(nh, w.dA, w.Z1);
+  gemm(s, NH, NIN, B, w.dA, 1, NH, w.X, NIN, 1, gW1, NIN);
+  mlpt::k_colsum<<<1, NH, 0, s>>>(B, NH, w.dA, gb1);
+  c->launches += 21;
+  CK(cudaGetLastError());
+  return 0;
+}
+
+static int mlp_set_wt(fvm_ctx *c, MlpWork &w, const float *wt) {
+  float h[mlp::NOUT];
+  for (int k = 0; k < mlp::NOUT; k++) h[k] = wt ? wt[k] : 1.0f;
+  CK(cudaMemcpyAsync(w.wt, h, sizeof(h), cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));  // h is on the stack
+  return 0;
+}
+
+int fvm_mlp_grad(fvm_ctx *c, int n, const float *X, const float *T, const float *wt, float *grad, float *loss) {
+  if (!c || n <= 0 || !X || !T || !grad || !loss) return FVM_EINVAL;
+  if (!c->mlp_param) { c->err = "fvm_mlp_grad: no weights"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  MlpWork w;
+  int rc = mlp_work(c, w, n);
+  if (rc) return rc;
+  if ((rc = mlp_set_wt(c, w, wt))) return rc;
+  CK(cudaMemcpyAsync(w.X, X, (size_t)n * mlp::NIN * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(w.T, T, (size_t)n * mlp::NOUT * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  if ((rc = mlp_fwd_bwd(c, w, c->mlp_param))) return rc;
+  CK(cudaMemcpyAsync(grad, w.grad, mlp::NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(loss, w.loss, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaFreeAsync(w.base, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int fvm_mlp_train(fvm_ctx *c, long long n, const float *X, const float *T, const float *wt, int batch, int steps,
+                  float lr, unsigned long long seed, float *loss_out) {
+  if (!c || n <= 0 || !X || !T || batch <= 0 || steps < 0 || !(lr > 0.0f)) return FVM_EINVAL;
+  if (!c->mlp_param) { c->err = "fvm_mlp_train: no initial weights"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  MlpWork w;
+  int rc = mlp_work(c, w, batch);
+  if (rc) return rc;
+  if ((rc = mlp_set_wt(c, w, wt))) return rc;
+  float *dX = nullptr, *dT = nullptr, *hist = nullptr;
+  CK(cudaMallocAsync(&dX, (size_t)n * mlp::NIN * sizeof(float), c->st));
+  CK(cudaMallocAsync(&dT, (size_t)n * mlp::NOUT * sizeof(float), c->st));
+  CK(cudaMallocAsync(&hist, (size_t)(steps > 0 ? steps : 1) * sizeof(float), c->st));
+  CK(cudaMemcpyAsync(dX, X, (size_t)n * mlp::NIN * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dT, T, (size_t)n * mlp::NOUT * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  const float b1 = 0.9f, b2 = 0.999f;
+  double p1 = 1.0, p2 = 1.0;
+  for (int it = 0; it < steps; it++) {
+    mlpt::k_gather<<<(batch + 127) / 128, 128, 0, c->st>>>(n, dX, dT, batch, seed, it, w.X, w.T);
+    CK(cudaMemsetAsync(w.loss, 0, sizeof(float), c->st));
+    if ((rc = mlp_fwd_bwd(c, w, c->mlp_param))) return rc;
+    p1 *= b1;
+    p2 *= b2;
+    mlpt::k_adam<<<(mlp::NPARAM + 255) / 256, 256, 0, c->st>>>(mlp::NPARAM, c->mlp_param, w.grad, w.m, w.v, lr, b1,
+                                                               b2, 1e-8f, (float)(1.0 - p1), (float)(1.0 - p2));
+    CK(cudaMemcpyAsync(hist + it, w.loss, sizeof(float), cudaMemcpyDeviceToDevice, c->st));
+    c->launches += 2;
+  }
+  CK(cudaGetLastError());
+  mlp::k_mlp_pack<<<(mlp::NH * mlp::NH + 255) / 256, 256, 0, c->st>>>(c->mlp_param, c->mlp_img, c->mlp_bias);
+  LAUNCH_CHECK();
+  if (loss_out && steps > 0)
+    CK(cudaMemcpyAsync(loss_out, hist, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaFreeAsync(dX, c->st));
+  CK(cudaFreeAsync(dT, c->st));
+  CK(cudaFreeAsync(hist, c->st));
+  CK(cudaFreeAsync(w.base, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int fvm_mlp_eval(fvm_ctx *c, int n, const float *X, float *Y) {
+  if (!c || n < 0 || (n > 0 && (!X || !Y))) return FVM_EINVAL;
+  if (!c->mlp_img) { c->err = "fvm_mlp_eval: no weights (fvm_mlp_set_weights)"; return FVM_EINVAL; }
+  if (n == 0) return 0;
+  CK(cudaSetDevice(c->device));
+  const size_t nx = (size_t)n * mlp::NIN, ny = (size_t)n * mlp::NOUT;
+  float *dx = nullptr, *dy = nullptr;
+  __nv_bfloat16 *db = nullptr;
+  CK(cudaMallocAsync(&dx, nx * sizeof(float), c->st));
+  CK(cudaMallocAsync(&db, nx * sizeof(__nv_bfloat16), c->st));
+  CK(cudaMallocAsync(&dy, ny * sizeof(float), c->st));
+  CK(cudaMemcpyAsync(dx, X, nx * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  mlp::k_f32_to_bf16<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>((long long)nx, dx, db);
+  LAUNCH_CHECK();
+  int rc = mlp_launch(c, n, db, dy);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(Y, dy, ny * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  int herr = 0;
+  CK(cudaMemcpyAsync(&herr, c->mlp_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaFreeAsync(dx, c->st));
+  CK(cudaFreeAsync(db, c->st));
+  CK(cudaFreeAsync(dy, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (herr) { c->err = "fvm_mlp_eval: tensor-core pipeline wait timed out"; return FVM_ECUDA; }
+  return 0;
+}
+
+}  // extern "C"
+
+extern "C" {
+
+int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, int judge, int hstride,
+                      long long hcap) {
+  if (!c || mode < 0 || mode > 2 || judge < 0 || hstride < 1 || hcap < 0) return FVM_EINVAL;
+  if (!c->have_mesh) { c->err = "fvm_set_flux_mode: no mesh"; return FVM_ENOMESH; }
+  if (mode == 1 && !c->mlp_img) { c->err = "fvm_set_flux_mode: no network weights"; return FVM_EINVAL; }
+  if (!(drho >= 0.0f) || !(dp >= 0.0f) || !(mach >= 0.0f)) { c->err = "fvm_set_flux_mode: bad gate"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  drop_graphs(c);
+  Dev &d = c->d;
+  const size_t nf = (size_t)(c->nf > 0 ? c->nf : 1);
+  int rc = 0;
+  if (!d.lX) {
+    rc |= dalloc_bytes(c, &d.lX, nf * 16 * sizeof(__nv_bfloat16));
+    rc |= dalloc_bytes(c, &d.lY, nf * 8 * sizeof(float));
+    rc |= dalloc_bytes(c, &d.lface, nf * sizeof(int));
+    rc |= dalloc_bytes(c, &d.lcount, sizeof(int));
+    rc |= dalloc_bytes(c, &d.lstats, LSTAT_COUNT * sizeof(double));
+    rc |= dalloc_bytes(c, &d.lhcount, sizeof(unsigned long long));
+    rc |= dalloc_bytes(c, &d.lnorm, 48 * sizeof(float));
+  }
+  if (mode == 2 && hcap > c->lb.hcap) {
+    rc |= dalloc_bytes(c, &d.lhx, (size_t)hcap * 16 * sizeof(float));
+    rc |= dalloc_bytes(c, &d.lhy, (size_t)hcap * 8 * sizeof(float));
+  }
+  if (rc) return FVM_ENOMEM;
+  LearnBuf &lb = c->lb;
+  lb.X = (__nv_bfloat16 *)d.lX;
+  lb.Y = (float *)d.lY;
+  lb.gface = (int *)d.lface;
+  lb.count = (int *)d.lcount;
+  lb.stats = (double *)d.lstats;
+  lb.hcount = (unsigned long long *)d.lhcount;
+  if (mode == 2 && hcap > lb.hcap) {
+    lb.hx = (float *)d.lhx;
+    lb.hy = (float *)d.lhy;
+    lb.hcap = hcap;
+  }
+  lb.hstride = (unsigned)hstride;
+  lb.judge = (unsigned)judge;
+  lb.U = d.U;
+  lb.norm = (const float *)d.lnorm;
+  CK(cudaMemcpy(d.lnorm, c->h_norm, sizeof(c->h_norm), cudaMemcpyHostToDevice));
+  lb.drho = drho;
+  lb.dp = dp;
+  lb.mach = mach;
+  CK(cudaMemsetAsync(lb.stats, 0, LSTAT_COUNT * sizeof(double), c->st));
+  CK(cudaMemsetAsync(lb.hcount, 0, sizeof(unsigned long long), c->st));
+  CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->learn_mode = mode;
+  return 0;
+}
+
+int fvm_mlp_set_norm(fvm_ctx *c, const float *mu_x, const float *sd_x, const float *mu_y, const float *sd_y) {
+  if (!c || !mu_x || !sd_x || !mu_y || !sd_y) return FVM_EINVAL;
+  for (int k = 0; k < 16; k++)
+    if (!(sd_x[k] > 0.0f)) { c->err = "fvm_mlp_set_norm: feature spreads must be positive"; return FVM_EINVAL; }
+  for (int k = 0; k < 16; k++) { c->h_norm[k] = mu_x[k]; c->h_norm[16 + k] = 1.0f / sd_x[k]; }
+  for (int k = 0; k < 8; k++) { c->h_norm[32 + k] = mu_y[k]; c->h_norm[40 + k] = sd_y[k]; }
+  if (c->d.lnorm) {
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaMemcpy(c->d.lnorm, c->h_norm, sizeof(c->h_norm), cudaMemcpyHostToDevice));
+  }
+  return 0;
+}
+
+int fvm_learn_stats(fvm_ctx *c, double *stats) {
+  if (!c || !stats) return FVM_EINVAL;
+  if (!c->lb.stats) { for (int k = 0; k < LSTAT_COUNT; k++) stats[k] = 0.0; return 0; }
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(stats, c->lb.stats, LSTAT_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+long long fvm_harvest_count(fvm_ctx *c) {
+  if (!c || !c->lb.hcount) return 0;
+  unsigned long long h = 0;
+  if (cudaMemcpyAsync(&h, c->lb.hcount, sizeof(h), cudaMemcpyDeviceToHost, c->st) != cudaSuccess) return -1;
+  if (cudaStreamSynchronize(c->st) != cudaSuccess) return -1;
+  return (long long)(h < (unsigned long long)c->lb.hcap ? h : (unsigned long long)c->lb.hcap);
+}
+
+int fvm_get_harvest(fvm_ctx *c, long long n, float *X, float *Y) {
+  if (!c || n < 0 || (n > 0 && (!X || !Y))) return FVM_EINVAL;
+  if (n > c->lb.hcap) { c->err = "fvm_get_harvest: more rows than harvested"; return FVM_ERANGE; }
+  if (n == 0) return 0;
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(X, c->lb.hx, (size_t)n * 16 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(Y, c->lb.hy, (size_t)n * 8 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   return 0;
 }

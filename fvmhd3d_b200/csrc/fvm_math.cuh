@@ -219,9 +219,26 @@ __device__ __forceinline__ void riemann_hlld(T gamma, T *flux, T Bx, T w, T dens
 // ---- rotated-frame face flux (MPI/compute_update.cpp:973-1095) -----------
 // Wi/Wj primitive face states, normal the unit normal i->j, wij the face
 // velocity.  Returns the 10 lab-frame fluxes, psi_ij and Bn_ij.
-template <typename T>
-__device__ __forceinline__ void compute_flux(const Params &P, const T *wij, const T *Wi, const T *Wj,
-                                             int jbnd, const T *normal, T &psi_ij, T &Bn_ij, T *flux) {
+// The exact Riemann solver as a compute_flux hook.
+struct HlldSolver {
+  template <typename T>
+  __device__ __forceinline__ bool operator()(T gamma, T *F, T Bx, T w, T dens_L, T pres_L, T ethm_L, T velx_L,
+                                             T vely_L, T velz_L, T By_L, T Bz_L, T dens_R, T pres_R, T ethm_R,
+                                             T velx_R, T vely_R, T velz_R, T By_R, T Bz_R, T chL, T chR,
+                                             int jbnd) {
+    riemann_hlld<T>(gamma, F, Bx, w, dens_L, pres_L, ethm_L, velx_L, vely_L, velz_L, By_L, Bz_L, dens_R, pres_R,
+                    ethm_R, velx_R, vely_R, velz_R, By_R, Bz_R);
+    return true;
+  }
+};
+
+// compute_flux with the rotated-frame Riemann solve delegated to `solve`
+// (which may decline: then nothing after psi_ij / Bn_ij is computed and
+// false is returned).
+template <typename T, typename Solver>
+__device__ __forceinline__ bool compute_flux_with(const Params &P, const T *wij, const T *Wi, const T *Wj,
+                                                  int jbnd, const T *normal, T &psi_ij, T &Bn_ij, T *flux,
+                                                  Solver &solve) {
   const T gamma = T(P.gamma);
   const T ex = normal[0], ey = normal[1], ez = normal[2];
   const T ds = sqrt(ex * ex + ey * ey);
@@ -259,8 +276,9 @@ __device__ __forceinline__ void compute_flux(const Params &P, const T *wij, cons
   Bn_ij = (Bx_L * chL + Bx_R * chR + (psiL - psiR)) * ich;
   psi_ij = (psiL * chR + psiR * chL + chR * chL * (Bx_L - Bx_R)) * ich;
   T F[8];
-  riemann_hlld<T>(gamma, F, Bn_ij, wn_ij, dens_L, pres_L, ethm_L, velx_L, vely_L, velz_L, By_L, Bz_L,
-                  dens_R, pres_R, ethm_R, velx_R, vely_R, velz_R, By_R, Bz_R);
+  if (!solve(gamma, F, Bn_ij, wn_ij, dens_L, pres_L, ethm_L, velx_L, vely_L, velz_L, By_L, Bz_L, dens_R, pres_R,
+             ethm_R, velx_R, vely_R, velz_R, By_R, Bz_R, chL, chR, jbnd))
+    return false;
   // back-rotation with the transpose of A
   flux[MASS] = F[MASS];
   flux[ENER] = F[ENER];
@@ -272,6 +290,14 @@ __device__ __forceinline__ void compute_flux(const Params &P, const T *wij, cons
   flux[WBZ] = Axz * F[WBX] + Azz * F[WBZ];
   flux[MPSI] = F[MASS] * (F[MASS] > T(0) ? psiL : psiR);
   flux[MENTR] = F[MASS] * (F[MASS] > T(0) ? entrL : entrR);
+  return true;
+}
+
+template <typename T>
+__device__ __forceinline__ void compute_flux(const Params &P, const T *wij, const T *Wi, const T *Wj,
+                                             int jbnd, const T *normal, T &psi_ij, T &Bn_ij, T *flux) {
+  HlldSolver exact;
+  compute_flux_with<T>(P, wij, Wi, Wj, jbnd, normal, psi_ij, Bn_ij, flux, exact);
 }
 
 // ---- limiter (MPI/compute_reconstruction.cpp:5-22) -----------------------

@@ -23,6 +23,7 @@ import numpy as np
 from . import _lib
 from .mesh import Mesh
 
+MLP_NPARAM = 36232
 FVM_PREC_FP64 = 0
 FVM_PREC_FP32 = 1
 
@@ -175,6 +176,79 @@ class System:
         v = [ctypes.c_int(0) for _ in range(3)]
         self._check(self.L.fvm_last_adjust_stats(self.h, *[ctypes.byref(x) for x in v]), "fvm_last_adjust_stats")
         return tuple(x.value for x in v)
+
+    # -- learned face flux ---------------------------------------------------
+    def mlp_set_weights(self, params) -> None:
+        """Network parameters (FVM_MLP_NPARAM floats, order of
+        fvmhd3d_b200.learned.unpack)."""
+        p = np.ascontiguousarray(params, np.float32).ravel()
+        if p.size != MLP_NPARAM:
+            raise ValueError(f"expected {MLP_NPARAM} parameters, got {p.size}")
+        self._check(self.L.fvm_mlp_set_weights(self.h, _p(p)), "fvm_mlp_set_weights")
+
+    def mlp_eval(self, X) -> np.ndarray:
+        """Network outputs (n x 8) for inputs X (n x 16) on the tensor cores."""
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.zeros((X.shape[0], 8), np.float32)
+        self._check(self.L.fvm_mlp_eval(self.h, X.shape[0], _p(X), _p(Y)), "fvm_mlp_eval")
+        return Y
+
+    def set_flux_mode(self, mode, drho=0.05, dp=0.05, mach=1.0, judge=1024, hstride=1, hcap=0) -> None:
+        """Learned-flux mode of the flux passes: 0 exact, 1 network on gated
+        faces, 2 exact with harvesting (see fvm_set_flux_mode)."""
+        self._check(self.L.fvm_set_flux_mode(self.h, int(mode), ctypes.c_float(drho), ctypes.c_float(dp),
+                                             ctypes.c_float(mach), int(judge), int(hstride), int(hcap)),
+                    "fvm_set_flux_mode")
+
+    def mlp_set_norm(self, mu_x, sd_x, mu_y, sd_y) -> None:
+        """Standardisation of the network's inputs and outputs."""
+        a = [np.ascontiguousarray(v, np.float32).ravel() for v in (mu_x, sd_x, mu_y, sd_y)]
+        self._check(self.L.fvm_mlp_set_norm(self.h, *[_p(v) for v in a]), "fvm_mlp_set_norm")
+
+    def learn_stats(self) -> dict:
+        s = np.zeros(8)
+        self._check(self.L.fvm_learn_stats(self.h, _p(s)), "fvm_learn_stats")
+        return {"deferred": int(s[0]), "fallback": int(s[1]), "judged": int(s[2]),
+                "judged_rel_l1": float(s[3] / s[4]) if s[4] > 0 else 0.0,
+                "judged_mean_abs": float(s[3] / (8 * s[2])) if s[2] > 0 else 0.0, "judged_max_abs": float(s[5])}
+
+    def harvest(self):
+        """(X, Y) pairs harvested in mode 2 so far."""
+        n = int(self.L.fvm_harvest_count(self.h))
+        if n < 0:
+            raise FvmError("fvm_harvest_count failed")
+        X = np.zeros((n, 16), np.float32)
+        Y = np.zeros((n, 8), np.float32)
+        self._check(self.L.fvm_get_harvest(self.h, n, _p(X), _p(Y)), "fvm_get_harvest")
+        return X, Y
+
+    def mlp_get_weights(self) -> np.ndarray:
+        out = np.zeros(MLP_NPARAM, np.float32)
+        self._check(self.L.fvm_mlp_get_weights(self.h, _p(out)), "fvm_mlp_get_weights")
+        return out
+
+    def mlp_grad(self, X, T, wt=None):
+        """(loss, gradient) of the mean-squared loss at the current parameters,
+        from the training kernels."""
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        w = None if wt is None else np.ascontiguousarray(wt, np.float32)
+        g = np.zeros(MLP_NPARAM, np.float32)
+        loss = ctypes.c_float(0.0)
+        self._check(self.L.fvm_mlp_grad(self.h, X.shape[0], _p(X), _p(T), _p(w), _p(g), ctypes.byref(loss)),
+                    "fvm_mlp_grad")
+        return float(loss.value), g
+
+    def mlp_train(self, X, T, wt=None, batch=4096, steps=1000, lr=1e-3, seed=1) -> np.ndarray:
+        """Adam training on the GPU from the current parameters; returns the
+        minibatch losses."""
+        X = np.ascontiguousarray(X, np.float32)
+        T = np.ascontiguousarray(T, np.float32)
+        w = None if wt is None else np.ascontiguousarray(wt, np.float32)
+        hist = np.zeros(max(steps, 1), np.float32)
+        self._check(self.L.fvm_mlp_train(self.h, X.shape[0], _p(X), _p(T), _p(w), int(batch), int(steps),
+                                         ctypes.c_float(lr), ctypes.c_ulonglong(seed), _p(hist)), "fvm_mlp_train")
+        return hist[:steps]
 
     def clock(self):
         """(tsysU, dt_global, iteration): the scheduler clock after the last

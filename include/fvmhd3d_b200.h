@@ -194,6 +194,63 @@ int fvm_compute_flux(fvm_ctx *c, int nface, const double *wij, const double *Wi,
 int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const double *Wi, const double *Wj,
                             const int *jbnd, const double *normal, double *psi, double *Bn, double *flux);
 
+/* ---- learned face flux (the MLP stand-in for riemann_solver) ------------- */
+
+/* Network 16 -> 128 -> 128 -> 128 -> 8 with GELU hidden layers; parameters in
+ * this order, row-major, FP32: W1[128x16], b1[128], W2[128x128], b2[128],
+ * W3[128x128], b3[128], W4[8x128], b4[8].  Weights are rounded to BF16 for the
+ * tensor cores; biases stay FP32. */
+#define FVM_MLP_NPARAM 36232
+int fvm_mlp_set_weights(fvm_ctx *c, const float *params);
+
+/* Known-answer entry: Y[n x 8] = network(X[n x 16]) on the tensor cores, host
+ * buffers in and out (X rounded to BF16). */
+int fvm_mlp_eval(fvm_ctx *c, int n, const float *X, float *Y);
+
+/* The FP32 master parameters (FVM_MLP_NPARAM floats). */
+int fvm_mlp_get_weights(fvm_ctx *c, float *params);
+
+/* Loss L = mean over rows and outputs of wt[k] (Y - T)^2 and its gradient with
+ * respect to every parameter, by the training kernels' forward and backward
+ * passes over all n rows at the current parameters (wt may be NULL: 1). */
+int fvm_mlp_grad(fvm_ctx *c, int n, const float *X, const float *T, const float *wt, float *grad, float *loss);
+
+/* Trains from the current parameters with Adam (beta 0.9 / 0.999): `steps`
+ * updates on minibatches of `batch` rows drawn from the n pairs (X n x 16,
+ * T n x 8) by a seeded hash; loss_out[steps] gets each minibatch loss (may
+ * be NULL).  The tensor-core inference weights are refreshed at the end. */
+int fvm_mlp_train(fvm_ctx *c, long long n, const float *X, const float *T, const float *wt, int batch, int steps,
+                  float lr, unsigned long long seed, float *loss_out);
+
+/* Learned-flux mode of the two flux passes.  mode 0: the exact HLLD solver on
+ * every face (the default, restored by fvm_set_mesh); 1: faces that pass the
+ * gate take the network (weights from fvm_mlp_set_weights), the others the
+ * exact solver; 2: exact everywhere, and one gated face in `hstride` (hash
+ * sampled) appends its (features, targets) to a device harvest buffer of
+ * hcap rows.  Gate: ideal-gas EOS, no boundary neighbour, relative density
+ * and pressure jumps at most drho and dp, normal Mach number in the face
+ * frame at most mach.  In mode 1 a face whose network flux would move more
+ * than half of either cell's mass within its step falls back to the exact
+ * solver, and one deferred face in `judge` (0: none) is also solved exactly
+ * to record the network's error.  Resets the statistics. */
+int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, int judge, int hstride,
+                      long long hcap);
+
+/* Standardisation of the network: inputs (features - mu_x) / sd_x, outputs
+ * mu_y + sd_y * network (16, 16, 8, 8 floats; identity by default). */
+int fvm_mlp_set_norm(fvm_ctx *c, const float *mu_x, const float *sd_x, const float *mu_y, const float *sd_y);
+
+/* Cumulative learned-flux statistics since fvm_set_flux_mode: [0] deferred
+ * faces, [1] exact fallbacks, [2] judged faces, [3] sum over judged faces of
+ * the L1 error of the 8 scaled outputs, [4] sum of their L1 norms, [5] the
+ * largest single-output error. */
+int fvm_learn_stats(fvm_ctx *c, double *stats8);
+
+/* Rows harvested so far (capped at hcap), and a copy of the first n of them
+ * (X n x 16 features, Y n x 8 targets). */
+long long fvm_harvest_count(fvm_ctx *c);
+int fvm_get_harvest(fvm_ctx *c, long long n, float *X, float *Y);
+
 /* Timing helper: CUDA-event time in ms of the last fvm_step's kernels. */
 float fvm_last_step_ms(const fvm_ctx *c);
 /* The context's CUDA stream (a cudaStream_t), for callers that order their

@@ -352,6 +352,11 @@ def run_gpu(args):
         "timing": "value: CUDA events around K graph-replayed steps on the context stream; kernels/roofline: "
                   "CUDA events around each kernel of a separate profiled pass of eager steps",
     }
+    # the metric's comparison: learned flux + FP32 bulk against this plain FP64
+    # run, same mesh and steps (relative L1 error per conserved variable)
+    weights = os.path.join(ROOT, "fvmhd3d_b200", "data", "flux_mlp.npz")
+    if (not args.no_learned and shared and args.problem == "blast" and pb == 8 and os.path.exists(weights)):
+        line["learned_fp32"] = learned_leg(F, m, W, S, 100, weights, stream_of=torch.cuda.ExternalStream)
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
             line["cpu_baseline"] = cpu_leg(args.cpu_nside, args.problem, args.cpu_steps, 1)
@@ -362,6 +367,47 @@ def run_gpu(args):
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
+
+
+def learned_leg(F, m, W, plain, steps, weights, stream_of):
+    """The learned-flux + FP32 bulk path on the same mesh and initial state
+    for `steps` global steps: face-updates/s (CUDA events) and its relative
+    L1 error per conserved variable against the plain FP64 context `plain`
+    advanced by the same number of steps from the same start."""
+    import torch
+    from fvmhd3d_b200 import learned as L
+    z = np.load(weights)
+    model = {k: z[k] for k in ("params", "mu_x", "sd_x", "mu_y", "sd_y")}
+    ref = F.System(precision=F.FVM_PREC_FP64)
+    ref.set_mesh(m)
+    ref.init_problem(W)
+    ref.run(steps, shared=True)
+    s = F.System(precision=F.FVM_PREC_FP32)
+    s.set_mesh(m)
+    s.init_problem(W)
+    L.apply(s, model)
+    s.set_flux_mode(1, **L.GATE)
+    st = stream_of(s.stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(st)
+    _, faces = s.run(steps, shared=True)
+    e1.record(st)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    Ua, Ub = ref.get_state()["U"], s.get_state()["U"]
+    rel = np.abs(Ub - Ua).sum(axis=0) / np.maximum(np.abs(Ua).sum(axis=0), 1e-300)
+    stats = s.learn_stats()
+    out = {"value": faces / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+           "rel_l1_vs_plain_fp64": {"density": float(rel[0]), "energy": float(rel[4]),
+                                    "momentum": float(rel[1:4].max()), "magnetic": float(rel[5:8].max())},
+           "network_faces_fraction": stats["deferred"] / max(2 * faces, 1),
+           "fallback_fraction": stats["fallback"] / max(stats["deferred"], 1),
+           "judged_rel_l1": stats["judged_rel_l1"],
+           "dtype": "f32 bulk + bf16 network", "weights": "fvmhd3d_b200/data/flux_mlp.npz"}
+    ref.close()
+    s.close()
+    return out
 
 
 def run_reference(args):
@@ -399,6 +445,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-flux + FP32 comparison leg")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "fvm":
         args.warmup = 3

@@ -49,6 +49,15 @@ using namespace fvm;
 #define FVM_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CELL_MINB_F : FVM_CELL_MINB_D)
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
 // cell-kernel mappings: grouped (16 lanes per cell) or two threads per cell
+#ifndef FVM_CELL_LFJ
+#define FVM_CELL_LFJ 0  // cell kernels take (face, neighbour) from the link table instead of s12
+#endif
+#ifndef FVM_CELL_UNROLL
+#define FVM_CELL_UNROLL 1  // unroll factor of the cell kernels' face loops
+#endif
+#define FVM_PRAGMA(x) _Pragma(#x)
+#define FVM_CELL_LOOP_(n) FVM_PRAGMA(unroll n)
+#define FVM_CELL_LOOP FVM_CELL_LOOP_(FVM_CELL_UNROLL)
 #ifndef FVM_ADJUST_REPLAY
 #define FVM_ADJUST_REPLAY 1  // adjust_timesteps by parallel replay (sequential sweep as fallback)
 #endif
@@ -224,7 +233,7 @@ constexpr int KH = 5;  // primitives per thread in the two-threads-per-cell kern
 
 template <typename R>
 __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm) {
@@ -234,6 +243,7 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
   const int i = perm[t >> 1];
   const int k0 = (int)(t & 1) * KH;
   if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
+  const double ti = tlast[i];
   const R *ri = Wrec + 50 * (size_t)i + k0;
   R mn[KH], mx[KH], ln[KH], lq[KH], wi[KH];
 #pragma unroll
@@ -241,13 +251,22 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
   const int q0 = off[i], q1 = off[i + 1];
   bool zero = false;
   // pass 1: min/max of neighbour differences over active interior faces
+  FVM_CELL_LOOP
   for (int q = q0; q < q1; q++) {
+#if FVM_CELL_LFJ
+    const int2 fj = lfj[q];
+    const int f = fj.x, j = fj.y >= 0 ? fj.y : ~fj.y;
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE)) continue;
+    if (ff & (FF_BND1 | FF_BND2)) { zero = true; continue; }
+#else
     const int f = lnk[q];
     const unsigned char ff = fflag[f];
     if (!(ff & FF_ACTIVE)) continue;
     if (ff & (FF_BND1 | FF_BND2)) { zero = true; continue; }
     const int2 e = s12[f];
     const int j = e.x == i ? e.y : e.x;
+#endif
     const R *rj = Wrec + 50 * (size_t)j + k0;
 #pragma unroll
     for (int k = 0; k < KH; k++) {
@@ -266,14 +285,24 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
 #pragma unroll
     for (int k = 0; k < KH; k++) { gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k]; }
     // pass 2: limiter of the extrapolated difference at each active face
+    FVM_CELL_LOOP
     for (int q = q0; q < q1; q++) {
+#if FVM_CELL_LFJ
+      const int2 fj = lfj[q];
+      const int f = fj.x;
+      if (!(fflag[f] & FF_ACTIVE)) continue;
+      const bool own = fj.y >= 0;
+      const double tj = tlast[own ? fj.y : ~fj.y];
+      const double dtI = t_global - (own ? ti : tj), dtJ = t_global - (own ? tj : ti);
+#else
       const int f = lnk[q];
       if (!(fflag[f] & FF_ACTIVE)) continue;
       const int2 e = s12[f];
       const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
+      const bool own = e.x == i;
+#endif
       const double dth = 0.5 * smin(dtI, dtJ);
       const double4 g = geo[f], d = dr1[f];
-      const bool own = e.x == i;
       const double dsl = own ? 0.0 : 2.0 * d.w;
       const R dr[3] = {R(d.x - g.x * dsl), R(d.y - g.y * dsl), R(d.z - g.z * dsl)};
       const R dtt = R(own ? dtI - dth : dtJ - dth);
@@ -293,15 +322,26 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
   }
   // pass 3: the half-step extrapolated state of this cell at each active
   // interior face (MPI/compute_update.cpp:157-212), stored per face side
+  FVM_CELL_LOOP
   for (int q = q0; q < q1; q++) {
+#if FVM_CELL_LFJ
+    const int2 fj = lfj[q];
+    const int f = fj.x;
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE) || (ff & (FF_BND1 | FF_BND2))) continue;
+    const bool own = fj.y >= 0;
+    const double tj = tlast[own ? fj.y : ~fj.y];
+    const double dtI = t_global - (own ? ti : tj), dtJ = t_global - (own ? tj : ti);
+#else
     const int f = lnk[q];
     const unsigned char ff = fflag[f];
     if (!(ff & FF_ACTIVE) || (ff & (FF_BND1 | FF_BND2))) continue;
     const int2 e = s12[f];
     const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
+    const bool own = e.x == i;
+#endif
     const double dt = smin(dtI, dtJ);
     const double4 g = geo[f], d = dr1[f];
-    const bool own = e.x == i;
     const double dsl = own ? 0.0 : 2.0 * d.w;
     const R dr[3] = {R(d.x - g.x * dsl), R(d.y - g.y * dsl), R(d.z - g.z * dsl)};
     const R dtt = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
@@ -1583,7 +1623,7 @@ __global__ void __launch_bounds__(256) k_pred_cell_g(int n, Params P, const Sche
 // the updated primitives, local limiter, density positivity rescale.
 template <typename R>
 __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm) {
@@ -1608,13 +1648,23 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
   for (int k = 0; k < KH; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = R(0); }
   double sc[3] = {0.0, 0.0, 0.0};
   bool zero = false;
+  FVM_CELL_LOOP
   for (int q = q0; q < q1; q++) {
+#if FVM_CELL_LFJ
+    const int2 fj = lfj[q];
+    const int f = fj.x;
+    const bool own = fj.y >= 0;
+    const int j = own ? fj.y : ~fj.y;
+#else
     const int f = lnk[q];
     const int2 e = s12[f];
+    const bool own = e.x == c;
+    const int j = own ? e.y : e.x;
+#endif
     const double4 g = geo[f];
-    const double4 o4 = e.x == c ? dr1[f] : dr2[f];
+    const double4 o4 = own ? dr1[f] : dr2[f];
     double d[3] = {o4.x, o4.y, o4.z};
-    if (e.x == c) wrap3(P, d);
+    if (own) wrap3(P, d);
     sc[0] = sc[0] + d[0]; sc[1] = sc[1] + d[1]; sc[2] = sc[2] + d[2];
     const double area = g.w;
     const double sgn = (d[0] * g.x + d[1] * g.y + d[2] * g.z) < 0.0 ? -1.0 : 1.0;
@@ -1624,7 +1674,6 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
     const R drh[3] = {R(nrm[0] * dsh), R(nrm[1] * dsh), R(nrm[2] * dsh)};
     const R fij[3] = {R(d[0] - nrm[0] * dsh), R(d[1] - nrm[1] * dsh), R(d[2] - nrm[2] * dsh)};
     const R ia = R(idsA);
-    const int j = e.x == c ? e.y : e.x;
     if (bnd[j] != NO_BOUNDARY) { zero = true; break; }
     const R *Wj = Wst + 10 * (size_t)j + k0;
 #pragma unroll
@@ -1648,9 +1697,16 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
   R ln[KH], lq[KH];
 #pragma unroll
   for (int k = 0; k < KH; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; ln[k] = R(1); lq[k] = R(1); }
+  FVM_CELL_LOOP
   for (int q = q0; q < q1; q++) {
+#if FVM_CELL_LFJ
+    const int2 fj = lfj[q];
+    const int f = fj.x;
+    const bool own = fj.y >= 0;
+#else
     const int f = lnk[q];
     const bool own = s12[f].x == c;
+#endif
     const double4 o4 = own ? dr1[f] : dr2[f];
     double d[3] = {o4.x, o4.y, o4.z};
     if (own) wrap3(P, d);
@@ -2313,7 +2369,7 @@ static int enq_limiter(fvm_ctx *c) {
                                                           d.fflag, d.act, d.tlast, (const R *)d.Wrec, (R *)d.tau,
                                                           (R *)d.fst));
 #else
-  BULK(k_limiter<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.geo, d.dr1,
+  BULK(k_limiter<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1,
                                                               d.fflag, d.act, d.tlast, (const R *)d.Wrec,
                                                               (R *)d.tau, (R *)d.fst, d.perm));
 #endif
@@ -2478,7 +2534,7 @@ static int enq_recon(fvm_ctx *c) {
                                                         d.dr2, d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
                                                         (R *)d.Wrec));
 #else
-  BULK(k_recon<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.s12, d.geo, d.dr1, d.dr2,
+  BULK(k_recon<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
                                                             d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
                                                             (R *)d.Wrec, d.perm));
 #endif

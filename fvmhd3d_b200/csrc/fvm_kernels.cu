@@ -50,22 +50,19 @@ using namespace fvm;
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
 // cell-kernel mappings: grouped (16 lanes per cell) or two threads per cell
 #ifndef FVM_CELL_LFJ
-#define FVM_CELL_LFJ 0  // cell kernels take (face, neighbour) from the link table instead of s12
+#define FVM_CELL_LFJ 1  // cell kernels take (face, neighbour) from the link table instead of s12
 #endif
 #ifndef FVM_CELL_UNROLL
-#define FVM_CELL_UNROLL 1  // unroll factor of the cell kernels' face loops
+#define FVM_CELL_UNROLL 2  // unroll factor of the cell kernels' face loops
+#endif
+#ifndef FVM_REUSE_MINMAX
+#define FVM_REUSE_MINMAX 1  // the limiter reuses the reconstruction's neighbour min/max when every cell steps
 #endif
 #define FVM_PRAGMA(x) _Pragma(#x)
 #define FVM_CELL_LOOP_(n) FVM_PRAGMA(unroll n)
 #define FVM_CELL_LOOP FVM_CELL_LOOP_(FVM_CELL_UNROLL)
 #ifndef FVM_ADJUST_REPLAY
 #define FVM_ADJUST_REPLAY 1  // adjust_timesteps by parallel replay (sequential sweep as fallback)
-#endif
-#ifndef FVM_CELLMAP_GROUPED
-#define FVM_CELLMAP_GROUPED 0
-#endif
-#ifndef FVM_GATHER_GROUPED
-#define FVM_GATHER_GROUPED 0
 #endif
 // Thread-to-cell indirection: inside each window of CPW consecutive cells the
 // threads visit cells in order of face count, so the lanes of a warp run face
@@ -92,6 +89,7 @@ struct Sched {
                  // [6] adjust_timesteps replays, [7] 1 if the sequential sweep ran
   unsigned long long nactive_total, nfaces_total, steps;
   unsigned long long tprevU;  // tsysU before the last pull_active_list
+  int mnmx_ok;                // the last step reconstructed every cell (its min/max are current)
 };
 
 struct Dev {
@@ -106,6 +104,8 @@ struct Dev {
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
   double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
   int *aflag;               // adjust_timesteps replay flags
+  void *mnmx;               // per cell: the reconstruction's neighbour min and max (20 of the bulk type)
+  unsigned char *mz;        // per cell: the reconstruction met a boundary (the limiter is zero)
   // learned-flux buffers (fvm_set_flux_mode)
   void *lX, *lY, *lface, *lcount, *lstats, *lhx, *lhy, *lhcount, *lnorm;
   // state
@@ -236,8 +236,13 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
-    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm) {
+    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
   const double t_global = S->t_global;
+  // every cell steps and every cell was reconstructed by the last step: the
+  // neighbour min/max of pass 1 are the reconstruction's (same states, same
+  // faces, exact min/max)
+  const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if ((t >> 1) >= n) return;
   const int i = perm[t >> 1];
@@ -250,9 +255,15 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
   for (int k = 0; k < KH; k++) { mn[k] = R(0); mx[k] = R(0); ln[k] = R(1); lq[k] = R(1); wi[k] = ri[k]; }
   const int q0 = off[i], q1 = off[i + 1];
   bool zero = false;
+  if (reuse) {
+    const R *mm = mnmx + 20 * (size_t)i + k0;
+#pragma unroll
+    for (int k = 0; k < KH; k++) { mn[k] = mm[k]; mx[k] = mm[10 + k]; }
+    zero = mz[i] != 0;
+  }
   // pass 1: min/max of neighbour differences over active interior faces
   FVM_CELL_LOOP
-  for (int q = q0; q < q1; q++) {
+  for (int q = q0; q < (reuse ? q0 : q1); q++) {
 #if FVM_CELL_LFJ
     const int2 fj = lfj[q];
     const int f = fj.x, j = fj.y >= 0 ? fj.y : ~fj.y;
@@ -348,278 +359,6 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
     R *o = fst + 20 * (size_t)f + (own ? 0 : 10) + k0;
 #pragma unroll
     for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2]) + gt[k] * dtt);
-  }
-}
-
-// ---- grouped cell kernels -------------------------------------------------
-// Each cell is handled by 16 lanes: two subgroups of GL = 8 lanes, one per
-// half of the ten primitives (KV = 5 each).  Lane l of a subgroup takes the
-// cell's faces l, l+8, ..., so a cell's faces are read by 8 lanes at once; the
-// cell record is staged in shared memory and the per-face partials are
-// combined with 3-step shuffle reductions inside the subgroup.  Min/max
-// reductions are exact; sums are reassociated (a few ulps).
-constexpr int GL = 8;                 // lanes per subgroup (faces in flight per cell)
-constexpr int KV = 5;                 // primitives per subgroup
-constexpr int GTB = 256;              // threads per block
-constexpr int GCB = GTB / (2 * GL);   // cells per block
-
-template <typename T>
-__device__ __forceinline__ T gmin(T v) {
-#pragma unroll
-  for (int o = GL / 2; o > 0; o >>= 1) v = smin(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-template <typename T>
-__device__ __forceinline__ T gmax(T v) {
-#pragma unroll
-  for (int o = GL / 2; o > 0; o >>= 1) v = smax(v, __shfl_xor_sync(0xffffffffu, v, o));
-  return v;
-}
-template <typename T>
-__device__ __forceinline__ T gsum(T v) {
-#pragma unroll
-  for (int o = GL / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  return v;
-}
-// minimum of the fractions n/q (q > 0) held by the lanes of a subgroup
-template <typename T>
-__device__ __forceinline__ void gmin_frac(T &n, T &q) {
-#pragma unroll
-  for (int o = GL / 2; o > 0; o >>= 1) {
-    const T n2 = __shfl_xor_sync(0xffffffffu, n, o), q2 = __shfl_xor_sync(0xffffffffu, q, o);
-    if (n2 * q < n * q2) { n = n2; q = q2; }
-  }
-}
-__device__ __forceinline__ unsigned group_mask() {  // the 16 lanes of this cell
-  return 0xffffu << ((threadIdx.x & 31) & 16);
-}
-__device__ __forceinline__ bool gany(bool v) {      // any lane of this cell
-  return (__ballot_sync(0xffffffffu, v) & group_mask()) != 0;
-}
-
-// slope_limiter (MPI/compute_reconstruction.cpp:201-602): pass 1 min/max of
-// neighbour differences, pass 2 limiter minimum of the extrapolated
-// difference, pass 3 the half-step extrapolated face states.
-template <typename R>
-__global__ void __launch_bounds__(GTB) k_limiter_g(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
-    const unsigned char *__restrict__ act, const double *__restrict__ tlast,
-    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst) {
-  __shared__ R sh[GCB][50];
-  const double t_global = S->t_global;
-  const int g = threadIdx.x / (2 * GL), k0 = ((threadIdx.x / GL) & 1) * KV, l = threadIdx.x % GL;
-  const int c = blockIdx.x * GCB + g;
-  const bool valid = c < n && (act[c] & (A_ACTIVE | A_LNGB));
-  R *rec = sh[g];
-  if (valid)
-    for (int k = threadIdx.x % (2 * GL); k < 50; k += 2 * GL) rec[k] = Wrec[50 * (size_t)c + k];
-  __syncthreads();
-  const int q0 = valid ? off[c] : 0, q1 = valid ? off[c + 1] : 0;
-  R mn[KV], mx[KV];
-#pragma unroll
-  for (int k = 0; k < KV; k++) { mn[k] = R(0); mx[k] = R(0); }
-  bool zero = false;
-  for (int q = q0 + l; q < q1; q += GL) {
-    const int f = lnk[q];
-    const unsigned char ff = fflag[f];
-    if (!(ff & FF_ACTIVE)) continue;
-    if (ff & (FF_BND1 | FF_BND2)) { zero = true; continue; }
-    const int2 e = s12[f];
-    const int j = e.x == c ? e.y : e.x;
-    const R *rj = Wrec + 50 * (size_t)j + k0;
-#pragma unroll
-    for (int k = 0; k < KV; k++) {
-      const R diff = rj[k] - rec[k0 + k];
-      mn[k] = smin(mn[k], diff);
-      mx[k] = smax(mx[k], diff);
-    }
-  }
-  zero = gany(zero);
-#pragma unroll
-  for (int k = 0; k < KV; k++) { mn[k] = gmin(mn[k]); mx[k] = gmax(mx[k]); }
-  R ln[KV], lq[KV];
-#pragma unroll
-  for (int k = 0; k < KV; k++) { ln[k] = R(1); lq[k] = R(1); }
-  if (!zero) {
-    for (int q = q0 + l; q < q1; q += GL) {
-      const int f = lnk[q];
-      if (!(fflag[f] & FF_ACTIVE)) continue;
-      const int2 e = s12[f];
-      const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
-      const double dth = 0.5 * smin(dtI, dtJ);
-      const double4 gg = geo[f], d = dr1[f];
-      const bool own = e.x == c;
-      const double dsl = own ? 0.0 : 2.0 * d.w;
-      const R dr[3] = {R(d.x - gg.x * dsl), R(d.y - gg.y * dsl), R(d.z - gg.z * dsl)};
-      const R dtt = R(own ? dtI - dth : dtJ - dth);
-#pragma unroll
-      for (int k = 0; k < KV; k++) {
-        const R dWx = rec[10 + k0 + k] * dr[0] + rec[20 + k0 + k] * dr[1] + rec[30 + k0 + k] * dr[2];
-        const R dW = dWx + rec[40 + k0 + k] * dtt;
-        limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
-      }
-    }
-  }
-  R tk[KV];
-#pragma unroll
-  for (int k = 0; k < KV; k++) {
-    gmin_frac(ln[k], lq[k]);
-    tk[k] = zero ? R(0) : ln[k] / lq[k];
-  }
-  if (valid) {
-#pragma unroll
-    for (int k = 0; k < KV; k++)
-      if (k == l) tau[10 * (size_t)c + k0 + k] = tk[k];
-  }
-  for (int q = q0 + l; q < q1; q += GL) {
-    const int f = lnk[q];
-    const unsigned char ff = fflag[f];
-    if (!(ff & FF_ACTIVE) || (ff & (FF_BND1 | FF_BND2))) continue;
-    const int2 e = s12[f];
-    const double dtI = t_global - tlast[e.x], dtJ = t_global - tlast[e.y];
-    const double dt = smin(dtI, dtJ);
-    const double4 gg = geo[f], d = dr1[f];
-    const bool own = e.x == c;
-    const double dsl = own ? 0.0 : 2.0 * d.w;
-    const R dr[3] = {R(d.x - gg.x * dsl), R(d.y - gg.y * dsl), R(d.z - gg.z * dsl)};
-    const R dtt = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
-    R *o = fst + 20 * (size_t)f + (own ? 0 : 10) + k0;
-#pragma unroll
-    for (int k = 0; k < KV; k++) {
-      const R t = tk[k];
-      const int kk = k0 + k;
-      o[k] = rec[kk] + (((rec[10 + kk] * t) * dr[0] + (rec[20 + kk] * t) * dr[1] + (rec[30 + kk] * t) * dr[2]) +
-                        (rec[40 + kk] * t) * dtt);
-    }
-  }
-}
-
-// compute_reconstruction (MPI/compute_reconstruction.cpp:41-198): Voronoi
-// face gradient, local limiter, density positivity, per active cell.
-template <typename R>
-__global__ void __launch_bounds__(GTB) k_recon_g(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
-    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec) {
-  __shared__ R wsh[GCB][NF];
-  __shared__ R gsh[GCB][3 * NF];
-  const int g = threadIdx.x / (2 * GL), k0 = ((threadIdx.x / GL) & 1) * KV, l = threadIdx.x % GL;
-  const int c = blockIdx.x * GCB + g;
-  const bool valid = c < n && (act[c] & A_ACTIVE);
-  const bool boundary = valid && bnd[c] != NO_BOUNDARY;
-  R *wi = wsh[g];
-  if (valid && threadIdx.x % (2 * GL) < NF) wi[threadIdx.x % (2 * GL)] = Wst[10 * (size_t)c + threadIdx.x % (2 * GL)];
-  __syncthreads();
-  const int q0 = (valid && !boundary) ? off[c] : 0, q1 = (valid && !boundary) ? off[c + 1] : 0;
-  R Wx[KV], Wy[KV], Wz[KV], mn[KV], mx[KV];
-#pragma unroll
-  for (int k = 0; k < KV; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = R(0); }
-  double sc[3] = {0.0, 0.0, 0.0};
-  bool zero = false;
-  for (int q = q0 + l; q < q1; q += GL) {
-    const int f = lnk[q];
-    const int2 e = s12[f];
-    const bool own = e.x == c;
-    const int j = own ? e.y : e.x;
-    const double4 gg = geo[f];
-    const double4 o4 = own ? dr1[f] : dr2[f];
-    double d[3] = {o4.x, o4.y, o4.z};
-    if (own) wrap3(P, d);
-    sc[0] += d[0]; sc[1] += d[1]; sc[2] += d[2];
-    if (bnd[j] != NO_BOUNDARY) { zero = true; continue; }
-    const double area = gg.w;
-    const double sgn = (d[0] * gg.x + d[1] * gg.y + d[2] * gg.z) < 0.0 ? -1.0 : 1.0;
-    const double nrm[3] = {gg.x * sgn, gg.y * sgn, gg.z * sgn};
-    const double dsh = d[0] * nrm[0] + d[1] * nrm[1] + d[2] * nrm[2];
-    const double idsA = area * ((dsh != 0.0) ? 0.5 / dsh : 0.0);
-    const R drh[3] = {R(nrm[0] * dsh), R(nrm[1] * dsh), R(nrm[2] * dsh)};
-    const R fij[3] = {R(d[0] - nrm[0] * dsh), R(d[1] - nrm[1] * dsh), R(d[2] - nrm[2] * dsh)};
-    const R ia = R(idsA);
-    const R *Wj = Wst + 10 * (size_t)j + k0;
-#pragma unroll
-    for (int k = 0; k < KV; k++) {
-      const R wj = Wj[k], w0 = wi[k0 + k];
-      const R sum = wj + w0;
-      const R diff = wj - w0;
-      mn[k] = smin(mn[k], diff);
-      mx[k] = smax(mx[k], diff);
-      Wx[k] += (sum * drh[0] + diff * fij[0]) * ia;
-      Wy[k] += (sum * drh[1] + diff * fij[1]) * ia;
-      Wz[k] += (sum * drh[2] + diff * fij[2]) * ia;
-    }
-  }
-  zero = gany(zero);
-  const R invV = valid ? R(1.0 / cvol[c]) : R(0);
-  R *gr = gsh[g];
-#pragma unroll
-  for (int k = 0; k < KV; k++) {
-    mn[k] = gmin(mn[k]);
-    mx[k] = gmax(mx[k]);
-    const R gx = gsum(Wx[k]) * invV, gy = gsum(Wy[k]) * invV, gz = gsum(Wz[k]) * invV;
-    if (l == 0) { gr[k0 + k] = gx; gr[NF + k0 + k] = gy; gr[2 * NF + k0 + k] = gz; }
-  }
-  sc[0] = gsum(sc[0]); sc[1] = gsum(sc[1]); sc[2] = gsum(sc[2]);
-  __syncwarp();
-  R ln[KV], lq[KV];
-#pragma unroll
-  for (int k = 0; k < KV; k++) { ln[k] = R(1); lq[k] = R(1); }
-  if (!zero) {
-    for (int q = q0 + l; q < q1; q += GL) {
-      const int f = lnk[q];
-      const bool own = s12[f].x == c;
-      const double4 o4 = own ? dr1[f] : dr2[f];
-      double d[3] = {o4.x, o4.y, o4.z};
-      if (own) wrap3(P, d);
-      const R dd[3] = {R(d[0]), R(d[1]), R(d[2])};
-#pragma unroll
-      for (int k = 0; k < KV; k++) {
-        const int kk = k0 + k;
-        const R dWx = gr[kk] * dd[0] + gr[NF + kk] * dd[1] + gr[2 * NF + kk] * dd[2];
-        limiter_min(ln[k], lq[k], dWx, mn[k], mx[k]);
-      }
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < KV; k++) gmin_frac(ln[k], lq[k]);
-  if (!valid) return;
-  R *r = Wrec + 50 * (size_t)c;
-  if (boundary || zero) {
-    for (int k5 = l; k5 < 5 * KV; k5 += GL) {
-      const int blk = k5 / KV, k = k0 + k5 % KV;
-      r[blk * NF + k] = blk == 0 ? wi[k] : R(0);
-    }
-    return;
-  }
-  // density positivity (subgroup k0 == 0 holds DENS): every lane reads t of DENS
-  R a0 = R(1);
-  if (k0 == 0) {
-    const R lm0 = ln[0] / lq[0];
-    const R t0 = r[40] * lm0;
-    const R sum_dt = R(get_dt(P, rung[c]));
-    const R dWx = (gr[0] * lm0) * R(sc[0]) + (gr[NF] * lm0) * R(sc[1]) + (gr[2 * NF] * lm0) * R(sc[2]);
-    const R dWp = dWx + t0 * sum_dt;
-    const R dW = smax(dWx, dWp);
-    if (dW > R(0)) a0 = smin(R(1), R(0.9) * wi[0] / dW);
-  }
-  // every lane of the cell has read r[40] before it is rewritten
-  __syncwarp(group_mask());
-  for (int k5 = l; k5 < 5 * KV; k5 += GL) {
-    const int blk = k5 / KV, kv = k5 % KV, k = k0 + kv;
-    R v;
-    if (blk == 0) {
-      v = wi[k];
-    } else {
-      R lmk = R(1);
-#pragma unroll
-      for (int t = 0; t < KV; t++)
-        if (t == kv) lmk = ln[t] / lq[t];
-      const R base = blk == 4 ? r[40 + k] : gr[(blk - 1) * NF + k];
-      v = base * lmk;
-      if (k == 0) v *= a0;
-    }
-    r[blk * NF + k] = v;
   }
 }
 
@@ -779,35 +518,6 @@ __device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int 
   }
 }
 
-// Grouped form of gather_contrib: the GL lanes of a group split the cell's
-// faces and their partial sums (in double) are added in a fixed tree, so the
-// result is the same on every run.
-template <typename R>
-__device__ __forceinline__ void gather_contrib_g(int c, int q0, int q1, int l, const int *__restrict__ lnk,
-                                                 const int2 *__restrict__ s12, const R *__restrict__ fcon,
-                                                 const unsigned char *__restrict__ fcode, bool skipj_allowed,
-                                                 double *s) {
-#pragma unroll
-  for (int k = 0; k < 14; k++) s[k] = 0.0;
-  for (int q = q0 + l; q < q1; q += GL) {
-    const int f = lnk[q];
-    const unsigned char code = fcode[f];
-    if (code & F_OFF) continue;
-    const int2 e = s12[f];
-    const int fi = (code & F_SWAP) ? e.y : e.x;
-    const bool is_i = c == fi;
-    if (!is_i && skipj_allowed && (code & F_SKIPJ)) continue;
-    const R *o = fcon + 14 * (size_t)f;
-#pragma unroll
-    for (int k = 0; k < 14; k++) {
-      const double v = double(o[k]);
-      s[k] += ((k < NF) == is_i) ? -v : v;
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 14; k++) s[k] = gsum(s[k]);
-}
-
 // ---- compute_update cell pass (MPI/compute_update.cpp:274-498) -----------
 template <typename R>
 __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched *__restrict__ S,
@@ -826,112 +536,6 @@ __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched 
   if (!(ac & (A_ACTIVE | A_LNGB))) return;
   double s[14];
   gather_contrib<R>(c, off[c], off[c + 1], lnk, s12, fcon, fcode, true, s);
-  double *d0 = dU + 14 * (size_t)c;
-  if (!(ac & A_ACTIVE)) {
-    // inactive neighbour: accumulate until its own step (collect_results,
-    // MPI/distribute_work.cpp:714-720)
-    if (stepdU) {
-#pragma unroll
-      for (int k = 0; k < 14; k++) stepdU[14 * (size_t)c + k] = s[k];
-    }
-    if (bnd[c] == NO_BOUNDARY) {
-#pragma unroll
-      for (int k = 0; k < NF; k++) d0[k] += s[k];
-      d0[13] += s[13];
-      d0[10] = d0[10] + s[10]; d0[11] = d0[11] + s[11]; d0[12] = d0[12] + s[12];
-    }
-    return;
-  }
-  const double V = cvol[c];
-  if (bnd[c] != NO_BOUNDARY) {
-    volp[c] = V;
-#pragma unroll
-    for (int k = 0; k < 14; k++) d0[k] = 0.0;
-    if (stepdU) {
-#pragma unroll
-      for (int k = 0; k < 14; k++) stepdU[14 * (size_t)c + k] = s[k];
-    }
-    return;
-  }
-  double Uc[NF];
-  const double *Ui = U + 10 * (size_t)c;
-#pragma unroll
-  for (int k = 0; k < NF; k++) Uc[k] = Ui[k] + (d0[k] + s[k]);
-  const double divB = d0[13] + s[13];
-  const double dPsi[3] = {d0[10] + s[10], d0[11] + s[11], d0[12] + s[12]};
-  const double dt = t_global - tlast[c];
-  divb[c] = float(dt > 0.0 ? divB / dt / V : divB);  // divBi (MPI/distribute_work.cpp:681)
-#pragma unroll
-  for (int k = 0; k < 14; k++) d0[k] = 0.0;  // dU_local = 0 (collect_results)
-  if (stepdU) {
-    double *sd = stepdU + 14 * (size_t)c;
-#pragma unroll
-    for (int k = 0; k < 13; k++) sd[k] = 0.0;
-    sd[13] = dt > 0.0 ? divB / dt / V : divB;
-  }
-  const R *r = Wrec + 50 * (size_t)c;
-  const R *tc = tau + 10 * (size_t)c;
-  double W1[NF];
-  if (Uc[MASS] <= 0.0) {
-    // failed-mass fallback (MPI/compute_update.cpp:438-468)
-    atomicAdd(&counters[0], 1ULL);
-    double Ut[NF];
-#pragma unroll
-    for (int k = 0; k < NF; k++) W1[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dt;
-    to_conservative(W1, volp[c], Ut);
-    to_primitive(Ut, V, W1);
-  } else {
-    const double dth = 0.5 * dt;
-    double Wh[NF];
-#pragma unroll
-    for (int k = 0; k < NF; k++) Wh[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dth;
-    Uc[WBX] -= Wh[VELX] * divB;
-    Uc[WBY] -= Wh[VELY] * divB;
-    Uc[WBZ] -= Wh[VELZ] * divB;
-    // Dedner divergence cleaning (MPI/compute_update.cpp:373-387, 403-405)
-    const double pres = pressure(P, Wh);
-    const double B2 = Wh[BX] * Wh[BX] + Wh[BY] * Wh[BY] + Wh[BZ] * Wh[BZ];
-    const double dcs2 = P.gamma * pres + B2;
-    const double ch_sig = sqrt(dcs2 / Wh[DENS]);
-    Uc[WBX] -= dPsi[0];
-    Uc[WBY] -= dPsi[1];
-    Uc[WBZ] -= dPsi[2];
-    Uc[MPSI] -= dcs2 * divB;
-    const double l_min = pow(V / (4.0 * M_PI / 3.0), 1.0 / 3.0);
-    Uc[MPSI] *= exp(-0.5 * ch_sig / l_min * dt);
-    to_primitive(Uc, V, W1);
-  }
-  volp[c] = V;
-  W1[ETHM] = ethm_update(P, W1, pos + 3 * (size_t)c);
-  if (W1[ETHM] <= 0.0) {
-    atomicAdd(&counters[1], 1ULL);
-    W1[ETHM] = ethm_from_entropy(P, W1);
-  } else {
-    W1[ENTR] = entropy_from_ethm(P, W1);
-  }
-  double Un[NF];
-  to_conservative(W1, V, Un);
-  double *Uo = U + 10 * (size_t)c;
-#pragma unroll
-  for (int k = 0; k < NF; k++) Uo[k] = Un[k];
-}
-
-template <typename R>
-__global__ void __launch_bounds__(256) k_corr_cell_g(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const double *__restrict__ pos, const double *__restrict__ tlast, double *__restrict__ volp,
-    const R *__restrict__ Wrec, const R *__restrict__ tau,
-    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
-    double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
-    unsigned long long *__restrict__ counters, float *__restrict__ divb) {
-  const double t_global = S->t_global;
-  const int c = blockIdx.x * (256 / GL) + threadIdx.x / GL, l = threadIdx.x % GL;
-  const unsigned char ac = c < n ? act[c] : 0;
-  const bool valid = ac & (A_ACTIVE | A_LNGB);
-  double s[14];
-  gather_contrib_g<R>(c, valid ? off[c] : 0, valid ? off[c + 1] : 0, l, lnk, s12, fcon, fcode, true, s);
-  if (!valid || l != 0) return;
   double *d0 = dU + 14 * (size_t)c;
   if (!(ac & A_ACTIVE)) {
     // inactive neighbour: accumulate until its own step (collect_results,
@@ -1559,65 +1163,6 @@ __global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched 
   tend[c] = t_global + get_dt(P, rf);
 }
 
-template <typename R>
-__global__ void __launch_bounds__(256) k_pred_cell_g(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
-    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const double *__restrict__ pos, const double *__restrict__ U,
-    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
-    int *__restrict__ rung, double *__restrict__ tend, R *__restrict__ Wrec) {
-  const double t_global = S->t_global;
-  const int min_rung = S->min_rung;
-  const int c = blockIdx.x * (256 / GL) + threadIdx.x / GL, l = threadIdx.x % GL;
-  const bool valid = c < n && (act[c] & A_ACTIVE) && bnd[c] == NO_BOUNDARY;
-  double dot[14];
-  gather_contrib_g<R>(c, valid ? off[c] : 0, valid ? off[c + 1] : 0, l, lnk, s12, fcon, fcode, false, dot);
-  if (!valid || l != 0) return;
-  const double V = cvol[c];
-  const double *U0 = U + 10 * (size_t)c;
-  double u0[NF], W0[NF];
-#pragma unroll
-  for (int k = 0; k < NF; k++) u0[k] = U0[k];
-  to_primitive(u0, V, W0);
-  int rg = rung[c];
-  while (rg < RUNGMAX - 1 && u0[MASS] + dot[MASS] * get_dt(P, rg) <= 0.0 * u0[MASS]) rg++;
-  const double dt = get_dt(P, rg);
-  double Uc[NF];
-#pragma unroll
-  for (int k = 0; k < NF; k++) Uc[k] = u0[k] + dot[k] * dt;
-  {
-    const double divB = dot[13];
-    Uc[WBX] -= W0[VELX] * divB * dt;
-    Uc[WBY] -= W0[VELY] * divB * dt;
-    Uc[WBZ] -= W0[VELZ] * divB * dt;
-    const double pres = pressure(P, W0);
-    const double B2 = W0[BX] * W0[BX] + W0[BY] * W0[BY] + W0[BZ] * W0[BZ];
-    const double dcs2 = P.gamma * pres + B2;
-    const double ch_sig = sqrt(dcs2 / W0[DENS]);
-    Uc[WBX] -= dot[10] * dt;
-    Uc[WBY] -= dot[11] * dt;
-    Uc[WBZ] -= dot[12] * dt;
-    Uc[MPSI] -= dcs2 * divB * dt;
-    const double l_min = pow(V / (4.0 * M_PI / 3.0), 1.0 / 3.0);
-    Uc[MPSI] *= exp(-0.5 * ch_sig / l_min * dt);
-  }
-  double W1[NF];
-  to_primitive(Uc, V, W1);
-  W1[ETHM] = ethm_update(P, W1, pos + 3 * (size_t)c);
-  if (W1[ETHM] <= 0.0) W1[ETHM] = W0[ETHM];
-  else W1[ENTR] = entropy_from_ethm(P, W1);
-  const double idt = 1.0 / dt;
-  R *r = Wrec + 50 * (size_t)c;
-#pragma unroll
-  for (int k = 0; k < NF; k++) r[40 + k] = R((W1[k] - W0[k]) * idt);
-  // collect_reconstruction: rung = max(rung, get_rung(dt)), tend = t + dt(rung)
-  int rf = rung[c];
-  const int rb = get_rung(P, dt, min_rung);
-  rf = rf < rb ? rb : rf;
-  rung[c] = rf;
-  tend[c] = t_global + get_dt(P, rf);
-}
-
 // ---- compute_reconstruction (MPI/compute_reconstruction.cpp:41-198) -------
 // Two threads per active cell, five primitives each: Voronoi face gradient of
 // the updated primitives, local limiter, density positivity rescale.
@@ -1626,7 +1171,8 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm) {
+    const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm,
+    R *__restrict__ mnmx, unsigned char *__restrict__ mz) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if ((t >> 1) >= n) return;
   const int c = perm[t >> 1];
@@ -1640,6 +1186,7 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
   if (bnd[c] != NO_BOUNDARY) {
 #pragma unroll
     for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = R(0); r[20 + k] = R(0); r[30 + k] = R(0); r[40 + k] = R(0); }
+    if (k0 == 0) mz[c] = 1;
     return;
   }
   const int q0 = off[c], q1 = off[c + 1];
@@ -1687,6 +1234,13 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
       Wy[k] += (sum * drh[1] + diff * fij[1]) * ia;
       Wz[k] += (sum * drh[2] + diff * fij[2]) * ia;
     }
+  }
+  // the next step's limiter pass 1 (neighbour min/max of the same states)
+  {
+    R *mm = mnmx + 20 * (size_t)c + k0;
+#pragma unroll
+    for (int k = 0; k < KH; k++) { mm[k] = mn[k]; mm[10 + k] = mx[k]; }
+    if (k0 == 0) mz[c] = zero ? 1 : 0;
   }
   if (zero) {
 #pragma unroll
@@ -1788,7 +1342,8 @@ __global__ void k_sched_begin(Params P, Sched *S) {
   S->iscal[3] = 0;
 }
 
-__global__ void k_sched_end(Sched *S) {
+__global__ void k_sched_end(Sched *S, int n) {
+  S->mnmx_ok = S->iscal[1] == n;
   S->nactive_total += (unsigned long long)S->iscal[1];
   S->nfaces_total += (unsigned long long)S->iscal[3];
   S->steps += 1;
@@ -1797,6 +1352,7 @@ __global__ void k_sched_end(Sched *S) {
 __global__ void k_sched_set(Params P, Sched *S, unsigned long long tsysU, int reset_err) {
   S->tsysU = S->tprevU = tsysU;
   S->t_global = P.dt_tick * (double)tsysU;
+  S->mnmx_ok = 0;  // the state was replaced
   if (reset_err) {
     S->min_rung = 0;
     S->iscal[2] = 0;
@@ -2113,6 +1669,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc(c, &d.lsort, nl); rc |= dalloc(c, &d.lpart, nl);
   rc |= dalloc(c, &d.rdv, nl); rc |= dalloc(c, &d.wrv, nl); rc |= dalloc(c, &d.dt0, ncell);
   rc |= dalloc(c, &d.aflag, 8);
+  rc |= dalloc_bytes(c, &d.mnmx, 20 * c->rb * (size_t)ncell); rc |= dalloc(c, &d.mz, ncell);
   rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
   if ((ncell + CB - 1) / CB > CB * 16) { c->err = "fvm_set_mesh: more than 16M cells"; return FVM_ERANGE; }
   rc |= dalloc(c, &d.pos, 3 * (size_t)ncell); rc |= dalloc(c, &d.vel, 3 * (size_t)ncell);
@@ -2364,15 +1921,10 @@ static int enq_begin(fvm_ctx *c) {
 static int enq_limiter(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_LIMITER);
-#if FVM_CELLMAP_GROUPED
-  BULK(k_limiter_g<R><<<nblk(c->n, GCB), GTB, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.geo, d.dr1,
-                                                          d.fflag, d.act, d.tlast, (const R *)d.Wrec, (R *)d.tau,
-                                                          (R *)d.fst));
-#else
   BULK(k_limiter<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1,
                                                               d.fflag, d.act, d.tlast, (const R *)d.Wrec,
-                                                              (R *)d.tau, (R *)d.fst, d.perm));
-#endif
+                                                              (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx,
+                                                              d.mz));
   LAUNCH_CHECK();
   kt_end(c, KT_LIMITER);
   return 0;
@@ -2404,17 +1956,10 @@ static int enq_update(fvm_ctx *c) {
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_FLUX);
   kt_begin(c, KT_CORR_CELL);
-#if FVM_GATHER_GROUPED
-  BULK(k_corr_cell_g<R><<<nblk(c->n, 256 / GL), 256, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
-                                                          d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
-                                                          (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
-                                                          d.stepdU, d.counters, d.divb));
-#else
   BULK(k_corr_cell<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
                                                           (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
                                                           d.stepdU, d.counters, d.perm, d.divb));
-#endif
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_CELL);
   return 0;
@@ -2517,27 +2062,15 @@ static int enq_update0(fvm_ctx *c) {
 static int enq_recon(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_CELL);
-#if FVM_GATHER_GROUPED
-  BULK(k_pred_cell_g<R><<<nblk(c->n, 256 / GL), 256, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
-                                                          d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
-                                                          d.tend, (R *)d.Wrec));
-#else
   BULK(k_pred_cell<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
                                                           d.tend, (R *)d.Wrec, d.perm));
-#endif
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_CELL);
   kt_begin(c, KT_RECON);
-#if FVM_CELLMAP_GROUPED
-  BULK(k_recon_g<R><<<nblk(c->n, GCB), GTB, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.geo, d.dr1,
-                                                        d.dr2, d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
-                                                        (R *)d.Wrec));
-#else
   BULK(k_recon<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
                                                             d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
-                                                            (R *)d.Wrec, d.perm));
-#endif
+                                                            (R *)d.Wrec, d.perm, (R *)d.mnmx, d.mz));
   LAUNCH_CHECK();
   kt_end(c, KT_RECON);
   return 0;
@@ -2552,7 +2085,7 @@ static int enq_end(fvm_ctx *c, int shared) {
     k_shared_sync<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, c->P, d.S, d.act, d.S->iscal, d.rung, d.tend);
     LAUNCH_CHECK();
   }
-  k_sched_end<<<1, 1, 0, c->st>>>(d.S);
+  k_sched_end<<<1, 1, 0, c->st>>>(d.S, c->n);
   LAUNCH_CHECK();
   kt_end(c, KT_SYNC);
   return 0;

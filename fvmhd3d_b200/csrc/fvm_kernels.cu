@@ -61,6 +61,9 @@ using namespace fvm;
 #define FVM_PRAGMA(x) _Pragma(#x)
 #define FVM_CELL_LOOP_(n) FVM_PRAGMA(unroll n)
 #define FVM_CELL_LOOP FVM_CELL_LOOP_(FVM_CELL_UNROLL)
+#ifndef FVM_RECON_LIA
+#define FVM_RECON_LIA 1  // the reconstruction reads its face weights from a per-link table
+#endif
 #ifndef FVM_ADJUST_REPLAY
 #define FVM_ADJUST_REPLAY 1  // adjust_timesteps by parallel replay (sequential sweep as fallback)
 #endif
@@ -105,6 +108,7 @@ struct Dev {
   double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
   int *aflag;               // adjust_timesteps replay flags
   void *mnmx;               // per cell: the reconstruction's neighbour min and max (20 of the bulk type)
+  void *lia;                // per link: the reconstruction's face weight A / (2 dsh) (bulk type)
   unsigned char *mz;        // per cell: the reconstruction met a boundary (the limiter is zero)
   // learned-flux buffers (fvm_set_flux_mode)
   void *lX, *lY, *lface, *lcount, *lstats, *lhx, *lhy, *lhcount, *lnorm;
@@ -219,6 +223,40 @@ __device__ __forceinline__ void wrap3(const Params &P, double *d) {
     const double L = P.box[a];
     if (d[a] > 0.5 * L) d[a] -= L;
     else if (d[a] < -0.5 * L) d[a] += L;
+  }
+}
+
+// Geometry of one face side for the reconstruction
+// (MPI/compute_reconstruction.cpp:70-138): the min-image offset d of the face
+// centroid, the normal oriented along it and the normal distance dsh.
+__device__ __forceinline__ void recon_geom(const Params &P, bool own, const double4 &g, const double4 &o4, double *d,
+                                           double *nrm, double &dsh) {
+  d[0] = o4.x; d[1] = o4.y; d[2] = o4.z;
+  if (own) wrap3(P, d);
+  const double sgn = (d[0] * g.x + d[1] * g.y + d[2] * g.z) < 0.0 ? -1.0 : 1.0;
+  nrm[0] = g.x * sgn; nrm[1] = g.y * sgn; nrm[2] = g.z * sgn;
+  dsh = d[0] * nrm[0] + d[1] * nrm[1] + d[2] * nrm[2];
+}
+// A / (2 dsh), the face weight of the gradient.
+__device__ __forceinline__ double recon_ia(const double4 &g, double dsh) {
+  return g.w * ((dsh != 0.0) ? 0.5 / dsh : 0.0);
+}
+
+// The reconstruction's face weights per link, computed once per mesh (the
+// division is the costliest step of its face loop).
+template <typename R>
+__global__ void k_link_ia(int n, Params P, const int *__restrict__ off, const int2 *__restrict__ lfj,
+                          const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
+                          const double4 *__restrict__ dr2, R *__restrict__ lia) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  for (int q = off[c]; q < off[c + 1]; q++) {
+    const int2 fj = lfj[q];
+    const bool own = fj.y >= 0;
+    const double4 g = geo[fj.x];
+    double d[3], nrm[3], dsh;
+    recon_geom(P, own, g, own ? dr1[fj.x] : dr2[fj.x], d, nrm, dsh);
+    lia[q] = R(recon_ia(g, dsh));
   }
 }
 
@@ -1172,7 +1210,7 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm,
-    R *__restrict__ mnmx, unsigned char *__restrict__ mz) {
+    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lia) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if ((t >> 1) >= n) return;
   const int c = perm[t >> 1];
@@ -1209,18 +1247,16 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
     const int j = own ? e.y : e.x;
 #endif
     const double4 g = geo[f];
-    const double4 o4 = own ? dr1[f] : dr2[f];
-    double d[3] = {o4.x, o4.y, o4.z};
-    if (own) wrap3(P, d);
+    double d[3], nrm[3], dsh;
+    recon_geom(P, own, g, own ? dr1[f] : dr2[f], d, nrm, dsh);
     sc[0] = sc[0] + d[0]; sc[1] = sc[1] + d[1]; sc[2] = sc[2] + d[2];
-    const double area = g.w;
-    const double sgn = (d[0] * g.x + d[1] * g.y + d[2] * g.z) < 0.0 ? -1.0 : 1.0;
-    const double nrm[3] = {g.x * sgn, g.y * sgn, g.z * sgn};
-    const double dsh = d[0] * nrm[0] + d[1] * nrm[1] + d[2] * nrm[2];
-    const double idsA = area * ((dsh != 0.0) ? 0.5 / dsh : 0.0);
     const R drh[3] = {R(nrm[0] * dsh), R(nrm[1] * dsh), R(nrm[2] * dsh)};
     const R fij[3] = {R(d[0] - nrm[0] * dsh), R(d[1] - nrm[1] * dsh), R(d[2] - nrm[2] * dsh)};
-    const R ia = R(idsA);
+#if FVM_RECON_LIA
+    const R ia = lia[q];
+#else
+    const R ia = R(recon_ia(g, dsh));
+#endif
     if (bnd[j] != NO_BOUNDARY) { zero = true; break; }
     const R *Wj = Wst + 10 * (size_t)j + k0;
 #pragma unroll
@@ -1670,6 +1706,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc(c, &d.rdv, nl); rc |= dalloc(c, &d.wrv, nl); rc |= dalloc(c, &d.dt0, ncell);
   rc |= dalloc(c, &d.aflag, 8);
   rc |= dalloc_bytes(c, &d.mnmx, 20 * c->rb * (size_t)ncell); rc |= dalloc(c, &d.mz, ncell);
+  rc |= dalloc_bytes(c, &d.lia, c->rb * (size_t)nl);
   rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
   if ((ncell + CB - 1) / CB > CB * 16) { c->err = "fvm_set_mesh: more than 16M cells"; return FVM_ERANGE; }
   rc |= dalloc(c, &d.pos, 3 * (size_t)ncell); rc |= dalloc(c, &d.vel, 3 * (size_t)ncell);
@@ -1800,6 +1837,8 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   CK(cudaMemsetAsync(d.vel, 0, sizeof(double) * 3 * (size_t)n, c->st));
   CK(cudaMemsetAsync(d.tlast, 0, sizeof(double) * n, c->st));
   k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
+  LAUNCH_CHECK();
+  BULK(k_link_ia<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.off, d.lfj, d.geo, d.dr1, d.dr2, (R *)d.lia));
   LAUNCH_CHECK();
 
   BULK(k_init_state<R><<<nblk(n, 128), 128, 0, c->st>>>(n, dW, d.cvol, d.U, d.dU, (R *)d.Wrec, d.volp));
@@ -2070,7 +2109,8 @@ static int enq_recon(fvm_ctx *c) {
   kt_begin(c, KT_RECON);
   BULK(k_recon<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
                                                             d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
-                                                            (R *)d.Wrec, d.perm, (R *)d.mnmx, d.mz));
+                                                            (R *)d.Wrec, d.perm, (R *)d.mnmx, d.mz,
+                                                            (const R *)d.lia));
   LAUNCH_CHECK();
   kt_end(c, KT_RECON);
   return 0;

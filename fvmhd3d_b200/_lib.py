@@ -69,6 +69,7 @@ SIGNATURES = {
     "fvm_learn_stats": (c_int, [c_void_p, c_void_p]),
     "fvm_harvest_count": (c_ll, [c_void_p]),
     "fvm_get_harvest": (c_int, [c_void_p, c_ll, c_void_p, c_void_p]),
+    "fvm_autotune": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "fvm_compute_flux": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_compute_flux_static": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_last_step_ms": (c_float, [c_void_p]),

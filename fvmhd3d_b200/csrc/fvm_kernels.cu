@@ -47,6 +47,10 @@ using namespace fvm;
 #define FVM_CELL_MINB_F 6
 #endif
 #define FVM_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CELL_MINB_F : FVM_CELL_MINB_D)
+#ifndef FVM_LIMITER_MINB_D
+#define FVM_LIMITER_MINB_D 3  // the staged FP64 limiter prefers registers to occupancy
+#endif
+#define FVM_LIMITER_MINB(R) (sizeof(R) == 4 ? FVM_CELL_MINB_F : FVM_LIMITER_MINB_D)
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
 // cell-kernel mappings: grouped (16 lanes per cell) or two threads per cell
 #ifndef FVM_CELL_LFJ
@@ -61,6 +65,9 @@ using namespace fvm;
 #define FVM_PRAGMA(x) _Pragma(#x)
 #define FVM_CELL_LOOP_(n) FVM_PRAGMA(unroll n)
 #define FVM_CELL_LOOP FVM_CELL_LOOP_(FVM_CELL_UNROLL)
+#ifndef FVM_LIMITER_STAGE
+#define FVM_LIMITER_STAGE 1  // default: limiter face records staged in shared memory per block
+#endif
 #ifndef FVM_RECON_LIA
 #define FVM_RECON_LIA 1  // the reconstruction reads its face weights from a per-link table
 #endif
@@ -270,21 +277,12 @@ __global__ void k_link_ia(int n, Params P, const int *__restrict__ off, const in
 constexpr int KH = 5;  // primitives per thread in the two-threads-per-cell kernels
 
 template <typename R>
-__global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params P, const Sched *__restrict__ S,
+__device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double t_global,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
-    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
+    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst,
     const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
-  const double t_global = S->t_global;
-  // every cell steps and every cell was reconstructed by the last step: the
-  // neighbour min/max of pass 1 are the reconstruction's (same states, same
-  // faces, exact min/max)
-  const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if ((t >> 1) >= n) return;
-  const int i = perm[t >> 1];
-  const int k0 = (int)(t & 1) * KH;
   if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
   const double ti = tlast[i];
   const R *ri = Wrec + 50 * (size_t)i + k0;
@@ -399,6 +397,133 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
     for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2]) + gt[k] * dtt);
   }
 }
+
+// Staged limiter: a block's CST cells (two threads each) first compute the
+// per-face records of passes 2 and 3 (the side's offset dr, the two time
+// offsets, the face and its flags) for all their faces together, into shared
+// memory, so the face loops read no global memory but the cell's own record.
+// Used when the first pass is reused (every cell steps) and the block's faces
+// fit (LCAP); otherwise the block runs limiter_thread.
+constexpr int CST = 64;
+constexpr int LCAP = 1408;
+template <typename R>
+constexpr int limiter_stage_bytes() { return LCAP * (5 * (int)sizeof(R) + 4); }
+
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_LIMITER_MINB(R)) k_limiter_st(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
+    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
+    const unsigned char *__restrict__ act, const double *__restrict__ tlast,
+    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
+  extern __shared__ __align__(16) unsigned char lsm[];
+  __shared__ int soff[CST + 1];
+  const double t_global = S->t_global;
+  const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
+  const int tid = threadIdx.x;
+  const int c0 = blockIdx.x * CST;
+  const int c1 = c0 + CST < n ? c0 + CST : n;
+  const int L0 = off[c0], nL = off[c1] - L0;
+  const bool staged = reuse && nL <= LCAP;  // uniform over the block
+  R *sdx = reinterpret_cast<R *>(lsm), *sdy = sdx + LCAP, *sdz = sdy + LCAP, *st2 = sdz + LCAP, *st3 = st2 + LCAP;
+  int *sfk = reinterpret_cast<int *>(st3 + LCAP);
+  if (staged) {
+    for (int k = tid; k <= c1 - c0; k += blockDim.x) soff[k] = off[c0 + k] - L0;
+    __syncthreads();
+    for (int l = tid; l < nL; l += blockDim.x) {
+      int lo = 0, hi = c1 - c0;  // soff[lo] <= l < soff[hi]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (soff[mid] <= l) lo = mid; else hi = mid;
+      }
+      const int2 fj = lfj[L0 + l];
+      const int f = fj.x;
+      const bool own = fj.y >= 0;
+      const unsigned char ff = fflag[f];
+      const double ti = tlast[c0 + lo], tj = tlast[own ? fj.y : ~fj.y];
+      const double dtI = t_global - (own ? ti : tj), dtJ = t_global - (own ? tj : ti);
+      const double dth = 0.5 * smin(dtI, dtJ);
+      const double dt = smin(dtI, dtJ);
+      const double4 g = geo[f], d = dr1[f];
+      const double dsl = own ? 0.0 : 2.0 * d.w;
+      sdx[l] = R(d.x - g.x * dsl);
+      sdy[l] = R(d.y - g.y * dsl);
+      sdz[l] = R(d.z - g.z * dsl);
+      st2[l] = R(own ? dtI - dth : dtJ - dth);
+      st3[l] = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
+      sfk[l] = (f << 3) | ((ff & FF_ACTIVE) ? 1 : 0) | ((ff & (FF_BND1 | FF_BND2)) ? 2 : 0) | (own ? 4 : 0);
+    }
+  }
+  __syncthreads();
+  const int cl = tid >> 1, k0 = (tid & 1) * KH;
+  if (c0 + cl >= n) return;
+  if (!staged) {
+    limiter_thread<R>(perm[c0 + cl], k0, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast, Wrec, tau,
+                      fst, mnmx, mz);
+    return;
+  }
+  const int i = c0 + cl;  // the staged blocks assume the identity thread-to-cell map
+  if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
+  const R *ri = Wrec + 50 * (size_t)i + k0;
+  R mn[KH], mx[KH], ln[KH], lq[KH], wi[KH], gx[KH], gy[KH], gz[KH], gt[KH];
+  const R *mm = mnmx + 20 * (size_t)i + k0;
+#pragma unroll
+  for (int k = 0; k < KH; k++) {
+    mn[k] = mm[k]; mx[k] = mm[10 + k]; ln[k] = R(1); lq[k] = R(1); wi[k] = ri[k];
+  }
+  const bool zero = mz[i] != 0;
+  const int q0 = soff[cl], q1 = soff[cl + 1];
+  R *to = tau + 10 * (size_t)i + k0;
+  if (zero) {
+#pragma unroll
+    for (int k = 0; k < KH; k++) { to[k] = R(0); gx[k] = gy[k] = gz[k] = gt[k] = R(0); }
+  } else {
+#pragma unroll
+    for (int k = 0; k < KH; k++) { gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k]; }
+    for (int l = q0; l < q1; l++) {
+      if (!(sfk[l] & 1)) continue;
+      const R d0 = sdx[l], d1 = sdy[l], d2 = sdz[l], dtt = st2[l];
+#pragma unroll
+      for (int k = 0; k < KH; k++) {
+        const R dWx = gx[k] * d0 + gy[k] * d1 + gz[k] * d2;
+        const R dW = dWx + gt[k] * dtt;
+        limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KH; k++) {
+      const R tk = ln[k] / lq[k];
+      to[k] = tk;
+      gx[k] *= tk; gy[k] *= tk; gz[k] *= tk; gt[k] *= tk;
+    }
+  }
+  for (int l = q0; l < q1; l++) {
+    const int fk = sfk[l];
+    if (!(fk & 1) || (fk & 2)) continue;
+    const R d0 = sdx[l], d1 = sdy[l], d2 = sdz[l], dtt = st3[l];
+    R *o = fst + 20 * (size_t)(fk >> 3) + ((fk & 4) ? 0 : 10) + k0;
+#pragma unroll
+    for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * d0 + gy[k] * d1 + gz[k] * d2) + gt[k] * dtt);
+  }
+}
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
+    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
+    const unsigned char *__restrict__ act, const double *__restrict__ tlast,
+    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
+  const double t_global = S->t_global;
+  // every cell steps and every cell was reconstructed by the last step: the
+  // neighbour min/max of pass 1 are the reconstruction's (same states, same
+  // faces, exact min/max)
+  const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((t >> 1) >= n) return;
+  limiter_thread<R>(perm[t >> 1], (int)(t & 1) * KH, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
+                    Wrec, tau, fst, mnmx, mz);
+}
+
 
 // ---- compute_update face pass (MPI/compute_update.cpp:106-269) -----------
 // One thread per face: half-step extrapolated face states, face velocity,
@@ -1517,6 +1642,14 @@ struct fvm_ctx {
   int learn_mode = 0;
   LearnBuf lb{};
   float h_norm[48];  // standardisation of the network's inputs and outputs (fvm_mlp_set_norm)
+  // launch choices of the autotuner (fvm_autotune); the defaults are the
+  // tuned values of the 128^3 blast
+  struct {
+    int lim_staged = FVM_LIMITER_STAGE;  // staged limiter (shared-memory face records) or one record per thread
+    int bs_face = 64;    // threads per block of the face kernels
+    int bs_cell = 64;    // threads per block of the one-thread-per-cell gathers
+    int bs_cell2 = 64;   // threads per block of the two-threads-per-cell kernels
+  } tune;
   std::string err;
 };
 
@@ -1677,6 +1810,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   }
   const long long nl = off[ncell];
   if (off[0] != 0 || nl < 0 || nl > 0x7fffffffLL) { c->err = "fvm_set_mesh: bad CSR offsets"; return FVM_EINVAL; }
+  if (nface >= (1 << 28)) { c->err = "fvm_set_mesh: more than 2^28 faces"; return FVM_ERANGE; }
   for (int f = 0; f < nface; f++)
     if (s1[f] < 0 || s1[f] >= ncell || s2[f] < 0 || s2[f] >= ncell || s1[f] == s2[f]) {
       c->err = "fvm_set_mesh: face " + std::to_string(f) + " has a bad cell index";
@@ -1960,10 +2094,26 @@ static int enq_begin(fvm_ctx *c) {
 static int enq_limiter(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_LIMITER);
-  BULK(k_limiter<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1,
-                                                              d.fflag, d.act, d.tlast, (const R *)d.Wrec,
+  static_assert(FVM_CELL_PERM == 0, "the staged limiter maps threads to consecutive cells");
+  if (c->tune.lim_staged) {
+    BULK(({
+      static bool attr = false;
+      if (!attr) {
+        CK(cudaFuncSetAttribute(k_limiter_st<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                limiter_stage_bytes<R>()));
+        attr = true;
+      }
+      k_limiter_st<R><<<nblk(c->n, CST), 128, limiter_stage_bytes<R>(), c->st>>>(
+          c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
+          (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz);
+    }));
+  } else {
+    const int bs = c->tune.bs_cell2;
+    BULK(k_limiter<R><<<nblk(2LL * c->n, bs), bs, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo,
+                                                              d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
                                                               (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx,
                                                               d.mz));
+  }
   LAUNCH_CHECK();
   kt_end(c, KT_LIMITER);
   return 0;
@@ -1976,26 +2126,26 @@ static int enq_update(fvm_ctx *c) {
   kt_begin(c, KT_CORR_FLUX);
   const LearnBuf &lb = c->lb;
 #define CORR_FLUX(MODE, GRID)                                                                                   \
-  BULK(k_corr_flux<R, MODE><<<GRID, 128, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, \
+  BULK(k_corr_flux<R, MODE><<<GRID, c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, \
                                                      d.tlast, (const R *)d.Wrec, (const R *)d.fst, (R *)d.fcon,   \
                                                      d.fcode, lb))
   if (c->learn_mode == 1) {
     CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
-    CORR_FLUX(LM_DEFER, nblk(c->nf, 128));
+    CORR_FLUX(LM_DEFER, nblk(c->nf, c->tune.bs_face));
     LAUNCH_CHECK();
     int rc = mlp_launch_dev(c, c->nf, lb.count, lb.X, lb.Y);
     if (rc) return rc;
-    CORR_FLUX(LM_FINISH, nblk(c->nf, 128));
+    CORR_FLUX(LM_FINISH, nblk(c->nf, c->tune.bs_face));
   } else if (c->learn_mode == 2) {
-    CORR_FLUX(LM_HARVEST, nblk(c->nf, 128));
+    CORR_FLUX(LM_HARVEST, nblk(c->nf, c->tune.bs_face));
   } else {
-    CORR_FLUX(LM_EXACT, nblk(c->nf, 128));
+    CORR_FLUX(LM_EXACT, nblk(c->nf, c->tune.bs_face));
   }
 #undef CORR_FLUX
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_FLUX);
   kt_begin(c, KT_CORR_CELL);
-  BULK(k_corr_cell<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+  BULK(k_corr_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
                                                           (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
                                                           d.stepdU, d.counters, d.perm, d.divb));
@@ -2077,7 +2227,7 @@ static int enq_update0(fvm_ctx *c) {
   kt_begin(c, KT_PRED_FLUX);
   const LearnBuf &lb = c->lb;
 #define PRED_FLUX(MODE)                                                                                       \
-  BULK(k_pred_flux<R, MODE><<<nblk(c->nf, 128), 128, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
+  BULK(k_pred_flux<R, MODE><<<nblk(c->nf, c->tune.bs_face), c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
                                                                  d.vel, (const R *)d.Wst, (R *)d.fcon2, d.fcode2, \
                                                                  d.S, d.rung, lb))
   if (c->learn_mode == 1) {
@@ -2101,13 +2251,13 @@ static int enq_update0(fvm_ctx *c) {
 static int enq_recon(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_CELL);
-  BULK(k_pred_cell<R><<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+  BULK(k_pred_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
                                                           d.tend, (R *)d.Wrec, d.perm));
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_CELL);
   kt_begin(c, KT_RECON);
-  BULK(k_recon<R><<<nblk(2LL * c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
+  BULK(k_recon<R><<<nblk(2LL * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
                                                             d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
                                                             (R *)d.Wrec, d.perm, (R *)d.mnmx, d.mz,
                                                             (const R *)d.lia));
@@ -2897,6 +3047,105 @@ int fvm_get_harvest(fvm_ctx *c, long long n, float *X, float *Y) {
   CK(cudaMemcpyAsync(X, c->lb.hx, (size_t)n * 16 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(Y, c->lb.hy, (size_t)n * 8 * sizeof(float), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+}  // extern "C"
+
+// ================================ autotuner ================================
+
+namespace {
+// The mutable per-cell state of a context (everything a step writes that
+// outlives the step), for trial steps that leave no trace.
+struct StateCopy {
+  std::vector<std::pair<void *, size_t>> items;
+  void *buf = nullptr;
+};
+
+int state_items(fvm_ctx *c, StateCopy &sc) {
+  Dev &d = c->d;
+  const size_t n = c->n, rb = c->rb;
+  sc.items = {{d.U, 10 * n * 8}, {d.dU, 14 * n * 8}, {d.Wrec, 50 * n * rb}, {d.vel, 3 * n * 8},
+              {d.tlast, n * 8},  {d.tend, n * 8},    {d.rung, n * 4},        {d.opos, 3 * n * 8},
+              {d.ovel, 3 * n * 8}, {d.divb, n * 4},  {d.volp, n * 8},        {d.mnmx, 20 * n * rb},
+              {d.mz, n},           {d.S, sizeof(Sched)}, {d.counters, 4 * sizeof(unsigned long long)}};
+  if (d.lstats) sc.items.push_back({d.lstats, LSTAT_COUNT * sizeof(double)});
+  size_t total = 0;
+  for (auto &it : sc.items) total += (it.second + 255) & ~(size_t)255;
+  CK(cudaMallocAsync(&sc.buf, total, c->st));
+  return 0;
+}
+
+int state_copy(fvm_ctx *c, StateCopy &sc, bool save) {
+  char *p = (char *)sc.buf;
+  for (auto &it : sc.items) {
+    if (save) CK(cudaMemcpyAsync(p, it.first, it.second, cudaMemcpyDeviceToDevice, c->st));
+    else CK(cudaMemcpyAsync(it.first, p, it.second, cudaMemcpyDeviceToDevice, c->st));
+    p += (it.second + 255) & ~(size_t)255;
+  }
+  return 0;
+}
+}  // namespace
+
+extern "C" {
+
+int fvm_autotune(fvm_ctx *c, int shared, int steps, int *choice) {
+  if (!c || steps < 1) return FVM_EINVAL;
+  if (!c->have_state || c->in_step) { c->err = "fvm_autotune: no state, or inside a step"; return FVM_ENOMESH; }
+  CK(cudaSetDevice(c->device));
+  StateCopy sc;
+  int rc = state_items(c, sc);
+  if (rc) return rc;
+  if ((rc = state_copy(c, sc, true))) return rc;
+  const bool prof = c->prof;
+  const unsigned long long tsys0 = c->tsysU;
+  const double t0 = c->t_global;
+  // one trial: `steps` eager steps with per-kernel events, then the state back
+  auto trial = [&](double *ms_out) -> int {
+    int r = fvm_set_profiling(c, 1);
+    if (r) return r;
+    for (int s = 0; s < steps; s++) {
+      r = fvm_step(c, shared);
+      if (r < 0) return r;
+    }
+    for (int k = 0; k < KT_COUNT; k++) ms_out[k] = c->kt_ms[k];
+    if ((r = state_copy(c, sc, false))) return r;
+    CK(cudaStreamSynchronize(c->st));
+    c->tsysU = tsys0;
+    c->t_global = t0;
+    return read_sched(c);
+  };
+  double ms[KT_COUNT];
+  // coordinate search, one family at a time, timed on its own kernels
+  struct Knob { int *v; int ncand; int cand[3]; int k1, k2; } knobs[] = {
+      {&c->tune.lim_staged, 2, {1, 0, 0}, KT_LIMITER, KT_LIMITER},
+      {&c->tune.bs_face, 3, {128, 64, 32}, KT_CORR_FLUX, KT_PRED_FLUX},
+      {&c->tune.bs_cell, 3, {128, 64, 32}, KT_CORR_CELL, KT_PRED_CELL},
+      {&c->tune.bs_cell2, 3, {128, 64, 32}, KT_RECON, KT_LIMITER},
+  };
+  for (auto &kb : knobs) {
+    double best = 1e300;
+    int bestv = *kb.v;
+    for (int ci = 0; ci < kb.ncand; ci++) {
+      const int v = kb.cand[ci];
+      *kb.v = v;
+      drop_graphs(c);
+      if ((rc = trial(ms)) != 0) { c->prof = prof; return rc; }
+      const double t = ms[kb.k1] + (kb.k2 != kb.k1 ? ms[kb.k2] : 0.0);
+      if (t < best) { best = t; bestv = v; }
+    }
+    *kb.v = bestv;
+  }
+  drop_graphs(c);
+  fvm_set_profiling(c, prof ? 1 : 0);
+  CK(cudaFreeAsync(sc.buf, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (choice) {
+    choice[0] = c->tune.lim_staged;
+    choice[1] = c->tune.bs_face;
+    choice[2] = c->tune.bs_cell;
+    choice[3] = c->tune.bs_cell2;
+  }
   return 0;
 }
 

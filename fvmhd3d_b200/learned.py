@@ -218,6 +218,8 @@ def main():
     ap.add_argument("--evaluate", action="store_true")
     ap.add_argument("--weights", default=None, help="evaluate these parameters instead of training")
     ap.add_argument("--profile-rows", type=int, default=0, help="only run the network on N random rows")
+    ap.add_argument("--eval-nside", type=int, default=128, help="blast lattice size of --evaluate")
+    ap.add_argument("--eval-steps", type=int, default=100, help="global steps of --evaluate")
     args = ap.parse_args()
     if args.profile_rows:
         s = System()
@@ -254,7 +256,7 @@ def main():
             np.savez_compressed(args.out, loss=hist, gate=json.dumps(GATE), **model)
     if args.evaluate:
         print(json.dumps({"holdout_blast128": holdout(model)}))
-        print(json.dumps(evaluate(model)))
+        print(json.dumps(evaluate(model, nside=args.eval_nside, steps=args.eval_steps)))
 
 
 if __name__ == "__main__":

@@ -250,6 +250,13 @@ class System:
                                          ctypes.c_float(lr), ctypes.c_ulonglong(seed), _p(hist)), "fvm_mlp_train")
         return hist[:steps]
 
+    def autotune(self, shared=True, steps=3) -> dict:
+        """Pick launch choices by timing trial steps (the state is restored)."""
+        ch = np.zeros(4, np.int32)
+        self._check(self.L.fvm_autotune(self.h, 1 if shared else 0, int(steps), _p(ch)), "fvm_autotune")
+        return {"staged_limiter": int(ch[0]), "face_block": int(ch[1]), "cell_block": int(ch[2]),
+                "cell2_block": int(ch[3])}
+
     def clock(self):
         """(tsysU, dt_global, iteration): the scheduler clock after the last
         step (the reference's Scheduler::tsysU, system::dt_global and

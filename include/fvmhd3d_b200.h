@@ -251,6 +251,14 @@ int fvm_learn_stats(fvm_ctx *c, double *stats8);
 long long fvm_harvest_count(fvm_ctx *c);
 int fvm_get_harvest(fvm_ctx *c, long long n, float *X, float *Y);
 
+/* Autotuner: picks, by timing `steps` trial steps per candidate on the
+ * current state (restored after every trial, so the run is unchanged), the
+ * limiter variant (face records staged in shared memory or not) and the
+ * block sizes of the face kernels, the one-thread-per-cell gathers and the
+ * two-threads-per-cell kernels.  choice (4 ints, may be NULL) receives
+ * {staged limiter, face block, cell block, two-thread cell block}. */
+int fvm_autotune(fvm_ctx *c, int shared, int steps, int *choice);
+
 /* Timing helper: CUDA-event time in ms of the last fvm_step's kernels. */
 float fvm_last_step_ms(const fvm_ctx *c);
 /* The context's CUDA stream (a cudaStream_t), for callers that order their

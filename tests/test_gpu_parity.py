@@ -203,3 +203,24 @@ def test_adjust_timesteps_replay_vs_oracle():
         for k in ("rung", "tend", "tlast"):
             assert np.array_equal(st[k], so[k]), k
     assert dirty_steps >= 3
+
+
+def test_autotune_leaves_the_state_and_keeps_parity():
+    """fvm_autotune times trial steps on the live state and restores it bit
+    for bit; steps with the launch choices it picks stay at parity with the
+    oracle."""
+    m, W = setup_case(16, "blast", seed=14, noise=0.02)
+    s, o = gpu_system(m, W), oracle_system(m, W)
+    for _ in range(2):
+        assert s.step(shared=True) == o.step(shared=True)
+    before = s.get_state()
+    t0, ticks0 = s.time, s.tsys_ticks
+    choice = s.autotune(shared=True, steps=2)
+    assert set(choice) == {"staged_limiter", "face_block", "cell_block", "cell2_block"}
+    after = s.get_state()
+    for k in before:
+        assert np.array_equal(before[k], after[k]), k
+    assert s.time == t0 and s.tsys_ticks == ticks0
+    for _ in range(3):
+        assert s.step(shared=True) == o.step(shared=True)
+    assert_state_close(s.get_state(), o.get_state())

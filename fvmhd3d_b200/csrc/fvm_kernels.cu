@@ -647,8 +647,8 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Par
 // path accumulates its single-precision contributions in double with
 // compensated (Kahan) summation.
 template <typename R>
-__device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int *__restrict__ lnk,
-                                               const int2 *__restrict__ s12, const R *__restrict__ fcon,
+__device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int2 *__restrict__ lfj,
+                                               const R *__restrict__ fcon,
                                                const unsigned char *__restrict__ fcode, bool skipj_allowed,
                                                double *s) {
   constexpr bool kahan = sizeof(R) == 4;
@@ -656,12 +656,13 @@ __device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int 
 #pragma unroll
   for (int k = 0; k < 14; k++) { s[k] = 0.0; comp[k] = 0.0; }
   for (int q = q0; q < q1; q++) {
-    const int f = lnk[q];
+    const int2 fj = lfj[q];
+    const int f = fj.x;
     const unsigned char code = fcode[f];
     if (code & F_OFF) continue;
-    const int2 e = s12[f];
-    const int fi = (code & F_SWAP) ? e.y : e.x;
-    const bool is_i = c == fi;
+    // this cell is the face's i side when it is s1 and the face was not
+    // swapped, or s2 and it was
+    const bool is_i = (fj.y >= 0) != ((code & F_SWAP) != 0);
     if (!is_i && skipj_allowed && (code & F_SKIPJ)) continue;
     const R *o = fcon + 14 * (size_t)f;
     // U: i gets -F, j gets +F;  gradPsi and divB: i gets +, j gets -
@@ -684,7 +685,7 @@ __device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int 
 // ---- compute_update cell pass (MPI/compute_update.cpp:274-498) -----------
 template <typename R>
 __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const int *__restrict__ off, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const double *__restrict__ pos, const double *__restrict__ tlast, double *__restrict__ volp,
     const R *__restrict__ Wrec, const R *__restrict__ tau,
@@ -698,7 +699,7 @@ __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched 
   const unsigned char ac = act[c];
   if (!(ac & (A_ACTIVE | A_LNGB))) return;
   double s[14];
-  gather_contrib<R>(c, off[c], off[c + 1], lnk, s12, fcon, fcode, true, s);
+  gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, true, s);
   double *d0 = dU + 14 * (size_t)c;
   if (!(ac & A_ACTIVE)) {
     // inactive neighbour: accumulate until its own step (collect_results,
@@ -1268,7 +1269,7 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Par
 // cell's final rung/tend.  Arithmetic in double for both bulk types.
 template <typename R>
 __global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ s12,
+    const int *__restrict__ off, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const double *__restrict__ pos, const double *__restrict__ U,
     const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
@@ -1281,7 +1282,7 @@ __global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched 
   if (!(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
   const double V = cvol[c];
   double dot[14];
-  gather_contrib<R>(c, off[c], off[c + 1], lnk, s12, fcon, fcode, false, dot);
+  gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, false, dot);
   const double *U0 = U + 10 * (size_t)c;
   double u0[NF], W0[NF];
 #pragma unroll
@@ -2145,7 +2146,7 @@ static int enq_update(fvm_ctx *c) {
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_FLUX);
   kt_begin(c, KT_CORR_CELL);
-  BULK(k_corr_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+  BULK(k_corr_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
                                                           (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
                                                           d.stepdU, d.counters, d.perm, d.divb));
@@ -2251,7 +2252,7 @@ static int enq_update0(fvm_ctx *c) {
 static int enq_recon(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_CELL);
-  BULK(k_pred_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.s12, d.cvol, d.act,
+  BULK(k_pred_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
                                                           d.tend, (R *)d.Wrec, d.perm));
   LAUNCH_CHECK();

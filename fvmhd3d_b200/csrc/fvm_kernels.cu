@@ -114,6 +114,7 @@ struct Dev {
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
   double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
   int *aflag;               // adjust_timesteps replay flags
+  unsigned char *awork;     // adjust_timesteps replay work lists (2 per cell)
   void *mnmx;               // per cell: the reconstruction's neighbour min and max (20 of the bulk type)
   void *lia;                // per link: the reconstruction's face weight A / (2 dsh) (bulk type)
   unsigned char *mz;        // per cell: the reconstruction met a boundary (the limiter is zero)
@@ -928,7 +929,7 @@ __global__ void k_adjust_mark(int n, const int *__restrict__ off, const int *__r
                               const int2 *__restrict__ s12, const unsigned char *__restrict__ act,
                               const int *__restrict__ bnd, const double *__restrict__ dtl,
                               unsigned char *__restrict__ hash, int *__restrict__ ndirty,
-                              unsigned char *__restrict__ site) {
+                              unsigned char *__restrict__ site, unsigned char *__restrict__ work) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   bool dirty = false, s = false;
   if (i < n && (act[i] & A_ACTIVE) && bnd[i] == NO_BOUNDARY) {
@@ -940,8 +941,12 @@ __global__ void k_adjust_mark(int n, const int *__restrict__ off, const int *__r
       const double dj = dtl[j];
       if (dj < 0.0) continue;
       hash[j] = 1;
-      if (2.0 * dj < di || 2.0 * di < dj) dirty = true;
+      if (2.0 * dj < di || 2.0 * di < dj) {
+        dirty = true;
+        work[j] = 1;  // both ends of a pair outside a factor 2 start the replay's work list
+      }
     }
+    if (dirty) work[i] = 1;
   }
   if (i < n) site[i] = s ? 1 : 0;
   __shared__ int bsum;
@@ -1046,6 +1051,11 @@ __global__ void k_adjust_seq(const int *__restrict__ off, const int *__restrict_
 // upper bound, so replays converge; a replay that changes nothing leaves the
 // exact result.  Replays after convergence return at once.  If ADJ_ITERS
 // replays have not settled, the sequential sweep runs from the initial dt.
+// A site's outputs are a function of its own initial dt and the entries it
+// reads, and equal their initial values while it is within a factor 2 of
+// every neighbour, so each replay walks only a work list: the ends of
+// out-of-bound pairs in the first, afterwards the sites whose entries the
+// previous replay lowered (awork, two alternating bytes per cell).
 // aflag[0..2]: changed flags of replays k % 3; [3] replays run; [4] fallback;
 // [5] settled (or nothing to do).
 constexpr int ADJ_ITERS = 24;
@@ -1073,7 +1083,7 @@ __global__ void k_adjust_replay(int n, int k, const int *__restrict__ off, const
                                 const int *__restrict__ lsort, const int *__restrict__ lpart,
                                 const unsigned char *__restrict__ act, const double *__restrict__ dt0,
                                 double *__restrict__ rdv, double *__restrict__ wrv, double *__restrict__ dtl,
-                                int *__restrict__ aflag) {
+                                int *__restrict__ aflag, unsigned char *__restrict__ work) {
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (aflag[5]) return;
   if (aflag[(k + 2) % 3] == 0) {  // the previous replay changed nothing (or none was needed)
@@ -1082,20 +1092,24 @@ __global__ void k_adjust_replay(int n, int k, const int *__restrict__ off, const
   }
   if (t0 == 0) { aflag[(k + 1) % 3] = 0; aflag[3] += 1; }
   bool changed = false;
+  unsigned char *cur = work + (size_t)(k & 1) * n, *nxt = work + (size_t)((k + 1) & 1) * n;
   for (int u = t0; u < n; u += gridDim.x * blockDim.x) {  // grid-stride: a settled replay costs one launch
+    if (!cur[u]) continue;  // inputs unchanged since u was last walked
+    cur[u] = 0;
     const unsigned char a = act[u];
     if (!(a & (A_ACTIVE | A_LNGB))) continue;
     const double d0 = dt0[u];
     if (d0 < 0.0) continue;  // boundary: neither swept nor relaxed
     const bool swept = (a & A_ACTIVE) != 0;
     const int q0 = off[u], q1 = off[u + 1];
-    double cur = d0;
+    double dtu = d0;
     bool own_done = !swept;
     auto own_slots = [&]() {  // the sweep at u's own position
       for (int q = q0; q < q1; q++) {
-        if (dt0[lfj_nb(lfj[q])] < 0.0) continue;
-        cur = smin(cur, 2.0 * rdv[q]);
-        if (cur < wrv[q]) { wrv[q] = cur; changed = true; }
+        const int v = lfj_nb(lfj[q]);
+        if (dt0[v] < 0.0) continue;
+        dtu = smin(dtu, 2.0 * rdv[q]);
+        if (dtu < wrv[q]) { wrv[q] = dtu; changed = true; nxt[v] = 1; }
       }
     };
     for (int t = q0; t < q1; t++) {  // neighbours in ascending index = sweep order
@@ -1104,12 +1118,12 @@ __global__ void k_adjust_replay(int n, int k, const int *__restrict__ off, const
       if (!own_done && v > u) { own_slots(); own_done = true; }
       if ((act[v] & A_ACTIVE) && dt0[v] >= 0.0) {  // the sweep at v's position, v's slot for this face
         const int p = lpart[q];
-        if (cur < rdv[p]) { rdv[p] = cur; changed = true; }
-        cur = smin(cur, 2.0 * wrv[p]);
+        if (dtu < rdv[p]) { rdv[p] = dtu; changed = true; nxt[v] = 1; }
+        dtu = smin(dtu, 2.0 * wrv[p]);
       }
     }
     if (!own_done) own_slots();
-    dtl[u] = cur;
+    dtl[u] = dtu;
   }
   if (changed) aflag[k % 3] = 1;
 }
@@ -1840,6 +1854,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc(c, &d.lsort, nl); rc |= dalloc(c, &d.lpart, nl);
   rc |= dalloc(c, &d.rdv, nl); rc |= dalloc(c, &d.wrv, nl); rc |= dalloc(c, &d.dt0, ncell);
   rc |= dalloc(c, &d.aflag, 8);
+  rc |= dalloc(c, &d.awork, 2 * (size_t)ncell);
   rc |= dalloc_bytes(c, &d.mnmx, 20 * c->rb * (size_t)ncell); rc |= dalloc(c, &d.mz, ncell);
   rc |= dalloc_bytes(c, &d.lia, c->rb * (size_t)nl);
   rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
@@ -2176,8 +2191,9 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(d.hash, 0, n, c->st));
     CK(cudaMemsetAsync(&d.S->iscal[4], 0, 4 * sizeof(int), c->st));
+    CK(cudaMemsetAsync(d.awork, 0, 2 * (size_t)n, c->st));
     k_adjust_mark<<<nblk(n, 128), 128, 0, c->st>>>(n, d.off, d.lnk, d.s12, d.act, d.bnd, d.dtl, d.hash,
-                                                   &d.S->iscal[4], d.act0);
+                                                   &d.S->iscal[4], d.act0, d.awork);
     LAUNCH_CHECK();
     const int nb = (int)((n + CB - 1) / CB);
     k_count_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount);
@@ -2193,7 +2209,7 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     LAUNCH_CHECK();
     for (int k = 0; k < ADJ_ITERS; k++) {
       k_adjust_replay<<<smin(nblk(n, 128), 148 * 16), 128, 0, c->st>>>(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv,
-                                                       d.wrv, d.dtl, d.aflag);
+                                                       d.wrv, d.dtl, d.aflag, d.awork);
       LAUNCH_CHECK();
     }
     k_adjust_restore<<<nblk(n, 256), 256, 0, c->st>>>(n, d.act, d.dt0, d.dtl, d.aflag, &d.S->iscal[6]);

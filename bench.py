@@ -152,7 +152,8 @@ def _cpu_worker(args):
     sys.path.insert(0, ROOT)
     import fvmhd3d_b200 as F
     from oracle import pyoracle
-    m = F.build_periodic(F.jittered_lattice(nside, 0.1, seed=seed), 1.0, nthreads=1)
+    pos = F.jittered_lattice(nside, 0.1, seed=seed)
+    m = F.build_periodic(pos[F.sort_local_data(pos, 1.0)], 1.0, nthreads=1)
     W = getattr(F.problems, problem)(m.pos)
     S = pyoracle.RefSystem() if kind == "reference" else pyoracle.OracleSystem()
     S.set_mesh(m)
@@ -182,7 +183,8 @@ def cpu_leg(nside, problem, steps, warmup, procs=None):
     t = max(r[1] for r in res)
     return {"value": faces / t, "unit": UNIT, "cores": P, "kind": kind,
             "sample": f"{P} concurrent single-rank processes, each {steps} global steps of the {problem} "
-                      f"on its own {nside}^3 jittered-lattice replica ({faces // (P * steps)} faces); no halo exchange"}
+                      f"on its own {nside}^3 jittered-lattice replica in Peano-Hilbert order ({faces // (P * steps)} faces); "
+                      f"no halo exchange"}
 
 
 # ---------------------------------------------------------------- GPU leg ---
@@ -228,13 +230,18 @@ def run_gpu(args):
         # static generators (the mesh is built once; generators that followed
         # the flow would need the mesh rebuilt every step)
         pos, box = F.problems.disk_generators(args.ncell, seed=3 + rank)
+        if args.order == "hilbert":  # the reference's sort_local_data
+            pos = pos[F.sort_local_data(pos, box)]
         m = F.build_periodic(pos, box)
         W, bnd = F.problems.disk(pos, box)
         sysargs = dict(gamma=1.0, courant=0.4, box=tuple(box), dtmax=1.0 / 16, eos=1, iso_GM=1.0, iso_cfac=0.05,
                        static_mesh=True)
         shared = False
     else:
-        m = F.build_periodic(F.jittered_lattice(args.nside, 0.1, seed=1 + rank), 1.0)
+        pos = F.jittered_lattice(args.nside, 0.1, seed=1 + rank)
+        if args.order == "hilbert":
+            pos = pos[F.sort_local_data(pos, 1.0)]
+        m = F.build_periodic(pos, 1.0)
         W = getattr(F.problems, args.problem)(m.pos)
         sysargs = {}
         shared = True
@@ -259,8 +266,10 @@ def run_gpu(args):
     S.set_profiling(True)
     n0 = S.launch_count
     prof_steps = max(2, min(args.steps, 5))
+    prof_cells = prof_faces = 0
     for _ in range(prof_steps):
-        S.step(shared=shared)
+        prof_cells += S.step(shared=shared)
+        prof_faces += S.active_face_count()
     torch.cuda.synchronize()
     launches_per_step = (S.launch_count - n0) / prof_steps
     ktimes = S.kernel_times()
@@ -328,7 +337,9 @@ def run_gpu(args):
     if dom:
         tot, calls = ktimes[dom]
         per_launch_s = tot / max(calls, 1) / 1e3
-        alg = kernel_bytes(dom, N, Fc, pb) or 0
+        # bytes of the mean step of the profiled pass: individual steps touch
+        # only their active cells and faces
+        alg = kernel_bytes(dom, prof_cells / prof_steps, prof_faces / prof_steps, pb) or 0
         ach = alg / per_launch_s / 1e9
         roofline = {"bound": "hbm", "kernel": dom, "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
                     "frac": round(ach / peak, 4), "peak_source": peak_kind,
@@ -349,7 +360,7 @@ def run_gpu(args):
                                 if shared else f"Keplerian disk {N} static generators, individual timesteps, ") +
                                f"{'plain FP64' if pb == 8 else 'FP32 bulk'} path",
                    "steps_mean_active_faces": round(faces / max(args.steps, 1), 1),
-                   "ncell": N, "nface_per_step": Fc, "faces_per_cell": round(Fc / N, 3),
+                   "ncell": N, "nface_per_step": Fc, "cell_order": args.order, "faces_per_cell": round(Fc / N, 3),
                    "l2": "inputs larger than L2 (state > 2 GB), no flush", "parallelism": f"replicas x{ws}",
                    "mesh_build_s": round(mesh_s, 2), "device_bytes": int(footprint), "autotuned": tuned},
         "roofline": roofline, "kernels": breakdown, "gpu_launches": launches, "e2e": e2e, "clocks": clocks,
@@ -444,6 +455,8 @@ def main():
     ap.add_argument("--nside", type=int, default=128)
     ap.add_argument("--ncell", type=int, default=1048576, help="generators of the disk workload")
     ap.add_argument("--problem", default="blast")
+    ap.add_argument("--order", default="hilbert", choices=["hilbert", "native"],
+                    help="cell order: Peano-Hilbert (the reference's sort_local_data) or as generated")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
     ap.add_argument("--cpu-nside", type=int, default=32)
     ap.add_argument("--cpu-steps", type=int, default=4)

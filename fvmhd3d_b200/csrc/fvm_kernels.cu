@@ -68,9 +68,6 @@ using namespace fvm;
 #ifndef FVM_LIMITER_STAGE
 #define FVM_LIMITER_STAGE 1  // default: limiter face records staged in shared memory per block
 #endif
-#ifndef FVM_RECON_LIA
-#define FVM_RECON_LIA 1  // the reconstruction reads its face weights from a per-link table
-#endif
 #ifndef FVM_ADJUST_REPLAY
 #define FVM_ADJUST_REPLAY 1  // adjust_timesteps by parallel replay (sequential sweep as fallback)
 #endif
@@ -116,7 +113,8 @@ struct Dev {
   int *aflag;               // adjust_timesteps replay flags
   unsigned char *awork;     // adjust_timesteps replay work lists (2 per cell)
   void *mnmx;               // per cell: the reconstruction's neighbour min and max (20 of the bulk type)
-  void *lia;                // per link: the reconstruction's face weight A / (2 dsh) (bulk type)
+  void *lrw;                // per link: the reconstruction's face weights (6, bulk type)
+  void *lrd;                // per link: the face centroid's offset from the cell (3, bulk type)
   unsigned char *mz;        // per cell: the reconstruction met a boundary (the limiter is zero)
   // learned-flux buffers (fvm_set_flux_mode)
   void *lX, *lY, *lface, *lcount, *lstats, *lhx, *lhy, *lhcount, *lnorm;
@@ -250,12 +248,16 @@ __device__ __forceinline__ double recon_ia(const double4 &g, double dsh) {
   return g.w * ((dsh != 0.0) ? 0.5 / dsh : 0.0);
 }
 
-// The reconstruction's face weights per link, computed once per mesh (the
-// division is the costliest step of its face loop).
+// The reconstruction's per-link records, computed once per mesh (the mesh is
+// fixed while it is installed).  The face term of the gradient,
+// ((wj + wi) dsh n + (wj - wi) (d - dsh n)) A / (2 dsh), becomes
+// (wj + wi) a + (wj - wi) b with a = dsh n A/(2 dsh), b = (d - dsh n) A/(2 dsh)
+// (lrw: a then b), and the limiter pass reads the min-image offset d (lrd).
+// The face loops then do no geometry, no division and one dependent load.
 template <typename R>
-__global__ void k_link_ia(int n, Params P, const int *__restrict__ off, const int2 *__restrict__ lfj,
-                          const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
-                          const double4 *__restrict__ dr2, R *__restrict__ lia) {
+__global__ void k_link_recon(int n, Params P, const int *__restrict__ off, const int2 *__restrict__ lfj,
+                             const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
+                             const double4 *__restrict__ dr2, R *__restrict__ lrw, R *__restrict__ lrd) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   for (int q = off[c]; q < off[c + 1]; q++) {
@@ -264,7 +266,14 @@ __global__ void k_link_ia(int n, Params P, const int *__restrict__ off, const in
     const double4 g = geo[fj.x];
     double d[3], nrm[3], dsh;
     recon_geom(P, own, g, own ? dr1[fj.x] : dr2[fj.x], d, nrm, dsh);
-    lia[q] = R(recon_ia(g, dsh));
+    const double ia = recon_ia(g, dsh);
+    R *w = lrw + 6 * (size_t)q, *o = lrd + 3 * (size_t)q;
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+      w[a] = R(nrm[a] * dsh * ia);
+      w[3 + a] = R((d[a] - nrm[a] * dsh) * ia);
+      o[a] = R(d[a]);
+    }
   }
 }
 
@@ -289,7 +298,7 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
   const R *ri = Wrec + 50 * (size_t)i + k0;
   R mn[KH], mx[KH], ln[KH], lq[KH], wi[KH];
 #pragma unroll
-  for (int k = 0; k < KH; k++) { mn[k] = R(0); mx[k] = R(0); ln[k] = R(1); lq[k] = R(1); wi[k] = ri[k]; }
+  for (int k = 0; k < KH; k++) { mn[k] = R(0); mx[k] = R(0); ln[k] = R(2); lq[k] = R(1); wi[k] = ri[k]; }
   const int q0 = off[i], q1 = off[i + 1];
   bool zero = false;
   if (reuse) {
@@ -330,8 +339,12 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
 #pragma unroll
     for (int k = 0; k < KH; k++) { to[k] = R(0); gx[k] = gy[k] = gz[k] = gt[k] = R(0); }
   } else {
+    R thr[KH];
 #pragma unroll
-    for (int k = 0; k < KH; k++) { gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k]; }
+    for (int k = 0; k < KH; k++) {
+      gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k];
+      thr[k] = limiter_thr(mn[k], mx[k]);
+    }
     // pass 2: limiter of the extrapolated difference at each active face
     FVM_CELL_LOOP
     for (int q = q0; q < q1; q++) {
@@ -358,12 +371,12 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
       for (int k = 0; k < KH; k++) {
         const R dWx = gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2];
         const R dW = dWx + gt[k] * dtt;
-        limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
+        limiter_ratio(ln[k], lq[k], dW, mn[k], mx[k], thr[k]);
       }
     }
 #pragma unroll
     for (int k = 0; k < KH; k++) {
-      const R tk = ln[k] / lq[k];
+      const R tk = limiter_finish(ln[k], lq[k]);
       to[k] = tk;
       gx[k] *= tk; gy[k] *= tk; gz[k] *= tk; gt[k] *= tk;
     }
@@ -470,7 +483,7 @@ __global__ void __launch_bounds__(128, FVM_LIMITER_MINB(R)) k_limiter_st(int n, 
   const R *mm = mnmx + 20 * (size_t)i + k0;
 #pragma unroll
   for (int k = 0; k < KH; k++) {
-    mn[k] = mm[k]; mx[k] = mm[10 + k]; ln[k] = R(1); lq[k] = R(1); wi[k] = ri[k];
+    mn[k] = mm[k]; mx[k] = mm[10 + k]; ln[k] = R(2); lq[k] = R(1); wi[k] = ri[k];
   }
   const bool zero = mz[i] != 0;
   const int q0 = soff[cl], q1 = soff[cl + 1];
@@ -479,8 +492,12 @@ __global__ void __launch_bounds__(128, FVM_LIMITER_MINB(R)) k_limiter_st(int n, 
 #pragma unroll
     for (int k = 0; k < KH; k++) { to[k] = R(0); gx[k] = gy[k] = gz[k] = gt[k] = R(0); }
   } else {
+    R thr[KH];
 #pragma unroll
-    for (int k = 0; k < KH; k++) { gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k]; }
+    for (int k = 0; k < KH; k++) {
+      gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k];
+      thr[k] = limiter_thr(mn[k], mx[k]);
+    }
     for (int l = q0; l < q1; l++) {
       if (!(sfk[l] & 1)) continue;
       const R d0 = sdx[l], d1 = sdy[l], d2 = sdz[l], dtt = st2[l];
@@ -488,12 +505,12 @@ __global__ void __launch_bounds__(128, FVM_LIMITER_MINB(R)) k_limiter_st(int n, 
       for (int k = 0; k < KH; k++) {
         const R dWx = gx[k] * d0 + gy[k] * d1 + gz[k] * d2;
         const R dW = dWx + gt[k] * dtt;
-        limiter_min(ln[k], lq[k], dW, mn[k], mx[k]);
+        limiter_ratio(ln[k], lq[k], dW, mn[k], mx[k], thr[k]);
       }
     }
 #pragma unroll
     for (int k = 0; k < KH; k++) {
-      const R tk = ln[k] / lq[k];
+      const R tk = limiter_finish(ln[k], lq[k]);
       to[k] = tk;
       gx[k] *= tk; gy[k] *= tk; gz[k] *= tk; gt[k] *= tk;
     }
@@ -1350,7 +1367,8 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm,
-    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lia) {
+    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw,
+    const R *__restrict__ lrd) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if ((t >> 1) >= n) return;
   const int c = perm[t >> 1];
@@ -1371,32 +1389,13 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
   R Wx[KH], Wy[KH], Wz[KH], mn[KH], mx[KH];
 #pragma unroll
   for (int k = 0; k < KH; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = R(0); }
-  double sc[3] = {0.0, 0.0, 0.0};
   bool zero = false;
   FVM_CELL_LOOP
   for (int q = q0; q < q1; q++) {
-#if FVM_CELL_LFJ
     const int2 fj = lfj[q];
-    const int f = fj.x;
-    const bool own = fj.y >= 0;
-    const int j = own ? fj.y : ~fj.y;
-#else
-    const int f = lnk[q];
-    const int2 e = s12[f];
-    const bool own = e.x == c;
-    const int j = own ? e.y : e.x;
-#endif
-    const double4 g = geo[f];
-    double d[3], nrm[3], dsh;
-    recon_geom(P, own, g, own ? dr1[f] : dr2[f], d, nrm, dsh);
-    sc[0] = sc[0] + d[0]; sc[1] = sc[1] + d[1]; sc[2] = sc[2] + d[2];
-    const R drh[3] = {R(nrm[0] * dsh), R(nrm[1] * dsh), R(nrm[2] * dsh)};
-    const R fij[3] = {R(d[0] - nrm[0] * dsh), R(d[1] - nrm[1] * dsh), R(d[2] - nrm[2] * dsh)};
-#if FVM_RECON_LIA
-    const R ia = lia[q];
-#else
-    const R ia = R(recon_ia(g, dsh));
-#endif
+    const int j = fj.y >= 0 ? fj.y : ~fj.y;
+    const R *w6 = lrw + 6 * (size_t)q;
+    const R a0 = w6[0], a1 = w6[1], a2 = w6[2], b0 = w6[3], b1 = w6[4], b2 = w6[5];
     if (bnd[j] != NO_BOUNDARY) { zero = true; break; }
     const R *Wj = Wst + 10 * (size_t)j + k0;
 #pragma unroll
@@ -1406,9 +1405,9 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
       const R diff = wj - Wi[k];
       mn[k] = smin(mn[k], diff);
       mx[k] = smax(mx[k], diff);
-      Wx[k] += (sum * drh[0] + diff * fij[0]) * ia;
-      Wy[k] += (sum * drh[1] + diff * fij[1]) * ia;
-      Wz[k] += (sum * drh[2] + diff * fij[2]) * ia;
+      Wx[k] += sum * a0 + diff * b0;
+      Wy[k] += sum * a1 + diff * b1;
+      Wz[k] += sum * a2 + diff * b2;
     }
   }
   // the next step's limiter pass 1 (neighbour min/max of the same states)
@@ -1424,33 +1423,28 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
     return;
   }
   const R invV = R(1.0 / cvol[c]);
-  R ln[KH], lq[KH];
+  R ln[KH], lq[KH], thr[KH];
 #pragma unroll
-  for (int k = 0; k < KH; k++) { Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; ln[k] = R(1); lq[k] = R(1); }
+  for (int k = 0; k < KH; k++) {
+    Wx[k] *= invV; Wy[k] *= invV; Wz[k] *= invV; ln[k] = R(2); lq[k] = R(1);
+    thr[k] = limiter_thr(mn[k], mx[k]);
+  }
+  double sc[3] = {0.0, 0.0, 0.0};
   FVM_CELL_LOOP
   for (int q = q0; q < q1; q++) {
-#if FVM_CELL_LFJ
-    const int2 fj = lfj[q];
-    const int f = fj.x;
-    const bool own = fj.y >= 0;
-#else
-    const int f = lnk[q];
-    const bool own = s12[f].x == c;
-#endif
-    const double4 o4 = own ? dr1[f] : dr2[f];
-    double d[3] = {o4.x, o4.y, o4.z};
-    if (own) wrap3(P, d);
-    const R dd[3] = {R(d[0]), R(d[1]), R(d[2])};
+    const R *o3 = lrd + 3 * (size_t)q;
+    const R dd[3] = {o3[0], o3[1], o3[2]};
+    sc[0] = sc[0] + double(dd[0]); sc[1] = sc[1] + double(dd[1]); sc[2] = sc[2] + double(dd[2]);
 #pragma unroll
     for (int k = 0; k < KH; k++) {
       const R dWx = Wx[k] * dd[0] + Wy[k] * dd[1] + Wz[k] * dd[2];
-      limiter_min(ln[k], lq[k], dWx, mn[k], mx[k]);
+      limiter_ratio(ln[k], lq[k], dWx, mn[k], mx[k], thr[k]);
     }
   }
   R tt[KH];
 #pragma unroll
   for (int k = 0; k < KH; k++) {
-    const R lm = ln[k] / lq[k];
+    const R lm = limiter_finish(ln[k], lq[k]);
     Wx[k] *= lm; Wy[k] *= lm; Wz[k] *= lm;
     tt[k] = r[40 + k] * lm;
   }
@@ -1856,7 +1850,8 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc(c, &d.aflag, 8);
   rc |= dalloc(c, &d.awork, 2 * (size_t)ncell);
   rc |= dalloc_bytes(c, &d.mnmx, 20 * c->rb * (size_t)ncell); rc |= dalloc(c, &d.mz, ncell);
-  rc |= dalloc_bytes(c, &d.lia, c->rb * (size_t)nl);
+  rc |= dalloc_bytes(c, &d.lrw, 6 * c->rb * (size_t)nl);
+  rc |= dalloc_bytes(c, &d.lrd, 3 * c->rb * (size_t)nl);
   rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
   if ((ncell + CB - 1) / CB > CB * 16) { c->err = "fvm_set_mesh: more than 16M cells"; return FVM_ERANGE; }
   rc |= dalloc(c, &d.pos, 3 * (size_t)ncell); rc |= dalloc(c, &d.vel, 3 * (size_t)ncell);
@@ -1988,7 +1983,8 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   CK(cudaMemsetAsync(d.tlast, 0, sizeof(double) * n, c->st));
   k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
   LAUNCH_CHECK();
-  BULK(k_link_ia<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.off, d.lfj, d.geo, d.dr1, d.dr2, (R *)d.lia));
+  BULK(k_link_recon<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.off, d.lfj, d.geo, d.dr1, d.dr2, (R *)d.lrw,
+                                                        (R *)d.lrd));
   LAUNCH_CHECK();
 
   BULK(k_init_state<R><<<nblk(n, 128), 128, 0, c->st>>>(n, dW, d.cvol, d.U, d.dU, (R *)d.Wrec, d.volp));
@@ -2277,7 +2273,7 @@ static int enq_recon(fvm_ctx *c) {
   BULK(k_recon<R><<<nblk(2LL * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
                                                             d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
                                                             (R *)d.Wrec, d.perm, (R *)d.mnmx, d.mz,
-                                                            (const R *)d.lia));
+                                                            (const R *)d.lrw, (const R *)d.lrd));
   LAUNCH_CHECK();
   kt_end(c, KT_RECON);
   return 0;

@@ -318,35 +318,32 @@ __device__ __forceinline__ T limiter(T dWi, T dWj_min, T dWj_max) {
   return flat ? T(1) : phi;
 }
 
-// Running minimum of limiter values, kept as a fraction n/q (q > 0) so that
-// each face costs one division (x = dWj/dWi) instead of two: Phi(x) is
-// n(x)/q(x) with q >= 2, and n1/q1 < n2/q2 <=> n1*q2 < n2*q1.  The caller
-// starts from n = q = 1 (the reference's initial 1.0) and finishes with one
-// division n/q per primitive.
-#ifndef FVM_LIMITER_DIVFREE
-#define FVM_LIMITER_DIVFREE 1
-#endif
+// Running minimum of the limiter over a cell's faces, with no division per
+// face.  Phi is increasing on [0, 2] (its derivative has the sign of
+// 4 + 4x - x^2 + e) and Phi(x) >= 1 exactly when x >= 2, so
+// min(1, min over faces of Phi(x_f)) = Phi(min(2, min over faces of x_f)),
+// a flat face counting as x_f = 2.  x_f = num/dWi >= 0 (num has the sign of
+// dWi) is kept as the fraction bn/bd = |num|/|dWi|, compared by
+// cross-multiplication; the caller starts from bn = 2, bd = 1 and ends with
+// limiter_finish, one evaluation of Phi.  thr = limiter_thr(min, max) is the
+// reference's flatness threshold, fixed over the face loop.  Where two faces'
+// ratios differ by less than rounding, the face kept may differ from the
+// reference's running minimum of rounded Phi values by a few units in the
+// last place.
 template <typename T>
-__device__ __forceinline__ void limiter_min(T &n, T &q, T dWi, T dWj_min, T dWj_max) {
-  const bool flat = fabs(dWi) <= T(1.0e-16) * smax(fabs(dWj_max), fabs(dWj_min));
-  const T num = dWi < T(0) ? dWj_min : dWj_max;
-  const T e = T(0.2 * 1.0e-16);
-  T pn, pq;
-#if FVM_LIMITER_DIVFREE
-  // Phi(m/d) = (m^2 + 2md + e d^2) / (m^2 + md + (2+e) d^2): no division per
-  // face.  Not flat means |d| > 1e-16 |m|, so neither part underflows for
-  // m != 0; m == 0 is Phi(0) = e/(2+e) exactly as in the reference.
-  const T m = num, d = dWi;
-  pn = m * m + T(2) * m * d + e * d * d;
-  pq = m * m + m * d + (T(2) + e) * d * d;
-  if (m == T(0)) { pn = e; pq = T(2) + e; }
-#else
-  const T x = num / (flat ? T(1) : dWi);
-  pn = x * x + T(2) * x + e;
-  pq = x * x + x + T(2) + e;
-#endif
-  if (flat) { pn = T(1); pq = T(1); }
-  if (pn * q < n * pq) { n = pn; q = pq; }
+__device__ __forceinline__ T limiter_thr(T dWj_min, T dWj_max) {
+  return T(1.0e-16) * smax(fabs(dWj_max), fabs(dWj_min));
+}
+template <typename T>
+__device__ __forceinline__ void limiter_ratio(T &bn, T &bd, T dWi, T dWj_min, T dWj_max, T thr) {
+  const T a = fabs(dWi < T(0) ? dWj_min : dWj_max), b = fabs(dWi);
+  if (b > thr && a * bd < bn * b) { bn = a; bd = b; }
+}
+template <typename T>
+__device__ __forceinline__ T limiter_finish(T bn, T bd) {
+  if (!(bn < T(2) * bd)) return T(1);
+  const T phi = Phi(bn / bd);
+  return phi < T(1) ? phi : T(1);
 }
 
 }  // namespace fvm

@@ -32,27 +32,14 @@
 using namespace fvm;
 
 // Minimum resident 128-thread blocks per SM for the face-flux kernels (caps
-// their registers: 3 -> 168 for FP64, 4 -> 128 for FP32, no spills) and for
-// the two-threads-per-cell kernels.
+// their registers: 3 -> 168 for FP64, 4 -> 128 for FP32, no spills).
 #ifndef FVM_FLUX_MINB_D
 #define FVM_FLUX_MINB_D 3
 #endif
 #ifndef FVM_FLUX_MINB_F
 #define FVM_FLUX_MINB_F 4
 #endif
-#ifndef FVM_CELL_MINB_D
-#define FVM_CELL_MINB_D 4
-#endif
-#ifndef FVM_CELL_MINB_F
-#define FVM_CELL_MINB_F 6
-#endif
-#define FVM_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CELL_MINB_F : FVM_CELL_MINB_D)
-#ifndef FVM_LIMITER_MINB_D
-#define FVM_LIMITER_MINB_D 3  // the staged FP64 limiter prefers registers to occupancy
-#endif
-#define FVM_LIMITER_MINB(R) (sizeof(R) == 4 ? FVM_CELL_MINB_F : FVM_LIMITER_MINB_D)
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
-// cell-kernel mappings: grouped (16 lanes per cell) or two threads per cell
 #ifndef FVM_CELL_LFJ
 #define FVM_CELL_LFJ 1  // cell kernels take (face, neighbour) from the link table instead of s12
 #endif
@@ -278,15 +265,26 @@ __global__ void k_link_recon(int n, Params P, const int *__restrict__ off, const
 }
 
 // ---- slope_limiter (MPI/compute_reconstruction.cpp:201-602) --------------
-// Two threads per imported cell, each owning five of the ten primitives: face
+// TPC threads per imported cell, each owning KH of the ten primitives: face
 // pass 1 (min/max of neighbour differences) and face pass 2 (limiter of the
 // space+time extrapolated difference) over the cell's active faces.  The
 // result tau is applied on the fly by the corrector, so Wrec is not modified.
 // R is the bulk type (double: plain path; float: FP32 path); face geometry
 // stays double and is rounded to R only where it multiplies bulk data.
-constexpr int KH = 5;  // primitives per thread in the two-threads-per-cell kernels
+// KH primitives per thread, TPC = 10 / KH threads per cell, and the blocks
+// per SM that the launch bounds ask for, per bulk type.  Timed on B200 on the
+// 128^3 blast: two primitives per thread (five threads per cell) give the
+// limiter and the FP64 reconstruction the occupancy that hides their loads;
+// the FP32 reconstruction is faster with five per thread.
+template <typename R> struct CellTune;
+template <> struct CellTune<double> {
+  static constexpr int KH_LIM = 2, MINB_LIM = 6, KH_REC = 2, MINB_REC = 8;
+};
+template <> struct CellTune<float> {
+  static constexpr int KH_LIM = 2, MINB_LIM = 8, KH_REC = 5, MINB_REC = 6;
+};
 
-template <typename R>
+template <typename R, int KH>
 __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double t_global,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
@@ -412,24 +410,25 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
   }
 }
 
-// Staged limiter: a block's CST cells (two threads each) first compute the
+// Staged limiter: a block's CST cells (TPC threads each) first compute the
 // per-face records of passes 2 and 3 (the side's offset dr, the two time
 // offsets, the face and its flags) for all their faces together, into shared
 // memory, so the face loops read no global memory but the cell's own record.
 // Used when the first pass is reused (every cell steps) and the block's faces
 // fit (LCAP); otherwise the block runs limiter_thread.
-constexpr int CST = 64;
-constexpr int LCAP = 1408;
-template <typename R>
-constexpr int limiter_stage_bytes() { return LCAP * (5 * (int)sizeof(R) + 4); }
+template <int KH> __host__ __device__ constexpr int limiter_cst() { return 128 / (10 / KH); }  // cells per block
+template <int KH> __host__ __device__ constexpr int limiter_lcap() { return 22 * limiter_cst<KH>(); }
+template <typename R, int KH>
+constexpr int limiter_stage_bytes() { return limiter_lcap<KH>() * (5 * (int)sizeof(R) + 4); }
 
-template <typename R>
-__global__ void __launch_bounds__(128, FVM_LIMITER_MINB(R)) k_limiter_st(int n, Params P, const Sched *__restrict__ S,
+template <typename R, int KH, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_limiter_st(int n, Params P, const Sched *__restrict__ S,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
     const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
+  constexpr int TPC = 10 / KH, CST = limiter_cst<KH>(), LCAP = limiter_lcap<KH>();
   extern __shared__ __align__(16) unsigned char lsm[];
   __shared__ int soff[CST + 1];
   const double t_global = S->t_global;
@@ -469,10 +468,10 @@ __global__ void __launch_bounds__(128, FVM_LIMITER_MINB(R)) k_limiter_st(int n, 
     }
   }
   __syncthreads();
-  const int cl = tid >> 1, k0 = (tid & 1) * KH;
-  if (c0 + cl >= n) return;
+  const int cl = tid / TPC, k0 = (tid % TPC) * KH;
+  if (cl >= CST || c0 + cl >= n) return;
   if (!staged) {
-    limiter_thread<R>(perm[c0 + cl], k0, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast, Wrec, tau,
+    limiter_thread<R, KH>(perm[c0 + cl], k0, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast, Wrec, tau,
                       fst, mnmx, mz);
     return;
   }
@@ -524,8 +523,8 @@ __global__ void __launch_bounds__(128, FVM_LIMITER_MINB(R)) k_limiter_st(int n, 
     for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * d0 + gy[k] * d1 + gz[k] * d2) + gt[k] * dtt);
   }
 }
-template <typename R>
-__global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params P, const Sched *__restrict__ S,
+template <typename R, int KH, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_limiter(int n, Params P, const Sched *__restrict__ S,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
@@ -536,9 +535,10 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_limiter(int n, Params
   // neighbour min/max of pass 1 are the reconstruction's (same states, same
   // faces, exact min/max)
   const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
+  constexpr int TPC = 10 / KH;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if ((t >> 1) >= n) return;
-  limiter_thread<R>(perm[t >> 1], (int)(t & 1) * KH, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
+  if (t / TPC >= n) return;
+  limiter_thread<R, KH>(perm[t / TPC], (int)(t % TPC) * KH, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
                     Wrec, tau, fst, mnmx, mz);
 }
 
@@ -1359,10 +1359,10 @@ __global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched 
 }
 
 // ---- compute_reconstruction (MPI/compute_reconstruction.cpp:41-198) -------
-// Two threads per active cell, five primitives each: Voronoi face gradient of
+// TPC threads per active cell, KH primitives each: Voronoi face gradient of
 // the updated primitives, local limiter, density positivity rescale.
-template <typename R>
-__global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P,
+template <typename R, int KH, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_recon(int n, Params P,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
@@ -1370,9 +1370,10 @@ __global__ void __launch_bounds__(128, FVM_CELL_MINB(R)) k_recon(int n, Params P
     R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw,
     const R *__restrict__ lrd) {
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if ((t >> 1) >= n) return;
-  const int c = perm[t >> 1];
-  const int k0 = (int)(t & 1) * KH;
+  constexpr int TPC = 10 / KH;
+  if (t / TPC >= n) return;
+  const int c = perm[t / TPC];
+  const int k0 = (int)(t % TPC) * KH;
   if (!(act[c] & A_ACTIVE)) return;
   R *r = Wrec + 50 * (size_t)c + k0;
   const R *wsi = Wst + 10 * (size_t)c + k0;
@@ -2111,17 +2112,21 @@ static int enq_limiter(fvm_ctx *c) {
     BULK(({
       static bool attr = false;
       if (!attr) {
-        CK(cudaFuncSetAttribute(k_limiter_st<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                limiter_stage_bytes<R>()));
+        CK(cudaFuncSetAttribute(k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                limiter_stage_bytes<R, CellTune<R>::KH_LIM>()));
         attr = true;
       }
-      k_limiter_st<R><<<nblk(c->n, CST), 128, limiter_stage_bytes<R>(), c->st>>>(
+      k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
+          <<<nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>()), 128, limiter_stage_bytes<R, CellTune<R>::KH_LIM>(),
+             c->st>>>(
           c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
           (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz);
     }));
   } else {
     const int bs = c->tune.bs_cell2;
-    BULK(k_limiter<R><<<nblk(2LL * c->n, bs), bs, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo,
+    BULK(k_limiter<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
+         <<<nblk((long long)(10 / CellTune<R>::KH_LIM) * c->n, bs), bs, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo,
                                                               d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
                                                               (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx,
                                                               d.mz));
@@ -2270,7 +2275,8 @@ static int enq_recon(fvm_ctx *c) {
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_CELL);
   kt_begin(c, KT_RECON);
-  BULK(k_recon<R><<<nblk(2LL * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
+  BULK(k_recon<R, CellTune<R>::KH_REC, CellTune<R>::MINB_REC>
+       <<<nblk((long long)(10 / CellTune<R>::KH_REC) * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
                                                             d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
                                                             (R *)d.Wrec, d.perm, (R *)d.mnmx, d.mz,
                                                             (const R *)d.lrw, (const R *)d.lrd));

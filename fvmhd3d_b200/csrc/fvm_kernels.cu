@@ -660,10 +660,27 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Par
   fcode[f] = code;
 }
 
+// The 14 contributions of face f as seven 2-wide loads (a face record is 112
+// bytes in FP64 and 56 in FP32, so every record starts on a 16- or 8-byte
+// boundary).
+__device__ __forceinline__ void load_contrib(const double *o, double *v) {
+  const double2 *o2 = reinterpret_cast<const double2 *>(o);
+#pragma unroll
+  for (int k = 0; k < 7; k++) { const double2 x = o2[k]; v[2 * k] = x.x; v[2 * k + 1] = x.y; }
+}
+__device__ __forceinline__ void load_contrib(const float *o, double *v) {
+  const float2 *o2 = reinterpret_cast<const float2 *>(o);
+#pragma unroll
+  for (int k = 0; k < 7; k++) { const float2 x = o2[k]; v[2 * k] = x.x; v[2 * k + 1] = x.y; }
+}
+
 // Sum of the face contributions of cell c in its face order (the reference
 // scatters in active-face order; both orders sum the same terms).  The FP32
 // path accumulates its single-precision contributions in double with
-// compensated (Kahan) summation.
+// compensated (Kahan) summation.  A face's record is loaded before its code
+// is tested and skipped faces add nothing (zero, or the Kahan state kept), so
+// each face costs one dependent load after the link table and two faces'
+// loads are in flight at once.
 template <typename R>
 __device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int2 *__restrict__ lfj,
                                                const R *__restrict__ fcon,
@@ -673,28 +690,30 @@ __device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int2
   double comp[14];
 #pragma unroll
   for (int k = 0; k < 14; k++) { s[k] = 0.0; comp[k] = 0.0; }
+#pragma unroll 2
   for (int q = q0; q < q1; q++) {
     const int2 fj = lfj[q];
     const int f = fj.x;
+    double v[14];
+    load_contrib(fcon + 14 * (size_t)f, v);
     const unsigned char code = fcode[f];
-    if (code & F_OFF) continue;
     // this cell is the face's i side when it is s1 and the face was not
     // swapped, or s2 and it was
     const bool is_i = (fj.y >= 0) != ((code & F_SWAP) != 0);
-    if (!is_i && skipj_allowed && (code & F_SKIPJ)) continue;
-    const R *o = fcon + 14 * (size_t)f;
+    const bool use = !(code & F_OFF) && !(!is_i && skipj_allowed && (code & F_SKIPJ));
     // U: i gets -F, j gets +F;  gradPsi and divB: i gets +, j gets -
+    // (a skipped face's record may hold anything, so it is never multiplied)
+    const double wu = is_i ? -1.0 : 1.0;
 #pragma unroll
     for (int k = 0; k < 14; k++) {
-      const double v = double(o[k]);
-      const double term = ((k < NF) == is_i) ? -v : v;
       if (kahan) {
+        const double term = ((k < NF) == is_i) ? -v[k] : v[k];
         const double y = term - comp[k];
         const double t = s[k] + y;
-        comp[k] = (t - s[k]) - y;
-        s[k] = t;
+        comp[k] = use ? (t - s[k]) - y : comp[k];
+        s[k] = use ? t : s[k];
       } else {
-        s[k] += term;
+        s[k] = fma(k < NF ? wu : -wu, use ? v[k] : 0.0, s[k]);  // exact: the weight is -1 or 1
       }
     }
   }

@@ -94,6 +94,7 @@ struct Dev {
   int *off, *lnk;
   int *perm;  // thread slot -> cell (face-count order inside windows of CPW cells)
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
+  int *flist, *fbcount; // ordered active-face list and its block offsets (partial steps)
   int2 *lfj;            // per link: face id, neighbour (~j when the cell is s2)
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
   double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
@@ -157,7 +158,8 @@ enum : unsigned char { FF_ACTIVE = 1, FF_BND1 = 2, FF_BND2 = 4 };
 // test never changes during this kernel.
 __global__ void k_faceflags(int nf, const int2 *__restrict__ s12, unsigned char *__restrict__ act,
                             const int *__restrict__ bnd, unsigned char *__restrict__ fflag,
-                            int *__restrict__ nface_active) {
+                            int *__restrict__ nface_active, unsigned char *__restrict__ fcode,
+                            unsigned char *__restrict__ fcode2) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   bool a = false;
   if (f < nf) {
@@ -169,6 +171,7 @@ __global__ void k_faceflags(int nf, const int2 *__restrict__ s12, unsigned char 
     if (b1) v |= FF_BND1;
     if (b2) v |= FF_BND2;
     fflag[f] = v;
+    if (!a) { fcode[f] = F_OFF; fcode2[f] = F_OFF; }  // the flux passes visit active faces only
     if (a1 != a2) {
       act[a1 ? e.y : e.x] = A_LNGB;
       act[a1 ? e.x : e.y] = A_ACTIVE | A_HASNGB;
@@ -596,7 +599,8 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Par
     const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
     const unsigned char *__restrict__ fflag, const int *__restrict__ bnd, const double *__restrict__ vel,
     const double *__restrict__ tlast, const R *__restrict__ Wrec, const R *__restrict__ fst,
-    R *__restrict__ fcon, unsigned char *__restrict__ fcode, LearnBuf lb) {
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode, LearnBuf lb, const int *__restrict__ flist,
+    int use_list) {
   const double t_global = S->t_global;
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   int slot = -1;
@@ -604,14 +608,24 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Par
     if (f >= *lb.count) return;
     slot = f;
     f = lb.gface[slot];
+  } else if (use_list) {  // the active faces (the others were coded F_OFF with the flags)
+    const int na = S->iscal[3];
+    if (f >= na) return;
+    if (na != nf) f = flist[f];  // the list is built only when some face is inactive
   } else if (f >= nf) {
     return;
   }
   const unsigned char ff = fflag[f];
-  if (!(ff & FF_ACTIVE)) { fcode[f] = F_OFF; return; }
+  if (!(ff & FF_ACTIVE)) return;  // coded F_OFF with the flags
   const int2 e = s12[f];
-  int i = e.x, j = e.y;
   const double4 g = geo[f], d = dr1[f];
+  R Wi[NF], Wj[NF];
+  {  // issued with the face record, before the boundary tests
+    const R *fs = fst + 20 * (size_t)f;
+#pragma unroll
+    for (int k = 0; k < NF; k++) { Wi[k] = fs[k]; Wj[k] = fs[10 + k]; }
+  }
+  int i = e.x, j = e.y;
   const double area = g.w;
   double nrm[3] = {g.x, g.y, g.z};
   double dri[3] = {d.x, d.y, d.z};
@@ -627,15 +641,10 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Par
   const double dtI = t_global - tlast[i], dtJ = t_global - tlast[j];
   const double dt = smin(dtI, dtJ);
   const double dsh = d.w;  // (-dri).(-n) = dri.n
-  R Wi[NF], Wj[NF];
-  if (jbnd) {
+  if (jbnd) {  // the extrapolated states were not written for a boundary face: replaced, never used
     const R *ri = Wrec + 50 * (size_t)i;
 #pragma unroll
     for (int k = 0; k < NF; k++) Wi[k] = Wj[k] = ri[k];
-  } else {
-    const R *fs = fst + 20 * (size_t)f;
-#pragma unroll
-    for (int k = 0; k < NF; k++) { Wi[k] = fs[k]; Wj[k] = fs[10 + k]; }
   }
   const double *vi = vel + 3 * (size_t)i, *vj = vel + 3 * (size_t)j;
   const double fij[3] = {dri[0] - nrm[0] * dsh, dri[1] - nrm[1] * dsh, dri[2] - nrm[2] * dsh};
@@ -1009,7 +1018,7 @@ __global__ void k_count_flags(int n, const unsigned char *__restrict__ flag, int
   if (threadIdx.x == 0) bcount[blockIdx.x] = bs;
 }
 __global__ void k_scan_counts(int nb, int *__restrict__ bcount, int *__restrict__ total) {
-  // one block of CB threads; nb <= CB * 16
+  // one block of CB threads, each summing ceil(nb / CB) consecutive counts
   __shared__ int part[CB];
   const int per = (nb + CB - 1) / CB;
   const int b0 = threadIdx.x * per;
@@ -1035,6 +1044,36 @@ __global__ void k_place_flags(int n, const unsigned char *__restrict__ flag, con
                               int *__restrict__ list) {
   const int i = blockIdx.x * CB + threadIdx.x;
   const bool v = i < n && flag[i];
+  __shared__ int wsum[CB / 32];
+  const unsigned b = __ballot_sync(0xffffffffu, v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(b);
+  __syncthreads();
+  int base = boff[blockIdx.x];
+  for (int k = 0; k < w; k++) base += wsum[k];
+  if (v) list[base + __popc(b & ((1u << lane) - 1u))] = i;
+}
+
+// The same compaction for the active faces (fflag & FF_ACTIVE); a no-op when
+// every face is active, where the flux passes map threads to faces directly.
+__global__ void k_count_faces(int nf, const unsigned char *__restrict__ fflag, const int *__restrict__ nactive,
+                              int *__restrict__ bcount) {
+  if (*nactive == nf) return;
+  const int i = blockIdx.x * CB + threadIdx.x;
+  const bool v = i < nf && (fflag[i] & FF_ACTIVE);
+  __shared__ int bs;
+  if (threadIdx.x == 0) bs = 0;
+  __syncthreads();
+  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, v));
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bs, (int)cnt);
+  __syncthreads();
+  if (threadIdx.x == 0) bcount[blockIdx.x] = bs;
+}
+__global__ void k_place_faces(int nf, const unsigned char *__restrict__ fflag, const int *__restrict__ nactive,
+                              const int *__restrict__ boff, int *__restrict__ list) {
+  if (*nactive == nf) return;
+  const int i = blockIdx.x * CB + threadIdx.x;
+  const bool v = i < nf && (fflag[i] & FF_ACTIVE);
   __shared__ int wsum[CB / 32];
   const unsigned b = __ballot_sync(0xffffffffu, v);
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1253,18 +1292,22 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Par
     const unsigned char *__restrict__ fflag, const int *__restrict__ bnd,
     const double *__restrict__ vel, const R *__restrict__ Wst,
     R *__restrict__ fcon, unsigned char *__restrict__ fcode, const Sched *__restrict__ S, const int *__restrict__ rung,
-    LearnBuf lb) {
+    LearnBuf lb, const int *__restrict__ flist, int use_list) {
   int f = blockIdx.x * blockDim.x + threadIdx.x;
   int slot = -1;
   if (MODE == LM_FINISH) {
     if (f >= *lb.count) return;
     slot = f;
     f = lb.gface[slot];
+  } else if (use_list) {  // the active faces (the others were coded F_OFF with the flags)
+    const int na = S->iscal[3];
+    if (f >= na) return;
+    if (na != nf) f = flist[f];  // the list is built only when some face is inactive
   } else if (f >= nf) {
     return;
   }
   const unsigned char ff = fflag[f];
-  if (!(ff & FF_ACTIVE)) { fcode[f] = F_OFF; return; }
+  if (!(ff & FF_ACTIVE)) return;  // coded F_OFF with the flags
   const int2 e = s12[f];
   int i = e.x, j = e.y;
   const double4 g = geo[f], d = dr1[f];
@@ -1633,6 +1676,9 @@ static const char *kKernelNames[KT_COUNT] = {"flags", "limiter", "corr_flux", "c
 
 struct fvm_ctx {
   int device;
+  // the flux passes walk the compacted active-face list (individual-timestep
+  // steps and the stage-by-stage entry points) or every face (global steps)
+  int use_flist = 1;
   // per-kernel CUDA-event timing (enabled by fvm_set_profiling)
   bool prof;
   cudaEvent_t kev[2 * KT_COUNT];
@@ -1883,6 +1929,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc_bytes(c, &d.Wrec, 50 * c->rb * (size_t)ncell);
   rc |= dalloc(c, &d.act0, ncell); rc |= dalloc(c, &d.act, ncell); rc |= dalloc(c, &d.hash, ncell);
   rc |= dalloc(c, &d.fcode, nface); rc |= dalloc(c, &d.fcode2, nface);
+  rc |= dalloc(c, &d.flist, nface); rc |= dalloc(c, &d.fbcount, (nface + CB - 1) / CB + 1);
   rc |= dalloc_bytes(c, &d.tau, 10 * c->rb * (size_t)ncell);
   rc |= dalloc_bytes(c, &d.fcon, 14 * c->rb * (size_t)nface);
   rc |= dalloc_bytes(c, &d.fcon2, 14 * c->rb * (size_t)nface);
@@ -2117,8 +2164,18 @@ static int enq_begin(fvm_ctx *c) {
   LAUNCH_CHECK();
   k_active<<<nblk(n, 256), 256, 0, c->st>>>(n, d.rung, d.S, d.act, &d.S->iscal[1]);
   LAUNCH_CHECK();
-  k_faceflags<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, d.s12, d.act, d.bnd, d.fflag, &d.S->iscal[3]);
+  k_faceflags<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, d.s12, d.act, d.bnd, d.fflag, &d.S->iscal[3], d.fcode,
+                                                    d.fcode2);
   LAUNCH_CHECK();
+  if (c->use_flist) {
+    const int nb = (int)((c->nf + CB - 1) / CB);
+    k_count_faces<<<nb, CB, 0, c->st>>>(c->nf, d.fflag, &d.S->iscal[3], d.fbcount);
+    LAUNCH_CHECK();
+    k_scan_counts<<<1, CB, 0, c->st>>>(nb, d.fbcount, &d.fbcount[nb]);
+    LAUNCH_CHECK();
+    k_place_faces<<<nb, CB, 0, c->st>>>(c->nf, d.fflag, &d.S->iscal[3], d.fbcount, d.flist);
+    LAUNCH_CHECK();
+  }
   kt_end(c, KT_FLAGS);
   return 0;
 }
@@ -2164,7 +2221,7 @@ static int enq_update(fvm_ctx *c) {
 #define CORR_FLUX(MODE, GRID)                                                                                   \
   BULK(k_corr_flux<R, MODE><<<GRID, c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, \
                                                      d.tlast, (const R *)d.Wrec, (const R *)d.fst, (R *)d.fcon,   \
-                                                     d.fcode, lb))
+                                                     d.fcode, lb, d.flist, c->use_flist))
   if (c->learn_mode == 1) {
     CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
     CORR_FLUX(LM_DEFER, nblk(c->nf, c->tune.bs_face));
@@ -2266,7 +2323,7 @@ static int enq_update0(fvm_ctx *c) {
 #define PRED_FLUX(MODE)                                                                                       \
   BULK(k_pred_flux<R, MODE><<<nblk(c->nf, c->tune.bs_face), c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
                                                                  d.vel, (const R *)d.Wst, (R *)d.fcon2, d.fcode2, \
-                                                                 d.S, d.rung, lb))
+                                                                 d.S, d.rung, lb, d.flist, c->use_flist))
   if (c->learn_mode == 1) {
     CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
     PRED_FLUX(LM_DEFER);
@@ -2321,6 +2378,7 @@ static int enq_end(fvm_ctx *c, int shared) {
 
 static int enq_step(fvm_ctx *c, int shared) {
   int rc;
+  c->use_flist = shared ? 0 : 1;  // a global step activates every face
   if ((rc = enq_begin(c))) return rc;
   if ((rc = enq_limiter(c))) return rc;
   if ((rc = enq_update(c))) return rc;
@@ -2354,6 +2412,7 @@ int fvm_begin_step(fvm_ctx *c) {
   if (!c || !c->have_state) { if (c) c->err = "fvm_begin_step: no state"; return FVM_ENOMESH; }
   if (c->in_step) { c->err = "fvm_begin_step: previous step not finished"; return FVM_EINVAL; }
   CK(cudaSetDevice(c->device));
+  c->use_flist = 1;
   int rc = enq_begin(c);
   if (rc) return rc;
   if ((rc = read_sched(c))) return rc;

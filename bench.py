@@ -72,12 +72,20 @@ def kernel_bytes(name, N, F, prec_bytes=8):
 # its face count.
 NCU_FACES_64 = 2085347
 NCU_TRAFFIC_64 = {
-    ("limiter", 8): 331.286272e6 + 310.062848e6, ("limiter", 4): 253.546752e6 + 135.535104e6,
-    ("corr_flux", 8): 494.430208e6 + 206.809088e6, ("corr_flux", 4): 327.699456e6 + 95.425536e6,
-    ("corr_cell", 8): 657.432320e6 + 31.601664e6, ("corr_cell", 4): 274.245888e6 + 38.991616e6,
-    ("pred_flux", 8): 179.952640e6 + 182.989056e6, ("pred_flux", 4): 169.291520e6 + 81.602048e6,
-    ("pred_cell", 8): 374.634496e6 + 24.192000e6, ("pred_cell", 4): 191.613952e6 + 18.486016e6,
-    ("recon", 8): 349.016064e6 + 116.758272e6, ("recon", 4): 315.905536e6 + 55.948800e6,
+    ("limiter", 8): 339.943424e6 + 310.681344e6, ("limiter", 4): 260.643328e6 + 141.116928e6,
+    ("corr_flux", 8): 495.774464e6 + 205.144320e6, ("corr_flux", 4): 328.350976e6 + 95.120896e6,
+    ("corr_cell", 8): 585.743360e6 + 31.117312e6, ("corr_cell", 4): 276.538368e6 + 36.321280e6,
+    ("pred_flux", 8): 181.332992e6 + 183.806464e6, ("pred_flux", 4): 170.044160e6 + 78.530304e6,
+    ("pred_cell", 8): 351.534336e6 + 24.011264e6, ("pred_cell", 4): 192.738048e6 + 15.876608e6,
+    ("recon", 8): 415.059200e6 + 132.006400e6, ("recon", 4): 243.856896e6 + 49.254144e6,
+}
+# FP64 floating-point operations per launch on the same 64^3 launches (ncu
+# thread-instruction counts: 2 per DFMA, 1 per DADD and DMUL; this includes
+# the FMAs inside the compiler's divide and square-root sequences).  The plain
+# FP64 path is compared with the measured FP64 FMA peak (fvm_fp64_peak).
+NCU_FP64_FLOPS_64 = {
+    "limiter": 0.8528e9, "corr_flux": 1.4451e9, "corr_cell": 0.2531e9, "pred_flux": 1.4389e9,
+    "pred_cell": 0.2497e9, "recon": 1.0849e9,
 }
 
 
@@ -259,6 +267,7 @@ def run_gpu(args):
         S.step(shared=shared)
     # launch choices by the library's autotuner (trial steps on a restored state)
     tuned = S.autotune(shared=shared, steps=3)
+    fp64_peak = S.fp64_peak() if prec == F.FVM_PREC_FP64 else None  # FLOP/s, measured on this GPU
     torch.cuda.synchronize()
     barrier(ws)
 
@@ -349,6 +358,22 @@ def run_gpu(args):
                     "traffic_source": "ncu dram bytes of the 64^3 blast launch, scaled by face count",
                     "step_bytes_per_face_update": round(step_bytes(N, Fc, pb), 1),
                     "step_frac": round(value / ws * step_bytes(N, Fc, pb) / 1e9 / peak, 4)}
+        if fp64_peak and shared and roofline:
+            # the FP64 roof: the same launches' FP64 operations (per face, scaled
+            # from the 64^3 counts) over the measured FMA throughput
+            scale = Fc / NCU_FACES_64
+            fl = {k: NCU_FP64_FLOPS_64[k] * scale for k in NCU_FP64_FLOPS_64}
+            kfl = {k: fl[k] / (ktimes[k][0] / max(ktimes[k][1], 1) / 1e3) for k in fl if k in ktimes}
+            step_fl = sum(NCU_FP64_FLOPS_64.values()) / NCU_FACES_64  # per face-update
+            roofline["fp64"] = {
+                "kernel": dom, "achieved": round(kfl.get(dom, 0.0) / 1e12, 3), "peak": round(fp64_peak / 1e12, 3),
+                "unit": "TFLOP/s", "frac": round(kfl.get(dom, 0.0) / fp64_peak, 4),
+                "flops_per_launch": int(fl.get(dom, 0)),
+                "per_kernel_frac": {k: round(v / fp64_peak, 4) for k, v in kfl.items()},
+                "step_flops_per_face_update": round(step_fl, 1),
+                "step_frac": round(value / ws * step_fl / fp64_peak, 4),
+                "source": "ncu FP64 instruction counts of the 64^3 blast launches scaled by face count; "
+                          "peak: fvm_fp64_peak (FMA chains, full occupancy, this GPU)"}
     breakdown = {k: {"ms_per_launch": round(v[0] / max(v[1], 1), 4), "share": round(v[0] / max(1e-9, sum(
         x[0] for x in ktimes.values())), 4)} for k, v in ktimes.items()}
 

@@ -78,6 +78,7 @@ SIGNATURES = {
     "fvm_last_adjust_stats": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "fvm_launch_count": (c_ll, [c_void_p]),
     "fvm_set_profiling": (c_int, [c_void_p, c_int]),
+    "fvm_fp64_peak": (c_int, [c_void_p, c_void_p]),
     "fvm_kernel_times": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_char_p), ctypes.POINTER(c_double),
                                  ctypes.POINTER(c_ll)]),
 }

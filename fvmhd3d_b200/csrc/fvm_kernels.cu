@@ -84,6 +84,7 @@ struct Sched {
   unsigned long long nactive_total, nfaces_total, steps;
   unsigned long long tprevU;  // tsysU before the last pull_active_list
   int mnmx_ok;                // the last step reconstructed every cell (its min/max are current)
+  double sink;                // written only by a calibration kernel, never in practice
 };
 
 struct Dev {
@@ -876,9 +877,11 @@ __global__ void k_pvel(int n, Params P, const unsigned char *__restrict__ act, c
 }
 
 // ---- compute_timestep(i) (MPI/compute_timestep.cpp:6-51) ------------------
-__device__ double cell_timestep(const Params &P, int i, bool with_faces, const int *off, const int *lnk,
-                                const int2 *s12, const int *bnd, const double *U, const double *volp,
-                                const double *vel) {
+// The face minimum min_f h / x_f is taken as h / max_f x_f: h > 0 and a
+// rounded quotient never increases with its divisor, so both give the same
+// double, with one division instead of one per face.
+__device__ double cell_timestep(const Params &P, int i, bool with_faces, const int *off, const int2 *lfj,
+                                const int *bnd, const double *U, const double *volp, const double *vel) {
   double W[NF];
   to_primitive(U + 10 * (size_t)i, volp[i], W);
   const double *pv = vel + 3 * (size_t)i;
@@ -896,17 +899,20 @@ __device__ double cell_timestep(const Params &P, int i, bool with_faces, const i
   double dti = h / (csi + vrel + 1.0 / FVM_HUGE);
   if (with_faces) {
     const double fac = b ? 0.0 : 1.0;
-    for (int q = off[i]; q < off[i + 1]; q++) {
-      const int2 e = s12[lnk[q]];
-      const int j = e.x == i ? e.y : e.x;
+    double xmax = 0.0;
+    const int q1 = off[i + 1];
+    for (int q = off[i]; q < q1; q++) {
+      const int2 fj = lfj[q];
+      const int j = fj.y >= 0 ? fj.y : ~fj.y;
       const double *vj = vel + 3 * (size_t)j;
       const double w3[3] = {(vj[0] + pv[0]) * 0.5, (vj[1] + pv[1]) * 0.5, (vj[2] + pv[2]) * 0.5};
       const double dw[3] = {vj[0] - pv[0], vj[1] - pv[1], vj[2] - pv[2]};
       const double r[3] = {W[VELX] - w3[0], W[VELY] - w3[1], W[VELZ] - w3[2]};
       const double rv = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
       const double dwa = sqrt(dw[0] * dw[0] + dw[1] * dw[1] + dw[2] * dw[2]);
-      dti = smin(dti, h / smax(fac * (csi + rv), 1.0 / FVM_HUGE + dwa));
+      xmax = smax(xmax, smax(fac * (csi + rv), 1.0 / FVM_HUGE + dwa));
     }
+    if (q1 > off[i]) dti = smin(dti, h / xmax);
   }
   return dti * P.courant;
 }
@@ -925,8 +931,8 @@ __device__ __forceinline__ void atomic_min_pos(double *addr, double v) {
 
 // compute_timesteps(false) first loops (MPI/compute_timestep.cpp:78-96); the
 // global minimum is reduced per warp before one atomic per warp
-__global__ void k_timestep(int n, Params P, const int *__restrict__ off, const int *__restrict__ lnk,
-                           const int2 *__restrict__ s12, const unsigned char *__restrict__ act,
+__global__ void k_timestep(int n, Params P, const int *__restrict__ off, const int2 *__restrict__ lfj,
+                           const unsigned char *__restrict__ act,
                            const int *__restrict__ bnd, const double *__restrict__ U,
                            const double *__restrict__ volp, const double *__restrict__ vel,
                            const double *__restrict__ pos, const double *__restrict__ tlast,
@@ -942,7 +948,7 @@ __global__ void k_timestep(int n, Params P, const int *__restrict__ off, const i
       dtl[i] = (tend[i] - tlast[i]) * (bnd[i] != NO_BOUNDARY ? -1.0 : 1.0);
     } else {
       const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
-                              cell_timestep(P, i, true, off, lnk, s12, bnd, U, volp, vel));
+                              cell_timestep(P, i, true, off, lfj, bnd, U, volp, vel));
       vmin = dti;
       dtl[i] = bnd[i] != NO_BOUNDARY ? -1.0 * dti : dti;
     }
@@ -970,8 +976,8 @@ __global__ void k_halve(int n, const unsigned char *__restrict__ act, const doub
 //  3. otherwise k_adjust_seq sweeps the ascending list of active
 //     non-boundary sites (compacted in parallel) in one thread, exactly as
 //     the reference does.
-__global__ void k_adjust_mark(int n, const int *__restrict__ off, const int *__restrict__ lnk,
-                              const int2 *__restrict__ s12, const unsigned char *__restrict__ act,
+__global__ void k_adjust_mark(int n, const int *__restrict__ off, const int2 *__restrict__ lfj,
+                              const unsigned char *__restrict__ act,
                               const int *__restrict__ bnd, const double *__restrict__ dtl,
                               unsigned char *__restrict__ hash, int *__restrict__ ndirty,
                               unsigned char *__restrict__ site, unsigned char *__restrict__ work) {
@@ -981,8 +987,8 @@ __global__ void k_adjust_mark(int n, const int *__restrict__ off, const int *__r
     s = true;
     const double di = dtl[i];
     for (int q = off[i]; q < off[i + 1]; q++) {
-      const int2 e = s12[lnk[q]];
-      const int j = e.x == i ? e.y : e.x;
+      const int2 fj = lfj[q];
+      const int j = fj.y >= 0 ? fj.y : ~fj.y;
       const double dj = dtl[j];
       if (dj < 0.0) continue;
       hash[j] = 1;
@@ -1608,7 +1614,7 @@ __global__ void k_init_dt(int n, Params P, const int *__restrict__ bnd, const do
   double vmin = FVM_HUGE;
   if (i < n)
     vmin = smin(extra_timestep(P, i, bnd, pos, vel),
-                cell_timestep(P, i, false, nullptr, nullptr, nullptr, bnd, U, volp, vel));
+                cell_timestep(P, i, false, nullptr, nullptr, bnd, U, volp, vel));
   for (int o = 16; o > 0; o >>= 1) vmin = smin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
   if ((threadIdx.x & 31) == 0) atomic_min_pos(dmin, vmin);
 }
@@ -2260,7 +2266,7 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
   Dev &d = c->d;
   const int n = c->n;
   kt_begin(c, KT_TIMESTEP);
-  k_timestep<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.off, d.lnk, d.s12, d.act, d.bnd, d.U, d.volp, d.vel,
+  k_timestep<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.off, d.lfj, d.act, d.bnd, d.U, d.volp, d.vel,
                                                d.pos, d.tlast, d.tend, d.dtl, &d.S->dtmin);
   LAUNCH_CHECK();
   if (!shared) {
@@ -2269,7 +2275,7 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     CK(cudaMemsetAsync(d.hash, 0, n, c->st));
     CK(cudaMemsetAsync(&d.S->iscal[4], 0, 4 * sizeof(int), c->st));
     CK(cudaMemsetAsync(d.awork, 0, 2 * (size_t)n, c->st));
-    k_adjust_mark<<<nblk(n, 128), 128, 0, c->st>>>(n, d.off, d.lnk, d.s12, d.act, d.bnd, d.dtl, d.hash,
+    k_adjust_mark<<<nblk(n, 128), 128, 0, c->st>>>(n, d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash,
                                                    &d.S->iscal[4], d.act0, d.awork);
     LAUNCH_CHECK();
     const int nb = (int)((n + CB - 1) / CB);
@@ -2613,6 +2619,47 @@ int fvm_last_adjust_stats(const fvm_ctx *c, int *dirty_sites, int *replays, int 
   if (dirty_sites) *dirty_sites = c->hS.iscal[4];
   if (replays) *replays = c->hS.iscal[6];
   if (sequential) *sequential = c->hS.iscal[7];
+  return 0;
+}
+
+// FP64 FMA throughput of the device, the denominator of the FP64 roofline:
+// a full-occupancy grid whose threads each run eight independent FMA chains
+// (a <- a * m + b, bounded for m < 1).  The final test never holds, so the
+// chains are live but nothing is stored.
+constexpr int FP64P_CHAINS = 8, FP64P_ITERS = 16384;
+__global__ void __launch_bounds__(256) k_fp64_peak(double m, double b, double *sink) {
+  double a[FP64P_CHAINS];
+#pragma unroll
+  for (int k = 0; k < FP64P_CHAINS; k++) a[k] = (double)(threadIdx.x + k) * 1e-3;
+#pragma unroll 16
+  for (int it = 0; it < FP64P_ITERS; it++)
+#pragma unroll
+    for (int k = 0; k < FP64P_CHAINS; k++) a[k] = fma(a[k], m, b);
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < FP64P_CHAINS; k++) s += a[k];
+  if (s == -1.0) *sink = s;
+}
+
+int fvm_fp64_peak(fvm_ctx *c, double *flops_per_s) {
+  if (!c || !flops_per_s || !c->d.S) { if (c) c->err = "fvm_fp64_peak: bad arguments"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  int sms = 0;
+  CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device));
+  const int blocks = sms * 8, threads = 256;
+  float best = 0.0f;
+  for (int rep = 0; rep < 4; rep++) {  // the first launch warms up; the fastest of the rest counts
+    CK(cudaEventRecord(c->ev0, c->st));
+    k_fp64_peak<<<blocks, threads, 0, c->st>>>(0.999999, 1e-6, &c->d.S->sink);
+    LAUNCH_CHECK();
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0.0f;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (rep > 0 && (best == 0.0f || ms < best)) best = ms;
+  }
+  const double flops = 2.0 * FP64P_CHAINS * (double)FP64P_ITERS * blocks * threads;
+  *flops_per_s = flops / (best * 1e-3);
   return 0;
 }
 

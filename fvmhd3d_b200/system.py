@@ -341,6 +341,12 @@ class System:
     def launch_count(self) -> int:
         return int(self.L.fvm_launch_count(self.h))
 
+    def fp64_peak(self) -> float:
+        """Measured FP64 FMA throughput of the device, FLOP/s."""
+        v = ctypes.c_double(0.0)
+        self._check(self.L.fvm_fp64_peak(self.h, ctypes.byref(v)), "fvm_fp64_peak")
+        return float(v.value)
+
     def set_profiling(self, on=True):
         self._check(self.L.fvm_set_profiling(self.h, int(bool(on))), "fvm_set_profiling")
 

@@ -271,6 +271,11 @@ int fvm_last_step_counts(const fvm_ctx *c, int *ncell_active, int *nface_active)
  * with a neighbour outside a factor 2, parallel replays run, and 1 if the
  * sequential sweep had to run instead (any pointer may be NULL). */
 int fvm_last_adjust_stats(const fvm_ctx *c, int *dirty_sites, int *replays, int *sequential);
+/* FP64 FMA throughput of the context's device in FLOP/s (2 per FMA), timed
+ * on a full-occupancy grid of independent FMA chains: the measured peak
+ * that FP64-bound kernels are compared with (after fvm_set_mesh).  No
+ * counterpart in the reference (a measurement aid). */
+int fvm_fp64_peak(fvm_ctx *c, double *flops_per_s);
 /* Number of kernels this context has launched so far. */
 long long fvm_launch_count(const fvm_ctx *c);
 /* Per-kernel CUDA-event timing: on != 0 enables it and clears the totals. */

@@ -259,6 +259,16 @@ def test_hilbert_ordered_blast_individual_timesteps_vs_oracle():
     assert_state_close(s.get_state(), o.get_state())
 
 
+def test_fp64_peak_is_plausible():
+    """The FP64 roofline's denominator: tens of TFLOP/s on a B200, and the
+    context still steps afterwards."""
+    m, W = setup_case(6, "alfven", seed=3)
+    s = gpu_system(m, W)
+    peak = s.fp64_peak()
+    assert 5e12 < peak < 2e14, peak
+    assert s.step(shared=True) == m.ncell
+
+
 def test_mesh_input_validation_keeps_the_context_usable():
     """Malformed meshes are rejected with FVM_EINVAL before any device work,
     and the context still takes a good mesh afterwards."""

@@ -267,7 +267,7 @@ def run_gpu(args):
         S.step(shared=shared)
     # launch choices by the library's autotuner (trial steps on a restored state)
     tuned = S.autotune(shared=shared, steps=3)
-    fp64_peak = S.fp64_peak() if prec == F.FVM_PREC_FP64 else None  # FLOP/s, measured on this GPU
+    fp64_peak = S.fp64_peak() if prec == F.FVM_PREC_FP64 and shared else None  # FLOP/s, this GPU
     torch.cuda.synchronize()
     barrier(ws)
 

@@ -443,6 +443,7 @@ def learned_leg(F, m, W, plain, steps, weights, stream_of):
                                     "momentum": float(rel[1:4].max()), "magnetic": float(rel[5:8].max())},
            "network_faces_fraction": stats["deferred"] / max(2 * faces, 1),
            "fallback_fraction": stats["fallback"] / max(stats["deferred"], 1),
+           "judged_mean_abs_scaled": stats["judged_mean_abs"], "judged_max_abs_scaled": stats["judged_max_abs"],
            "judged_rel_l1": stats["judged_rel_l1"],
            "dtype": "f32 bulk + bf16 network", "weights": "fvmhd3d_b200/data/flux_mlp.npz"}
     ref.close()

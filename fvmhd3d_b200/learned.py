@@ -29,6 +29,7 @@ import numpy as np
 
 from . import mesh as _mesh
 from . import problems
+from .ordering import sort_local_data
 from .system import FVM_PREC_FP32, FVM_PREC_FP64, MLP_NPARAM, System
 
 # gate: relative density and pressure jumps, normal Mach number in the face frame
@@ -53,9 +54,18 @@ def init_params(seed=0) -> np.ndarray:
     return p
 
 
-def harvest_run(problem, nside, steps, hstride, hcap, seed=1):
+def _lattice_mesh(nside, seed, order):
+    """Jittered-lattice periodic mesh with its cells in lattice order or in
+    Peano-Hilbert order (sort_local_data)."""
+    pos = _mesh.jittered_lattice(nside, 0.1, seed=seed)
+    if order == "hilbert":
+        pos = pos[sort_local_data(pos, 1.0)]
+    return _mesh.build_periodic(pos, 1.0)
+
+
+def harvest_run(problem, nside, steps, hstride, hcap, seed=1, order="native"):
     """(X, Y) harvested from an exact run (global timestep, FP32 bulk)."""
-    m = _mesh.build_periodic(_mesh.jittered_lattice(nside, 0.1, seed=seed), 1.0)
+    m = _lattice_mesh(nside, seed, order)
     W = getattr(problems, problem)(m.pos)
     s = System(precision=FVM_PREC_FP32)
     s.set_mesh(m)
@@ -70,14 +80,17 @@ def harvest_run(problem, nside, steps, hstride, hcap, seed=1):
 
 def harvest(scale=1.0):
     """About 20M pairs from the Alfven (32^3, 10 steps) and blast (64^3, 50
-    steps) workloads; `scale` shrinks the run sizes for tests."""
+    steps) workloads, each run once with its cells in lattice order and once
+    in Peano-Hilbert order: a face's orientation (which cell is s1) follows
+    the cell numbering, so the two orders give the network both orientations
+    of the same faces.  `scale` shrinks the run sizes for tests."""
     if scale >= 1.0:
-        runs = [("alfven", 32, 10, 1, 6_000_000), ("blast", 64, 50, 12, 16_000_000)]
+        runs = [("alfven", 32, 10, 2, 3_000_000), ("blast", 64, 50, 24, 8_000_000)]
     else:
-        runs = [("alfven", 16, 4, 1, 400_000), ("blast", 24, 10, 2, 1_000_000)]
+        runs = [("alfven", 16, 4, 2, 200_000), ("blast", 24, 10, 4, 500_000)]
     Xs, Ys = [], []
-    for problem, nside, steps, stride, cap in runs:
-        X, Y = harvest_run(problem, nside, steps, stride, cap)
+    for (problem, nside, steps, stride, cap), order in ((r, o) for r in runs for o in ("native", "hilbert")):
+        X, Y = harvest_run(problem, nside, steps, stride, cap, order=order)
         Xs.append(X)
         Ys.append(Y)
     return np.concatenate(Xs), np.concatenate(Ys)
@@ -147,12 +160,12 @@ def llf_dissipation(X):
     return D
 
 
-def holdout(model, problem="blast", nside=128, steps=20, hstride=64):
+def holdout(model, problem="blast", nside=128, steps=20, hstride=64, order="hilbert"):
     """The network on faces harvested from a run it was not trained on:
     mean and largest absolute error per output (scaled units), the targets'
     mean magnitude, the LLF dissipation's error, and the largest standardised
     input seen."""
-    X, Y = harvest_run(problem, nside, steps, hstride, 4_000_000)
+    X, Y = harvest_run(problem, nside, steps, hstride, 4_000_000, order=order)
     s = System()
     apply(s, model)
     P = predict(s, model, X)
@@ -167,14 +180,14 @@ def holdout(model, problem="blast", nside=128, steps=20, hstride=64):
             "max_std_input": float(z.max()), "max_std_input_feature": int(z.max(axis=0).argmax())}
 
 
-def evaluate(model, nside=128, steps=100, judge=1024):
+def evaluate(model, nside=128, steps=100, judge=1024, order="hilbert"):
     """The blast with the learned flux + FP32 bulk path against the plain
     FP64 path after `steps` global steps: relative L1 error per conserved
     variable, fallback and judged statistics, and face-updates/s of both."""
     import torch
-    m = _mesh.build_periodic(_mesh.jittered_lattice(nside, 0.1, seed=1), 1.0)
+    m = _lattice_mesh(nside, 1, order)
     W = problems.blast(m.pos)
-    out = {}
+    out = {"cell_order": order}
     states = {}
     for name, prec, mode in (("plain_fp64", FVM_PREC_FP64, 0), ("fp32", FVM_PREC_FP32, 0),
                              ("learned_fp32", FVM_PREC_FP32, 1)):
@@ -220,6 +233,8 @@ def main():
     ap.add_argument("--profile-rows", type=int, default=0, help="only run the network on N random rows")
     ap.add_argument("--eval-nside", type=int, default=128, help="blast lattice size of --evaluate")
     ap.add_argument("--eval-steps", type=int, default=100, help="global steps of --evaluate")
+    ap.add_argument("--eval-order", default="hilbert", choices=["hilbert", "native"],
+                    help="cell order of the --evaluate mesh")
     args = ap.parse_args()
     if args.profile_rows:
         s = System()
@@ -255,8 +270,8 @@ def main():
         if args.out:
             np.savez_compressed(args.out, loss=hist, gate=json.dumps(GATE), **model)
     if args.evaluate:
-        print(json.dumps({"holdout_blast128": holdout(model)}))
-        print(json.dumps(evaluate(model, nside=args.eval_nside, steps=args.eval_steps)))
+        print(json.dumps({"holdout_blast128": holdout(model, order=args.eval_order)}))
+        print(json.dumps(evaluate(model, nside=args.eval_nside, steps=args.eval_steps, order=args.eval_order)))
 
 
 if __name__ == "__main__":

@@ -85,6 +85,7 @@ struct Sched {
   unsigned long long tprevU;  // tsysU before the last pull_active_list
   int mnmx_ok;                // the last step reconstructed every cell (its min/max are current)
   double sink;                // written only by a calibration kernel, never in practice
+  int ninv;                   // cells in the involved-cell list of a partial step
 };
 
 struct Dev {
@@ -96,6 +97,7 @@ struct Dev {
   int *perm;  // thread slot -> cell (face-count order inside windows of CPW cells)
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
   int *flist, *fbcount; // ordered active-face list and its block offsets (partial steps)
+  int *clist, *cbcount; // ordered list of the step's active and neighbour cells, block offsets (partial steps)
   int2 *lfj;            // per link: face id, neighbour (~j when the cell is s2)
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
   double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
@@ -425,20 +427,18 @@ template <int KH> __host__ __device__ constexpr int limiter_lcap() { return 22 *
 template <typename R, int KH>
 constexpr int limiter_stage_bytes() { return limiter_lcap<KH>() * (5 * (int)sizeof(R) + 4); }
 
-template <typename R, int KH, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_limiter_st(int n, Params P, const Sched *__restrict__ S,
+// One block's CST cells (cell block cb); called by every thread of the block.
+template <typename R, int KH>
+__device__ __forceinline__ void limiter_st_block(int cb, int n, bool reuse, double t_global, int *soff,
+    unsigned char *lsm,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
     const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
   constexpr int TPC = 10 / KH, CST = limiter_cst<KH>(), LCAP = limiter_lcap<KH>();
-  extern __shared__ __align__(16) unsigned char lsm[];
-  __shared__ int soff[CST + 1];
-  const double t_global = S->t_global;
-  const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
   const int tid = threadIdx.x;
-  const int c0 = blockIdx.x * CST;
+  const int c0 = cb * CST;
   const int c1 = c0 + CST < n ? c0 + CST : n;
   const int L0 = off[c0], nL = off[c1] - L0;
   const bool staged = reuse && nL <= LCAP;  // uniform over the block
@@ -527,23 +527,50 @@ __global__ void __launch_bounds__(128, MINB) k_limiter_st(int n, Params P, const
     for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * d0 + gy[k] * d1 + gz[k] * d2) + gt[k] * dtt);
   }
 }
+
+// One block per CST cells; with only_all set (partial-step mode) the kernel
+// does nothing unless every cell is active this step, the case k_limiter's
+// list then skips.
+template <typename R, int KH, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_limiter_st(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
+    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
+    const unsigned char *__restrict__ act, const double *__restrict__ tlast,
+    const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz, int only_all) {
+  constexpr int CST = limiter_cst<KH>();
+  extern __shared__ __align__(16) unsigned char lsm[];
+  __shared__ int soff[CST + 1];
+  if (only_all && S->iscal[1] != n) return;
+  const double t_global = S->t_global;
+  const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
+  limiter_st_block<R, KH>(blockIdx.x, n, reuse, t_global, soff, lsm, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
+                          Wrec, tau, fst, perm, mnmx, mz);
+}
 template <typename R, int KH, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_limiter(int n, Params P, const Sched *__restrict__ S,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
-    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz, const int *__restrict__ clist,
+    int skip_if_all) {
+  if (skip_if_all && S->iscal[1] == n) return;  // the staged limiter has this step
   const double t_global = S->t_global;
   // every cell steps and every cell was reconstructed by the last step: the
   // neighbour min/max of pass 1 are the reconstruction's (same states, same
   // faces, exact min/max)
   const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
   constexpr int TPC = 10 / KH;
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (t / TPC >= n) return;
-  limiter_thread<R, KH>(perm[t / TPC], (int)(t % TPC) * KH, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
-                    Wrec, tau, fst, mnmx, mz);
+  // TPC threads per cell; in partial steps a fixed grid strides over clist
+  const long long cnt = (long long)TPC * (clist ? S->ninv : n);
+  const bool lst = clist && S->ninv != n;  // every cell involved: the list is the identity
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cnt;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int u = (int)(t / TPC);
+    limiter_thread<R, KH>(lst ? clist[u] : perm[u], (int)(t % TPC) * KH, reuse, t_global, off, lnk, lfj, s12, geo,
+                          dr1, fflag, act, tlast, Wrec, tau, fst, mnmx, mz);
+  }
 }
 
 
@@ -596,26 +623,11 @@ __device__ __forceinline__ bool learned_flux(const Params &P, const Sched *S, co
 }
 
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Params P, const Sched *__restrict__ S,
+__device__ __forceinline__ void corr_face(int f, int slot, double t_global, const Params &P, const Sched *__restrict__ S,
     const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
     const unsigned char *__restrict__ fflag, const int *__restrict__ bnd, const double *__restrict__ vel,
     const double *__restrict__ tlast, const R *__restrict__ Wrec, const R *__restrict__ fst,
-    R *__restrict__ fcon, unsigned char *__restrict__ fcode, LearnBuf lb, const int *__restrict__ flist,
-    int use_list) {
-  const double t_global = S->t_global;
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  int slot = -1;
-  if (MODE == LM_FINISH) {  // one deferred face per thread
-    if (f >= *lb.count) return;
-    slot = f;
-    f = lb.gface[slot];
-  } else if (use_list) {  // the active faces (the others were coded F_OFF with the flags)
-    const int na = S->iscal[3];
-    if (f >= na) return;
-    if (na != nf) f = flist[f];  // the list is built only when some face is inactive
-  } else if (f >= nf) {
-    return;
-  }
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode, const LearnBuf &lb) {
   const unsigned char ff = fflag[f];
   if (!(ff & FF_ACTIVE)) return;  // coded F_OFF with the flags
   const int2 e = s12[f];
@@ -668,6 +680,30 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Par
   o[10] = R(nrm[0] * pt); o[11] = R(nrm[1] * pt); o[12] = R(nrm[2] * pt);
   o[13] = R(double(Bn) * tarea);
   fcode[f] = code;
+}
+
+// One thread per face; in partial steps (use_list) a fixed grid strides over
+// the active-face list, so a step with few active faces launches few blocks.
+template <typename R, int MODE>
+__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Params P, const Sched *__restrict__ S,
+    const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
+    const unsigned char *__restrict__ fflag, const int *__restrict__ bnd, const double *__restrict__ vel,
+    const double *__restrict__ tlast, const R *__restrict__ Wrec, const R *__restrict__ fst,
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode, LearnBuf lb, const int *__restrict__ flist,
+    int use_list) {
+  const double t_global = S->t_global;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (MODE == LM_FINISH) {  // one deferred face per thread
+    if (t >= *lb.count) return;
+    corr_face<R, MODE>(lb.gface[t], t, t_global, P, S, s12, geo, dr1, fflag, bnd, vel, tlast, Wrec, fst, fcon, fcode, lb);
+  } else if (use_list) {  // the active faces (the others were coded F_OFF with the flags)
+    const int na = S->iscal[3];
+    for (int u = t; u < na; u += gridDim.x * blockDim.x)  // the list is built only when some face is inactive
+      corr_face<R, MODE>(na != nf ? flist[u] : u, -1, t_global, P, S, s12, geo, dr1, fflag, bnd, vel, tlast, Wrec,
+                         fst, fcon, fcode, lb);
+  } else if (t < nf) {
+    corr_face<R, MODE>(t, -1, t_global, P, S, s12, geo, dr1, fflag, bnd, vel, tlast, Wrec, fst, fcon, fcode, lb);
+  }
 }
 
 // The 14 contributions of face f as seven 2-wide loads (a face record is 112
@@ -731,18 +767,14 @@ __device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int2
 
 // ---- compute_update cell pass (MPI/compute_update.cpp:274-498) -----------
 template <typename R>
-__global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
+__device__ __forceinline__ void corr_cell_body(int c, double t_global, const Params &P,
+    const int *__restrict__ off, const int2 *__restrict__ lfj,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const double *__restrict__ pos, const double *__restrict__ tlast, double *__restrict__ volp,
     const R *__restrict__ Wrec, const R *__restrict__ tau,
     const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
     double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
-    unsigned long long *__restrict__ counters, const int *__restrict__ perm, float *__restrict__ divb) {
-  const double t_global = S->t_global;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int c = perm[t];
+    unsigned long long *__restrict__ counters, float *__restrict__ divb) {
   const unsigned char ac = act[c];
   if (!(ac & (A_ACTIVE | A_LNGB))) return;
   double s[14];
@@ -837,13 +869,33 @@ __global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched 
   for (int k = 0; k < NF; k++) Uo[k] = Un[k];
 }
 
+// One thread per cell; in partial steps a fixed grid strides over the
+// involved-cell list (clist, count ninv) instead of every cell.
+template <typename R>
+__global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const double *__restrict__ pos, const double *__restrict__ tlast, double *__restrict__ volp,
+    const R *__restrict__ Wrec, const R *__restrict__ tau,
+    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
+    double *__restrict__ U, double *__restrict__ dU, double *__restrict__ stepdU,
+    unsigned long long *__restrict__ counters, const int *__restrict__ perm, float *__restrict__ divb,
+    const int *__restrict__ clist) {
+  const double t_global = S->t_global;
+  const int cnt = clist ? S->ninv : n;
+  const bool lst = clist && cnt != n;  // every cell involved: the list is the identity
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x)
+    corr_cell_body<R>(lst ? clist[t] : perm[t], t_global, P, off, lfj, cvol, act, bnd, pos, tlast, volp, Wrec, tau,
+                      fcon, fcode, U, dU, stepdU, counters, divb);
+}
+
 // ---- compute_pvel (MPI/compute_pvel.cpp:5-52) -----------------------------
-__global__ void k_pvel(int n, Params P, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+__device__ __forceinline__ void pvel_body(int i, const Params &P, const unsigned char *__restrict__ act,
+                       const int *__restrict__ bnd,
                        const double *__restrict__ U, const double *__restrict__ volp,
                        const double *__restrict__ cvol, const double *__restrict__ ccen,
                        const double *__restrict__ pos, double *__restrict__ vel) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !(act[i] & A_ACTIVE)) return;
+  if (!(act[i] & A_ACTIVE)) return;
   if (P.static_mesh) {  // compute_pvel1 hook returning true (MPI/set_problem.cpp:61-72)
     double *vo = vel + 3 * (size_t)i;
     vo[0] = vo[1] = vo[2] = 0.0;
@@ -874,6 +926,18 @@ __global__ void k_pvel(int n, Params P, const unsigned char *__restrict__ act, c
   }
   double *vo = vel + 3 * (size_t)i;
   vo[0] = v[0]; vo[1] = v[1]; vo[2] = v[2];
+}
+
+// Every cell, or in partial steps the involved-cell list.
+__global__ void k_pvel(int n, Params P, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+                       const double *__restrict__ U, const double *__restrict__ volp,
+                       const double *__restrict__ cvol, const double *__restrict__ ccen,
+                       const double *__restrict__ pos, double *__restrict__ vel, const int *__restrict__ clist,
+                       const int *__restrict__ ninv) {
+  const int cnt = clist ? *ninv : n;
+  const bool lst = clist && cnt != n;  // every cell involved: the list is the identity
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x)
+    pvel_body(lst ? clist[t] : t, P, act, bnd, U, volp, cvol, ccen, pos, vel);
 }
 
 // ---- compute_timestep(i) (MPI/compute_timestep.cpp:6-51) ------------------
@@ -937,10 +1001,14 @@ __global__ void k_timestep(int n, Params P, const int *__restrict__ off, const i
                            const double *__restrict__ volp, const double *__restrict__ vel,
                            const double *__restrict__ pos, const double *__restrict__ tlast,
                            const double *__restrict__ tend, double *__restrict__ dtl,
-                           double *__restrict__ dmin) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+                           double *__restrict__ dmin, const int *__restrict__ clist, const int *__restrict__ ninv) {
+  // every cell, or in partial steps the involved-cell list (the dt of any
+  // other cell is never read)
   double vmin = FVM_HUGE;
-  if (i < n) {
+  const int cnt_ = clist ? *ninv : n;
+  const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
+  for (int t_ = blockIdx.x * blockDim.x + threadIdx.x; t_ < cnt_; t_ += gridDim.x * blockDim.x) {
+    const int i = lst ? clist[t_] : t_;
     const unsigned char a = act[i];
     if (!(a & (A_ACTIVE | A_LNGB))) {
       dtl[i] = FVM_HUGE;
@@ -949,7 +1017,7 @@ __global__ void k_timestep(int n, Params P, const int *__restrict__ off, const i
     } else {
       const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
                               cell_timestep(P, i, true, off, lfj, bnd, U, volp, vel));
-      vmin = dti;
+      vmin = smin(vmin, dti);
       dtl[i] = bnd[i] != NO_BOUNDARY ? -1.0 * dti : dti;
     }
   }
@@ -959,10 +1027,13 @@ __global__ void k_timestep(int n, Params P, const int *__restrict__ off, const i
 
 // dt >= 8 dt_min halving (MPI/compute_timestep.cpp:103-104)
 __global__ void k_halve(int n, const unsigned char *__restrict__ act, const double *__restrict__ dmin,
-                        double *__restrict__ dtl) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !(act[i] & A_ACTIVE)) return;
-  if (dtl[i] >= 8.0 * dmin[0]) dtl[i] *= 0.5;
+                        double *__restrict__ dtl, const int *__restrict__ clist, const int *__restrict__ ninv) {
+  const int cnt_ = clist ? *ninv : n;
+  const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
+  for (int t_ = blockIdx.x * blockDim.x + threadIdx.x; t_ < cnt_; t_ += gridDim.x * blockDim.x) {
+    const int i = lst ? clist[t_] : t_;
+    if ((act[i] & A_ACTIVE) && dtl[i] >= 8.0 * dmin[0]) dtl[i] *= 0.5;
+  }
 }
 
 // adjust_timesteps relaxation (MPI/compute_timestep.cpp:123-142).  The
@@ -980,11 +1051,17 @@ __global__ void k_adjust_mark(int n, const int *__restrict__ off, const int2 *__
                               const unsigned char *__restrict__ act,
                               const int *__restrict__ bnd, const double *__restrict__ dtl,
                               unsigned char *__restrict__ hash, int *__restrict__ ndirty,
-                              unsigned char *__restrict__ site, unsigned char *__restrict__ work) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  bool dirty = false, s = false;
-  if (i < n && (act[i] & A_ACTIVE) && bnd[i] == NO_BOUNDARY) {
-    s = true;
+                              unsigned char *__restrict__ site, unsigned char *__restrict__ work,
+                              const int *__restrict__ clist, const int *__restrict__ ninv) {
+  // site[] starts cleared; only the active non-boundary sites are marked
+  int ndirty_t = 0;
+  const int cnt_ = clist ? *ninv : n;
+  const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
+  for (int t_ = blockIdx.x * blockDim.x + threadIdx.x; t_ < cnt_; t_ += gridDim.x * blockDim.x) {
+    const int i = lst ? clist[t_] : t_;
+    if (!(act[i] & A_ACTIVE) || bnd[i] != NO_BOUNDARY) continue;
+    bool dirty = false;
+    site[i] = 1;
     const double di = dtl[i];
     for (int q = off[i]; q < off[i + 1]; q++) {
       const int2 fj = lfj[q];
@@ -997,14 +1074,13 @@ __global__ void k_adjust_mark(int n, const int *__restrict__ off, const int2 *__
         work[j] = 1;  // both ends of a pair outside a factor 2 start the replay's work list
       }
     }
-    if (dirty) work[i] = 1;
+    if (dirty) { work[i] = 1; ndirty_t++; }
   }
-  if (i < n) site[i] = s ? 1 : 0;
   __shared__ int bsum;
   if (threadIdx.x == 0) bsum = 0;
   __syncthreads();
-  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, dirty));
-  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bsum, (int)cnt);
+  for (int o = 16; o > 0; o >>= 1) ndirty_t += __shfl_xor_sync(0xffffffffu, ndirty_t, o);
+  if ((threadIdx.x & 31) == 0 && ndirty_t) atomicAdd(&bsum, ndirty_t);
   __syncthreads();
   if (threadIdx.x == 0 && bsum) atomicAdd(ndirty, bsum);
 }
@@ -1090,6 +1166,33 @@ __global__ void k_place_faces(int nf, const unsigned char *__restrict__ fflag, c
   if (v) list[base + __popc(b & ((1u << lane) - 1u))] = i;
 }
 
+// The cells a partial step works on (active, or inactive neighbours of
+// active cells), in index order.
+__global__ void k_count_cells(int n, const unsigned char *__restrict__ act, int *__restrict__ bcount) {
+  const int i = blockIdx.x * CB + threadIdx.x;
+  const bool v = i < n && (act[i] & (A_ACTIVE | A_LNGB));
+  __shared__ int bs;
+  if (threadIdx.x == 0) bs = 0;
+  __syncthreads();
+  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, v));
+  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bs, (int)cnt);
+  __syncthreads();
+  if (threadIdx.x == 0) bcount[blockIdx.x] = bs;
+}
+__global__ void k_place_cells(int n, const unsigned char *__restrict__ act, const int *__restrict__ boff,
+                              int *__restrict__ list) {
+  const int i = blockIdx.x * CB + threadIdx.x;
+  const bool v = i < n && (act[i] & (A_ACTIVE | A_LNGB));
+  __shared__ int wsum[CB / 32];
+  const unsigned b = __ballot_sync(0xffffffffu, v);
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (lane == 0) wsum[w] = __popc(b);
+  __syncthreads();
+  int base = boff[blockIdx.x];
+  for (int k = 0; k < w; k++) base += wsum[k];
+  if (v) list[base + __popc(b & ((1u << lane) - 1u))] = i;
+}
+
 __global__ void k_adjust_seq(const int *__restrict__ off, const int *__restrict__ lnk,
                              const int2 *__restrict__ s12, const int *__restrict__ alist,
                              const int *__restrict__ nsite, const int *__restrict__ ndirty,
@@ -1146,17 +1249,22 @@ __device__ __forceinline__ int lfj_nb(int2 fj) { return fj.y >= 0 ? fj.y : ~fj.y
 __global__ void k_adjust_init(int n, const int *__restrict__ off, const int2 *__restrict__ lfj,
                               const unsigned char *__restrict__ act, const int *__restrict__ ndirty,
                               const double *__restrict__ dtl, double *__restrict__ dt0, double *__restrict__ rdv,
-                              double *__restrict__ wrv, int *__restrict__ aflag) {
+                              double *__restrict__ wrv, int *__restrict__ aflag, const int *__restrict__ clist,
+                              const int *__restrict__ ninv) {
   if (*ndirty == 0) return;  // every pair is within a factor 2: nothing changes
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u == 0) aflag[2] = 1;  // replay 0 runs
-  if (u >= n || !(act[u] & (A_ACTIVE | A_LNGB))) return;
-  const double du = dtl[u];
-  dt0[u] = du;
-  for (int q = off[u]; q < off[u + 1]; q++) {
-    const int v = lfj_nb(lfj[q]);
-    rdv[q] = (act[v] & (A_ACTIVE | A_LNGB)) ? dtl[v] : du;
-    wrv[q] = du;
+  if (blockIdx.x == 0 && threadIdx.x == 0) aflag[2] = 1;  // replay 0 runs
+  const int cnt_ = clist ? *ninv : n;
+  const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
+  for (int t_ = blockIdx.x * blockDim.x + threadIdx.x; t_ < cnt_; t_ += gridDim.x * blockDim.x) {
+    const int u = lst ? clist[t_] : t_;
+    if (!(act[u] & (A_ACTIVE | A_LNGB))) continue;
+    const double du = dtl[u];
+    dt0[u] = du;
+    for (int q = off[u]; q < off[u + 1]; q++) {
+      const int v = lfj_nb(lfj[q]);
+      rdv[q] = (act[v] & (A_ACTIVE | A_LNGB)) ? dtl[v] : du;
+      wrv[q] = du;
+    }
   }
 }
 
@@ -1212,29 +1320,31 @@ __global__ void k_adjust_replay(int n, int k, const int *__restrict__ off, const
 // Not settled after ADJ_ITERS replays: restore the initial dt for the
 // sequential sweep.
 __global__ void k_adjust_restore(int n, const unsigned char *__restrict__ act, const double *__restrict__ dt0,
-                                 double *__restrict__ dtl, int *__restrict__ aflag, int *__restrict__ stats) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+                                 double *__restrict__ dtl, int *__restrict__ aflag, int *__restrict__ stats,
+                                 const int *__restrict__ clist, const int *__restrict__ ninv) {
   const bool fallback = !aflag[5] && aflag[(ADJ_ITERS - 1) % 3] != 0;
-  if (u == 0) { stats[0] = aflag[3]; stats[1] = fallback ? 1 : 0; }
+  const bool first = blockIdx.x == 0 && threadIdx.x == 0;
+  if (first) { stats[0] = aflag[3]; stats[1] = fallback ? 1 : 0; }
   if (!fallback) return;
-  if (u == 0) aflag[4] = 1;
-  if (u < n && (act[u] & (A_ACTIVE | A_LNGB))) dtl[u] = dt0[u];
+  if (first) aflag[4] = 1;
+  const int cnt_ = clist ? *ninv : n;
+  const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
+  for (int t_ = blockIdx.x * blockDim.x + threadIdx.x; t_ < cnt_; t_ += gridDim.x * blockDim.x) {
+    const int u = lst ? clist[t_] : t_;
+    if (act[u] & (A_ACTIVE | A_LNGB)) dtl[u] = dt0[u];
+  }
 }
 
 // rung assignment and inactive-neighbour promotion (MPI/compute_timestep.cpp
 // :144-199) fused with collect_results (MPI/distribute_work.cpp:676-713) and
 // the tlast/tend update of correct() (set_problem.cpp generic hook)
 template <typename R>
-__global__ void k_rungs(int n, Params P, const Sched *__restrict__ S, int shared,
+__device__ __forceinline__ void rungs_body(int i, double t_global, int min_rung, const Params &P, int shared,
                         const unsigned char *__restrict__ act, const unsigned char *__restrict__ hash,
                         const double *__restrict__ dtl, const double *__restrict__ dmin,
                         int *__restrict__ rung, double *__restrict__ tlast, double *__restrict__ tend,
                         R *__restrict__ Wrec, int *__restrict__ iscal, const double *__restrict__ vel,
                         double *__restrict__ opos, double *__restrict__ ovel) {
-  const double t_global = S->t_global;
-  const int min_rung = S->min_rung;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
   const unsigned char a = act[i];
   if (!(a & (A_ACTIVE | A_LNGB))) return;
   if (a & A_ACTIVE) {
@@ -1279,39 +1389,48 @@ __global__ void k_rungs(int n, Params P, const Sched *__restrict__ S, int shared
   }
 }
 
+// Every cell, or in partial steps the involved-cell list.
+template <typename R>
+__global__ void k_rungs(int n, Params P, const Sched *__restrict__ S, int shared,
+                        const unsigned char *__restrict__ act, const unsigned char *__restrict__ hash,
+                        const double *__restrict__ dtl, const double *__restrict__ dmin,
+                        int *__restrict__ rung, double *__restrict__ tlast, double *__restrict__ tend,
+                        R *__restrict__ Wrec, int *__restrict__ iscal, const double *__restrict__ vel,
+                        double *__restrict__ opos, double *__restrict__ ovel, const int *__restrict__ clist) {
+  const double t_global = S->t_global;
+  const int min_rung = S->min_rung;
+  const int cnt = clist ? S->ninv : n;
+  const bool lst = clist && cnt != n;  // every cell involved: the list is the identity
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x)
+    rungs_body<R>(lst ? clist[t] : t, t_global, min_rung, P, shared, act, hash, dtl, dmin, rung, tlast, tend, Wrec,
+                  iscal, vel, opos, ovel);
+}
+
 // distribute_fluid_update_data: primitives of the updated state
 template <typename R>
 __global__ void k_wst(int n, const unsigned char *__restrict__ act, const double *__restrict__ U,
-                      const double *__restrict__ volp, R *__restrict__ Wst) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n || !(act[i] & (A_ACTIVE | A_LNGB))) return;
-  double W[NF];
-  to_primitive(U + 10 * (size_t)i, volp[i], W);
+                      const double *__restrict__ volp, R *__restrict__ Wst, const int *__restrict__ clist,
+                      const int *__restrict__ ninv) {
+  const int cnt = clist ? *ninv : n;  // every cell, or in partial steps the involved-cell list
+  const bool lst = clist && cnt != n;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+    const int i = lst ? clist[t] : t;
+    if (!(act[i] & (A_ACTIVE | A_LNGB))) continue;
+    double W[NF];
+    to_primitive(U + 10 * (size_t)i, volp[i], W);
 #pragma unroll
-  for (int k = 0; k < NF; k++) Wst[10 * (size_t)i + k] = R(W[k]);
+    for (int k = 0; k < NF; k++) Wst[10 * (size_t)i + k] = R(W[k]);
+  }
 }
 
 // ---- compute_update0 face pass (MPI/compute_update.cpp:713-810) ----------
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Params P,
+__device__ __forceinline__ void pred_face(int f, int slot, const Params &P,
     const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
     const unsigned char *__restrict__ fflag, const int *__restrict__ bnd,
     const double *__restrict__ vel, const R *__restrict__ Wst,
     R *__restrict__ fcon, unsigned char *__restrict__ fcode, const Sched *__restrict__ S, const int *__restrict__ rung,
-    LearnBuf lb, const int *__restrict__ flist, int use_list) {
-  int f = blockIdx.x * blockDim.x + threadIdx.x;
-  int slot = -1;
-  if (MODE == LM_FINISH) {
-    if (f >= *lb.count) return;
-    slot = f;
-    f = lb.gface[slot];
-  } else if (use_list) {  // the active faces (the others were coded F_OFF with the flags)
-    const int na = S->iscal[3];
-    if (f >= na) return;
-    if (na != nf) f = flist[f];  // the list is built only when some face is inactive
-  } else if (f >= nf) {
-    return;
-  }
+    const LearnBuf &lb) {
   const unsigned char ff = fflag[f];
   if (!(ff & FF_ACTIVE)) return;  // coded F_OFF with the flags
   const int2 e = s12[f];
@@ -1362,22 +1481,39 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Par
   fcode[f] = code;
 }
 
+// One thread per face; a fixed grid strides over the active-face list in
+// partial steps (see k_corr_flux).
+template <typename R, int MODE>
+__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Params P,
+    const int2 *__restrict__ s12, const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
+    const unsigned char *__restrict__ fflag, const int *__restrict__ bnd,
+    const double *__restrict__ vel, const R *__restrict__ Wst,
+    R *__restrict__ fcon, unsigned char *__restrict__ fcode, const Sched *__restrict__ S, const int *__restrict__ rung,
+    LearnBuf lb, const int *__restrict__ flist, int use_list) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (MODE == LM_FINISH) {
+    if (t >= *lb.count) return;
+    pred_face<R, MODE>(lb.gface[t], t, P, s12, geo, dr1, fflag, bnd, vel, Wst, fcon, fcode, S, rung, lb);
+  } else if (use_list) {
+    const int na = S->iscal[3];
+    for (int u = t; u < na; u += gridDim.x * blockDim.x)
+      pred_face<R, MODE>(na != nf ? flist[u] : u, -1, P, s12, geo, dr1, fflag, bnd, vel, Wst, fcon, fcode, S, rung, lb);
+  } else if (t < nf) {
+    pred_face<R, MODE>(t, -1, P, s12, geo, dr1, fflag, bnd, vel, Wst, fcon, fcode, S, rung, lb);
+  }
+}
+
 // ---- compute_update0 cell pass + collect_reconstruction -------------------
 // (MPI/compute_update.cpp:812-964; MPI/distribute_work.cpp:820-834)
 // Writes the predicted time derivative t into the cell's Wrec and the
 // cell's final rung/tend.  Arithmetic in double for both bulk types.
 template <typename R>
-__global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched *__restrict__ S,
-    const int *__restrict__ off, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
+__device__ __forceinline__ void pred_cell_body(int c, double t_global, int min_rung, const Params &P,
+    const int *__restrict__ off, const int2 *__restrict__ lfj,
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const double *__restrict__ pos, const double *__restrict__ U,
     const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
-    int *__restrict__ rung, double *__restrict__ tend, R *__restrict__ Wrec, const int *__restrict__ perm) {
-  const double t_global = S->t_global;
-  const int min_rung = S->min_rung;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
-  const int c = perm[t];
+    int *__restrict__ rung, double *__restrict__ tend, R *__restrict__ Wrec) {
   if (!(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
   const double V = cvol[c];
   double dot[14];
@@ -1426,22 +1562,32 @@ __global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched 
   tend[c] = t_global + get_dt(P, rf);
 }
 
+// One thread per cell; in partial steps a fixed grid strides over clist.
+template <typename R>
+__global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const double *__restrict__ pos, const double *__restrict__ U,
+    const R *__restrict__ fcon, const unsigned char *__restrict__ fcode,
+    int *__restrict__ rung, double *__restrict__ tend, R *__restrict__ Wrec, const int *__restrict__ perm,
+    const int *__restrict__ clist) {
+  const double t_global = S->t_global;
+  const int min_rung = S->min_rung;
+  const int cnt = clist ? S->ninv : n;
+  const bool lst = clist && cnt != n;  // every cell involved: the list is the identity
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x)
+    pred_cell_body<R>(lst ? clist[t] : perm[t], t_global, min_rung, P, off, lfj, cvol, act, bnd, pos, U, fcon,
+                      fcode, rung, tend, Wrec);
+}
+
 // ---- compute_reconstruction (MPI/compute_reconstruction.cpp:41-198) -------
 // TPC threads per active cell, KH primitives each: Voronoi face gradient of
 // the updated primitives, local limiter, density positivity rescale.
-template <typename R, int KH, int MINB>
-__global__ void __launch_bounds__(128, MINB) k_recon(int n, Params P,
-    const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
-    const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const double4 *__restrict__ dr2,
-    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
-    const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm,
-    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw,
-    const R *__restrict__ lrd) {
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  constexpr int TPC = 10 / KH;
-  if (t / TPC >= n) return;
-  const int c = perm[t / TPC];
-  const int k0 = (int)(t % TPC) * KH;
+template <typename R, int KH>
+__device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const int *__restrict__ off,
+    const int2 *__restrict__ lfj, const double *__restrict__ cvol, const unsigned char *__restrict__ act,
+    const int *__restrict__ bnd, const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec,
+    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw, const R *__restrict__ lrd) {
   if (!(act[c] & A_ACTIVE)) return;
   R *r = Wrec + 50 * (size_t)c + k0;
   const R *wsi = Wst + 10 * (size_t)c + k0;
@@ -1531,6 +1677,25 @@ __global__ void __launch_bounds__(128, MINB) k_recon(int n, Params P,
   for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = Wx[k]; r[20 + k] = Wy[k]; r[30 + k] = Wz[k]; r[40 + k] = tt[k]; }
 }
 
+// TPC threads per cell; in partial steps a fixed grid strides over clist.
+template <typename R, int KH, int MINB>
+__global__ void __launch_bounds__(128, MINB) k_recon(int n, Params P, const Sched *__restrict__ S,
+    const int *__restrict__ off, const int2 *__restrict__ lfj,
+    const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
+    const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm,
+    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw,
+    const R *__restrict__ lrd, const int *__restrict__ clist) {
+  constexpr int TPC = 10 / KH;
+  const long long cnt = (long long)TPC * (clist ? S->ninv : n);
+  const bool lst = clist && S->ninv != n;  // every cell involved: the list is the identity
+  for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < cnt;
+       t += (long long)gridDim.x * blockDim.x) {
+    const int u = (int)(t / TPC);
+    recon_body<R, KH>(lst ? clist[u] : perm[u], (int)(t % TPC) * KH, P, off, lfj, cvol, act, bnd, Wst, rung, Wrec,
+                      mnmx, mz, lrw, lrd);
+  }
+}
+
 // Per link (a cell's entry in its face list, i.e. one side of a face), in the
 // order the cell walks its faces: the face id and the neighbour j, stored as
 // ~j when the cell is s2.  The mesh is fixed while it is installed.
@@ -1599,11 +1764,18 @@ __global__ void k_sched_set(Params P, Sched *S, unsigned long long tsysU, int re
   }
 }
 
+// Largest rung: a grid-stride maximum, one atomic per block.
 __global__ void k_maxrung(int n, const int *__restrict__ rung, int *__restrict__ out) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  int r = i < n ? rung[i] : 0;
+  int r = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) r = max(r, rung[i]);
   for (int o = 16; o > 0; o >>= 1) r = max(r, __shfl_xor_sync(0xffffffffu, r, o));
-  if ((threadIdx.x & 31) == 0) atomicMax(out, r);
+  __shared__ int wm[32];
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); w++) r = max(r, wm[w]);
+    atomicMax(out, r);
+  }
 }
 
 // ---- init: compute_pvel + compute_timesteps(true) -------------------------
@@ -1682,6 +1854,7 @@ static const char *kKernelNames[KT_COUNT] = {"flags", "limiter", "corr_flux", "c
 
 struct fvm_ctx {
   int device;
+  int sms = 148;  // SMs of the device (sizes the fixed grids of partial steps)
   // the flux passes walk the compacted active-face list (individual-timestep
   // steps and the stage-by-stage entry points) or every face (global steps)
   int use_flist = 1;
@@ -1812,6 +1985,16 @@ static int dalloc_bytes(fvm_ctx *c, void **p, size_t bytes) {
     }                              \
   } while (0)
 
+// Grid of a kernel that strides over a device-side count of items (at most
+// `items`): in partial steps (use_flist) a fixed grid of two full waves
+// (4096 threads per SM), so a step with few active items launches few blocks
+// and a step with many still fills every SM; otherwise one thread per item.
+static int sgrid(const fvm_ctx *c, long long items, int bs) {
+  const int g = nblk(items, bs);
+  const int cap = c->sms * (4096 / bs);
+  return (c->use_flist && g > cap) ? cap : g;
+}
+
 static void drop_graphs(fvm_ctx *c) {
   for (int k = 0; k < 2; k++)
     if (c->graph[k]) {
@@ -1833,6 +2016,8 @@ fvm_ctx *fvm_create(const fvm_params *p, int device) {
   if (!p) return nullptr;
   fvm_ctx *c = new fvm_ctx();
   c->device = device;
+  if (cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || c->sms <= 0)
+    c->sms = 148;
   for (int k = 0; k < 48; k++)  // identity standardisation until fvm_mlp_set_norm
     c->h_norm[k] = (k < 16 || (k >= 32 && k < 40)) ? 0.0f : 1.0f;
   c->prm = *p;
@@ -1936,6 +2121,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc(c, &d.act0, ncell); rc |= dalloc(c, &d.act, ncell); rc |= dalloc(c, &d.hash, ncell);
   rc |= dalloc(c, &d.fcode, nface); rc |= dalloc(c, &d.fcode2, nface);
   rc |= dalloc(c, &d.flist, nface); rc |= dalloc(c, &d.fbcount, (nface + CB - 1) / CB + 1);
+  rc |= dalloc(c, &d.clist, ncell); rc |= dalloc(c, &d.cbcount, (ncell + CB - 1) / CB + 1);
   rc |= dalloc_bytes(c, &d.tau, 10 * c->rb * (size_t)ncell);
   rc |= dalloc_bytes(c, &d.fcon, 14 * c->rb * (size_t)nface);
   rc |= dalloc_bytes(c, &d.fcon2, 14 * c->rb * (size_t)nface);
@@ -2034,7 +2220,7 @@ static int read_sched(fvm_ctx *c) {
 // Rung maximum over all cells into S->iscal[0] (the next step's max_rung).
 static int enqueue_maxrung(fvm_ctx *c) {
   CK(cudaMemsetAsync(&c->d.S->iscal[0], 0, sizeof(int), c->st));
-  k_maxrung<<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, c->d.rung, &c->d.S->iscal[0]);
+  k_maxrung<<<smin(nblk(c->n, 256), 4 * c->sms), 256, 0, c->st>>>(c->n, c->d.rung, &c->d.S->iscal[0]);
   LAUNCH_CHECK();
   return 0;
 }
@@ -2064,7 +2250,8 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   LAUNCH_CHECK();
   // compute_pvel on all cells, then the shared timestep
   CK(cudaMemsetAsync(d.act, A_ACTIVE, n, c->st));
-  k_pvel<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel);
+  k_pvel<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel, nullptr,
+                                          nullptr);
   LAUNCH_CHECK();
   CK(cudaMemcpyAsync(d.opos, d.pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, c->st));
   CK(cudaMemcpyAsync(d.ovel, d.vel, sizeof(double) * 3 * (size_t)n, cudaMemcpyDeviceToDevice, c->st));
@@ -2181,6 +2368,13 @@ static int enq_begin(fvm_ctx *c) {
     LAUNCH_CHECK();
     k_place_faces<<<nb, CB, 0, c->st>>>(c->nf, d.fflag, &d.S->iscal[3], d.fbcount, d.flist);
     LAUNCH_CHECK();
+    const int nbc = (int)((c->n + CB - 1) / CB);
+    k_count_cells<<<nbc, CB, 0, c->st>>>(c->n, d.act, d.cbcount);
+    LAUNCH_CHECK();
+    k_scan_counts<<<1, CB, 0, c->st>>>(nbc, d.cbcount, &d.S->ninv);
+    LAUNCH_CHECK();
+    k_place_cells<<<nbc, CB, 0, c->st>>>(c->n, d.act, d.cbcount, d.clist);
+    LAUNCH_CHECK();
   }
   kt_end(c, KT_FLAGS);
   return 0;
@@ -2190,7 +2384,12 @@ static int enq_limiter(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_LIMITER);
   static_assert(FVM_CELL_PERM == 0, "the staged limiter maps threads to consecutive cells");
-  if (c->tune.lim_staged) {
+  // Global steps: the staged limiter when the autotuner picked it, else the
+  // per-thread one.  Partial steps launch both: the staged one (one block per
+  // CST cells) works only in a step where every cell is active, the list one
+  // (on a fixed grid) only in the others.
+  const bool staged = c->tune.lim_staged != 0;
+  if (staged) {
     BULK(({
       static bool attr = false;
       if (!attr) {
@@ -2200,18 +2399,21 @@ static int enq_limiter(fvm_ctx *c) {
         attr = true;
       }
       k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
-          <<<nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>()), 128, limiter_stage_bytes<R, CellTune<R>::KH_LIM>(),
-             c->st>>>(
+          <<<nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>()), 128,
+             limiter_stage_bytes<R, CellTune<R>::KH_LIM>(), c->st>>>(
           c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
-          (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz);
+          (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, c->use_flist);
     }));
-  } else {
+    LAUNCH_CHECK();
+  }
+  if (!staged || c->use_flist) {
     const int bs = c->tune.bs_cell2;
     BULK(k_limiter<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
-         <<<nblk((long long)(10 / CellTune<R>::KH_LIM) * c->n, bs), bs, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo,
+         <<<sgrid(c, (long long)(10 / CellTune<R>::KH_LIM) * c->n, bs), bs, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo,
                                                               d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
                                                               (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx,
-                                                              d.mz));
+                                                              d.mz, c->use_flist ? d.clist : nullptr,
+                                                              staged && c->use_flist));
   }
   LAUNCH_CHECK();
   kt_end(c, KT_LIMITER);
@@ -2230,24 +2432,25 @@ static int enq_update(fvm_ctx *c) {
                                                      d.fcode, lb, d.flist, c->use_flist))
   if (c->learn_mode == 1) {
     CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
-    CORR_FLUX(LM_DEFER, nblk(c->nf, c->tune.bs_face));
+    CORR_FLUX(LM_DEFER, sgrid(c, c->nf, c->tune.bs_face));
     LAUNCH_CHECK();
     int rc = mlp_launch_dev(c, c->nf, lb.count, lb.X, lb.Y);
     if (rc) return rc;
     CORR_FLUX(LM_FINISH, nblk(c->nf, c->tune.bs_face));
   } else if (c->learn_mode == 2) {
-    CORR_FLUX(LM_HARVEST, nblk(c->nf, c->tune.bs_face));
+    CORR_FLUX(LM_HARVEST, sgrid(c, c->nf, c->tune.bs_face));
   } else {
-    CORR_FLUX(LM_EXACT, nblk(c->nf, c->tune.bs_face));
+    CORR_FLUX(LM_EXACT, sgrid(c, c->nf, c->tune.bs_face));
   }
 #undef CORR_FLUX
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_FLUX);
   kt_begin(c, KT_CORR_CELL);
-  BULK(k_corr_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
+  BULK(k_corr_cell<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
                                                           (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
-                                                          d.stepdU, d.counters, d.perm, d.divb));
+                                                          d.stepdU, d.counters, d.perm, d.divb,
+                                                          c->use_flist ? d.clist : nullptr));
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_CELL);
   return 0;
@@ -2256,7 +2459,8 @@ static int enq_update(fvm_ctx *c) {
 static int enq_pvel(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PVEL);
-  k_pvel<<<nblk(c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel);
+  k_pvel<<<sgrid(c, c->n, 128), 128, 0, c->st>>>(c->n, c->P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel,
+                                                 c->use_flist ? d.clist : nullptr, &d.S->ninv);
   LAUNCH_CHECK();
   kt_end(c, KT_PVEL);
   return 0;
@@ -2266,17 +2470,19 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
   Dev &d = c->d;
   const int n = c->n;
   kt_begin(c, KT_TIMESTEP);
-  k_timestep<<<nblk(n, 128), 128, 0, c->st>>>(n, c->P, d.off, d.lfj, d.act, d.bnd, d.U, d.volp, d.vel,
-                                               d.pos, d.tlast, d.tend, d.dtl, &d.S->dtmin);
+  const int *cl = c->use_flist ? d.clist : nullptr;  // partial steps: the involved cells only
+  k_timestep<<<sgrid(c, n, 128), 128, 0, c->st>>>(n, c->P, d.off, d.lfj, d.act, d.bnd, d.U, d.volp, d.vel,
+                                                  d.pos, d.tlast, d.tend, d.dtl, &d.S->dtmin, cl, &d.S->ninv);
   LAUNCH_CHECK();
   if (!shared) {
-    k_halve<<<nblk(n, 256), 256, 0, c->st>>>(n, d.act, &d.S->dtmin, d.dtl);
+    k_halve<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.act, &d.S->dtmin, d.dtl, cl, &d.S->ninv);
     LAUNCH_CHECK();
     CK(cudaMemsetAsync(d.hash, 0, n, c->st));
     CK(cudaMemsetAsync(&d.S->iscal[4], 0, 4 * sizeof(int), c->st));
     CK(cudaMemsetAsync(d.awork, 0, 2 * (size_t)n, c->st));
-    k_adjust_mark<<<nblk(n, 128), 128, 0, c->st>>>(n, d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash,
-                                                   &d.S->iscal[4], d.act0, d.awork);
+    CK(cudaMemsetAsync(d.act0, 0, n, c->st));
+    k_adjust_mark<<<sgrid(c, n, 128), 128, 0, c->st>>>(n, d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash,
+                                                      &d.S->iscal[4], d.act0, d.awork, cl, &d.S->ninv);
     LAUNCH_CHECK();
     const int nb = (int)((n + CB - 1) / CB);
     k_count_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount);
@@ -2287,15 +2493,16 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     LAUNCH_CHECK();
 #if FVM_ADJUST_REPLAY
     CK(cudaMemsetAsync(d.aflag, 0, 8 * sizeof(int), c->st));
-    k_adjust_init<<<nblk(n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.act, &d.S->iscal[4], d.dtl, d.dt0, d.rdv,
-                                                   d.wrv, d.aflag);
+    k_adjust_init<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.act, &d.S->iscal[4], d.dtl, d.dt0,
+                                                      d.rdv, d.wrv, d.aflag, cl, &d.S->ninv);
     LAUNCH_CHECK();
     for (int k = 0; k < ADJ_ITERS; k++) {
-      k_adjust_replay<<<smin(nblk(n, 128), 148 * 16), 128, 0, c->st>>>(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv,
+      k_adjust_replay<<<smin(nblk(n, 128), 4 * c->sms), 128, 0, c->st>>>(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv,
                                                        d.wrv, d.dtl, d.aflag, d.awork);
       LAUNCH_CHECK();
     }
-    k_adjust_restore<<<nblk(n, 256), 256, 0, c->st>>>(n, d.act, d.dt0, d.dtl, d.aflag, &d.S->iscal[6]);
+    k_adjust_restore<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.act, d.dt0, d.dtl, d.aflag, &d.S->iscal[6], cl,
+                                                         &d.S->ninv);
     LAUNCH_CHECK();
     k_adjust_seq<<<1, 32, 0, c->st>>>(d.off, d.lnk, d.s12, d.alist, &d.S->iscal[5], &d.aflag[4], d.dtl);
 #else
@@ -2305,9 +2512,9 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
   }
   kt_end(c, KT_TIMESTEP);
   kt_begin(c, KT_RUNGS);
-  BULK(k_rungs<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.S, shared, d.act, d.hash, d.dtl, &d.S->dtmin, d.rung,
+  BULK(k_rungs<R><<<sgrid(c, n, 256), 256, 0, c->st>>>(n, c->P, d.S, shared, d.act, d.hash, d.dtl, &d.S->dtmin, d.rung,
                                                    d.tlast, d.tend, (R *)d.Wrec, d.S->iscal, d.vel, d.opos,
-                                                   d.ovel));
+                                                   d.ovel, c->use_flist ? d.clist : nullptr));
   LAUNCH_CHECK();
   kt_end(c, KT_RUNGS);
   return 0;
@@ -2316,7 +2523,8 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
 static int enq_collect(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_WST);
-  BULK(k_wst<R><<<nblk(c->n, 256), 256, 0, c->st>>>(c->n, d.act, d.U, d.volp, (R *)d.Wst));
+  BULK(k_wst<R><<<sgrid(c, c->n, 256), 256, 0, c->st>>>(c->n, d.act, d.U, d.volp, (R *)d.Wst,
+                                                        c->use_flist ? d.clist : nullptr, &d.S->ninv));
   LAUNCH_CHECK();
   kt_end(c, KT_WST);
   return 0;
@@ -2326,21 +2534,21 @@ static int enq_update0(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_FLUX);
   const LearnBuf &lb = c->lb;
-#define PRED_FLUX(MODE)                                                                                       \
-  BULK(k_pred_flux<R, MODE><<<nblk(c->nf, c->tune.bs_face), c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
+#define PRED_FLUX(MODE, GRID)                                                                                 \
+  BULK(k_pred_flux<R, MODE><<<GRID, c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
                                                                  d.vel, (const R *)d.Wst, (R *)d.fcon2, d.fcode2, \
                                                                  d.S, d.rung, lb, d.flist, c->use_flist))
   if (c->learn_mode == 1) {
     CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
-    PRED_FLUX(LM_DEFER);
+    PRED_FLUX(LM_DEFER, sgrid(c, c->nf, c->tune.bs_face));
     LAUNCH_CHECK();
     int rc = mlp_launch_dev(c, c->nf, lb.count, lb.X, lb.Y);
     if (rc) return rc;
-    PRED_FLUX(LM_FINISH);
+    PRED_FLUX(LM_FINISH, nblk(c->nf, c->tune.bs_face));
   } else if (c->learn_mode == 2) {
-    PRED_FLUX(LM_HARVEST);
+    PRED_FLUX(LM_HARVEST, sgrid(c, c->nf, c->tune.bs_face));
   } else {
-    PRED_FLUX(LM_EXACT);
+    PRED_FLUX(LM_EXACT, sgrid(c, c->nf, c->tune.bs_face));
   }
 #undef PRED_FLUX
   LAUNCH_CHECK();
@@ -2351,17 +2559,16 @@ static int enq_update0(fvm_ctx *c) {
 static int enq_recon(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_CELL);
-  BULK(k_pred_cell<R><<<nblk(c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
+  BULK(k_pred_cell<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
-                                                          d.tend, (R *)d.Wrec, d.perm));
+                                                          d.tend, (R *)d.Wrec, d.perm, c->use_flist ? d.clist : nullptr));
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_CELL);
   kt_begin(c, KT_RECON);
   BULK(k_recon<R, CellTune<R>::KH_REC, CellTune<R>::MINB_REC>
-       <<<nblk((long long)(10 / CellTune<R>::KH_REC) * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(c->n, c->P, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.dr2,
-                                                            d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung,
-                                                            (R *)d.Wrec, d.perm, (R *)d.mnmx, d.mz,
-                                                            (const R *)d.lrw, (const R *)d.lrd));
+       <<<sgrid(c, (long long)(10 / CellTune<R>::KH_REC) * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(
+           c->n, c->P, d.S, d.off, d.lfj, d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung, (R *)d.Wrec, d.perm,
+           (R *)d.mnmx, d.mz, (const R *)d.lrw, (const R *)d.lrd, c->use_flist ? d.clist : nullptr));
   LAUNCH_CHECK();
   kt_end(c, KT_RECON);
   return 0;

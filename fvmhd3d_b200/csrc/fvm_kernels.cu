@@ -162,7 +162,7 @@ enum : unsigned char { FF_ACTIVE = 1, FF_BND1 = 2, FF_BND2 = 4 };
 __global__ void k_faceflags(int nf, const int2 *__restrict__ s12, unsigned char *__restrict__ act,
                             const int *__restrict__ bnd, unsigned char *__restrict__ fflag,
                             int *__restrict__ nface_active, unsigned char *__restrict__ fcode,
-                            unsigned char *__restrict__ fcode2) {
+                            unsigned char *__restrict__ fcode2, int *__restrict__ bcount) {
   const int f = blockIdx.x * blockDim.x + threadIdx.x;
   bool a = false;
   if (f < nf) {
@@ -173,8 +173,11 @@ __global__ void k_faceflags(int nf, const int2 *__restrict__ s12, unsigned char 
     unsigned char v = a ? FF_ACTIVE : 0;
     if (b1) v |= FF_BND1;
     if (b2) v |= FF_BND2;
+    const unsigned char was = fflag[f];
     fflag[f] = v;
-    if (!a) { fcode[f] = F_OFF; fcode2[f] = F_OFF; }  // the flux passes visit active faces only
+    // the flux passes visit active faces only: a face that goes inactive is
+    // coded F_OFF (codes start F_OFF when the state is installed)
+    if (!a && (was & FF_ACTIVE)) { fcode[f] = F_OFF; fcode2[f] = F_OFF; }
     if (a1 != a2) {
       act[a1 ? e.y : e.x] = A_LNGB;
       act[a1 ? e.x : e.y] = A_ACTIVE | A_HASNGB;
@@ -187,6 +190,7 @@ __global__ void k_faceflags(int nf, const int2 *__restrict__ s12, unsigned char 
   if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bsum, (int)cnt);
   __syncthreads();
   if (threadIdx.x == 0 && bsum) atomicAdd(nface_active, bsum);
+  if (bcount && threadIdx.x == 0) bcount[blockIdx.x] = bsum;  // per-block counts of the face compaction
 }
 
 // Face offsets used by every face loop, computed once per generator layout:
@@ -1136,21 +1140,9 @@ __global__ void k_place_flags(int n, const unsigned char *__restrict__ flag, con
   if (v) list[base + __popc(b & ((1u << lane) - 1u))] = i;
 }
 
-// The same compaction for the active faces (fflag & FF_ACTIVE); a no-op when
-// every face is active, where the flux passes map threads to faces directly.
-__global__ void k_count_faces(int nf, const unsigned char *__restrict__ fflag, const int *__restrict__ nactive,
-                              int *__restrict__ bcount) {
-  if (*nactive == nf) return;
-  const int i = blockIdx.x * CB + threadIdx.x;
-  const bool v = i < nf && (fflag[i] & FF_ACTIVE);
-  __shared__ int bs;
-  if (threadIdx.x == 0) bs = 0;
-  __syncthreads();
-  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, v));
-  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bs, (int)cnt);
-  __syncthreads();
-  if (threadIdx.x == 0) bcount[blockIdx.x] = bs;
-}
+// Ordered placement of the active faces (fflag & FF_ACTIVE), from the
+// per-block counts k_faceflags writes and their scan; a no-op when every face
+// is active, where the flux passes map threads to faces directly.
 __global__ void k_place_faces(int nf, const unsigned char *__restrict__ fflag, const int *__restrict__ nactive,
                               const int *__restrict__ boff, int *__restrict__ list) {
   if (*nactive == nf) return;
@@ -1268,11 +1260,14 @@ __global__ void k_adjust_init(int n, const int *__restrict__ off, const int2 *__
   }
 }
 
-__global__ void k_adjust_replay(int n, int k, const int *__restrict__ off, const int2 *__restrict__ lfj,
+__global__ void k_adjust_replay(int n, int kparam, const int *__restrict__ off, const int2 *__restrict__ lfj,
                                 const int *__restrict__ lsort, const int *__restrict__ lpart,
                                 const unsigned char *__restrict__ act, const double *__restrict__ dt0,
                                 double *__restrict__ rdv, double *__restrict__ wrv, double *__restrict__ dtl,
-                                int *__restrict__ aflag, unsigned char *__restrict__ work) {
+                                int *__restrict__ aflag, unsigned char *__restrict__ work, int kdev) {
+  // replay index: the launch's, or (in a captured step) aflag[7], which
+  // k_adjust_next advances between replays
+  const int k = kdev ? aflag[7] : kparam;
   const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
   if (aflag[5]) return;
   if (aflag[(k + 2) % 3] == 0) {  // the previous replay changed nothing (or none was needed)
@@ -1315,6 +1310,18 @@ __global__ void k_adjust_replay(int n, int k, const int *__restrict__ off, const
     dtl[u] = dtu;
   }
   if (changed) aflag[k % 3] = 1;
+}
+
+// In a captured step the replays run as the body of a conditional WHILE
+// node: after replay k this single thread stops the loop once replay k
+// changed nothing (settled) or ADJ_ITERS replays have run, and advances k.
+__global__ void k_adjust_next(int *__restrict__ aflag, cudaGraphConditionalHandle loop) {
+  const int k = aflag[7];
+  bool stop = aflag[5] != 0;
+  if (aflag[k % 3] == 0) { aflag[5] = 1; stop = true; }
+  if (k + 1 >= ADJ_ITERS) stop = true;
+  aflag[7] = k + 1;
+  cudaGraphSetConditional(loop, stop ? 0u : 1u);
 }
 
 // Not settled after ADJ_ITERS replays: restore the initial dt for the
@@ -2130,6 +2137,11 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   if (c->keep_step_dU) rc |= dalloc(c, &d.stepdU, 14 * (size_t)ncell);
   rc |= dalloc(c, &d.S, 1); rc |= dalloc(c, &d.counters, 4);
   if (rc) return FVM_ENOMEM;
+  // no face active yet, every face coded F_OFF (k_faceflags keeps this so for
+  // the faces it turns inactive)
+  CK(cudaMemsetAsync(d.fflag, 0, nface, c->st));
+  CK(cudaMemsetAsync(d.fcode, F_OFF, nface, c->st));
+  CK(cudaMemsetAsync(d.fcode2, F_OFF, nface, c->st));
   std::vector<int2> hs(nface);
   std::vector<double4> hg(nface), hc(nface);
   for (int f = 0; f < nface; f++) {
@@ -2357,13 +2369,12 @@ static int enq_begin(fvm_ctx *c) {
   LAUNCH_CHECK();
   k_active<<<nblk(n, 256), 256, 0, c->st>>>(n, d.rung, d.S, d.act, &d.S->iscal[1]);
   LAUNCH_CHECK();
-  k_faceflags<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, d.s12, d.act, d.bnd, d.fflag, &d.S->iscal[3], d.fcode,
-                                                    d.fcode2);
+  // partial steps: blocks of CB faces, whose counts start the face compaction
+  k_faceflags<<<nblk(c->nf, CB), CB, 0, c->st>>>(c->nf, d.s12, d.act, d.bnd, d.fflag, &d.S->iscal[3], d.fcode,
+                                                 d.fcode2, c->use_flist ? d.fbcount : nullptr);
   LAUNCH_CHECK();
   if (c->use_flist) {
     const int nb = (int)((c->nf + CB - 1) / CB);
-    k_count_faces<<<nb, CB, 0, c->st>>>(c->nf, d.fflag, &d.S->iscal[3], d.fbcount);
-    LAUNCH_CHECK();
     k_scan_counts<<<1, CB, 0, c->st>>>(nb, d.fbcount, &d.fbcount[nb]);
     LAUNCH_CHECK();
     k_place_faces<<<nb, CB, 0, c->st>>>(c->nf, d.fflag, &d.S->iscal[3], d.fbcount, d.flist);
@@ -2496,10 +2507,51 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     k_adjust_init<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.act, &d.S->iscal[4], d.dtl, d.dt0,
                                                       d.rdv, d.wrv, d.aflag, cl, &d.S->ninv);
     LAUNCH_CHECK();
-    for (int k = 0; k < ADJ_ITERS; k++) {
-      k_adjust_replay<<<smin(nblk(n, 128), 4 * c->sms), 128, 0, c->st>>>(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv,
-                                                       d.wrv, d.dtl, d.aflag, d.awork);
-      LAUNCH_CHECK();
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(c->st, &cs));
+    const int rgrid = smin(nblk(n, 128), 4 * c->sms);
+    if (cs == cudaStreamCaptureStatusActive) {
+      // a WHILE node whose body is one replay and k_adjust_next: the step
+      // graph runs as many replays as the relaxation needs, no launches after
+      cudaGraph_t g;
+      const cudaGraphNode_t *deps = nullptr;
+      size_t nd = 0;
+      CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
+      cudaGraphConditionalHandle h;
+      CK(cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault));
+      cudaGraphNodeParams cp = {};
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t cn;
+      CK(cudaGraphAddNode(&cn, g, deps, nd, &cp));
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      int k0 = 0, kdev = 1;
+      void *ra[] = {(void *)&n, &k0, &d.off, &d.lfj, &d.lsort, &d.lpart, &d.act, &d.dt0, &d.rdv, &d.wrv, &d.dtl,
+                    &d.aflag, &d.awork, &kdev};
+      cudaKernelNodeParams kp = {};
+      kp.func = (void *)k_adjust_replay;
+      kp.gridDim = dim3(rgrid);
+      kp.blockDim = dim3(128);
+      kp.kernelParams = ra;
+      cudaGraphNode_t kr, kx;
+      CK(cudaGraphAddKernelNode(&kr, body, nullptr, 0, &kp));
+      void *na[] = {&d.aflag, &h};
+      cudaKernelNodeParams kn = {};
+      kn.func = (void *)k_adjust_next;
+      kn.gridDim = dim3(1);
+      kn.blockDim = dim3(1);
+      kn.kernelParams = na;
+      CK(cudaGraphAddKernelNode(&kx, body, &kr, 1, &kn));
+      CK(cudaStreamUpdateCaptureDependencies(c->st, &cn, 1, cudaStreamSetCaptureDependencies));
+      c->launches += 2;
+    } else {
+      for (int k = 0; k < ADJ_ITERS; k++) {
+        k_adjust_replay<<<rgrid, 128, 0, c->st>>>(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv, d.wrv,
+                                                  d.dtl, d.aflag, d.awork, 0);
+        LAUNCH_CHECK();
+      }
     }
     k_adjust_restore<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.act, d.dt0, d.dtl, d.aflag, &d.S->iscal[6], cl,
                                                          &d.S->ninv);

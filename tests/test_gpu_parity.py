@@ -172,6 +172,28 @@ def test_graph_replay_matches_eager_steps(shared):
         assert np.array_equal(sa[k], sb[k]), k
 
 
+def test_graph_replay_with_adjust_replays_matches_eager():
+    """In a captured step the neighbour relaxation's replays run as a
+    conditional WHILE node of the graph; on a blast with a 1e6 pressure
+    contrast (out-of-bound neighbour pairs in several steps) the captured
+    steps give the eager steps' bits."""
+    m, W = setup_case(12, "blast", seed=9, noise=0.02)
+    W = W.copy()
+    r = np.linalg.norm(m.pos - 0.5, axis=1)
+    W[r < 0.12, 4] *= 1e4
+    a, b = gpu_system(m, W), gpu_system(m, W)
+    dirty = 0
+    for _ in range(10):
+        a.step(shared=False)
+        dirty += a.adjust_stats()[0] > 0
+    b.run(10, shared=False)
+    assert dirty >= 2
+    assert a.time == b.time and a.tsys_ticks == b.tsys_ticks
+    sa, sb = a.get_state(), b.get_state()
+    for k in sa:
+        assert np.array_equal(sa[k], sb[k]), k
+
+
 def test_adjust_timesteps_replay_vs_oracle():
     """adjust_timesteps (the order-dependent neighbour relaxation) on a blast
     with a 1e6 pressure contrast, individual timesteps: the relaxed dt list,

@@ -2509,7 +2509,7 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     LAUNCH_CHECK();
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     CK(cudaStreamIsCapturing(c->st, &cs));
-    const int rgrid = smin(nblk(n, 128), 4 * c->sms);
+    const int rgrid = smin(nblk(n, 128), 16 * c->sms);
     if (cs == cudaStreamCaptureStatusActive) {
       // a WHILE node whose body is one replay and k_adjust_next: the step
       // graph runs as many replays as the relaxation needs, no launches after

@@ -294,6 +294,25 @@ template <> struct CellTune<float> {
   static constexpr int KH_LIM = 2, MINB_LIM = 8, KH_REC = 5, MINB_REC = 6;
 };
 
+// KH consecutive bulk values from p, as 2-wide loads when KH is even: the
+// callers' rows (10 or 50 values per cell, 6 per link) and even offsets then
+// start on 16-byte (FP64) or 8-byte (FP32) boundaries.
+template <typename R> struct Vec2;
+template <> struct Vec2<double> { using T = double2; };
+template <> struct Vec2<float> { using T = float2; };
+template <typename R, int N>
+__device__ __forceinline__ void load_n(const R *__restrict__ p, R *v) {
+  if constexpr (N % 2 == 0) {
+    using V = typename Vec2<R>::T;
+    const V *p2 = reinterpret_cast<const V *>(p);
+#pragma unroll
+    for (int h = 0; h < N / 2; h++) { const V x = p2[h]; v[2 * h] = x.x; v[2 * h + 1] = x.y; }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; k++) v[k] = p[k];
+  }
+}
+
 template <typename R, int KH>
 __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double t_global,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
@@ -332,7 +351,8 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
     const int2 e = s12[f];
     const int j = e.x == i ? e.y : e.x;
 #endif
-    const R *rj = Wrec + 50 * (size_t)j + k0;
+    R rj[KH];
+    load_n<R, KH>(Wrec + 50 * (size_t)j + k0, rj);
 #pragma unroll
     for (int k = 0; k < KH; k++) {
       const R diff = rj[k] - wi[k];
@@ -1616,10 +1636,12 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
   for (int q = q0; q < q1; q++) {
     const int2 fj = lfj[q];
     const int j = fj.y >= 0 ? fj.y : ~fj.y;
-    const R *w6 = lrw + 6 * (size_t)q;
+    R w6[6];
+    load_n<R, 6>(lrw + 6 * (size_t)q, w6);
     const R a0 = w6[0], a1 = w6[1], a2 = w6[2], b0 = w6[3], b1 = w6[4], b2 = w6[5];
     if (bnd[j] != NO_BOUNDARY) { zero = true; break; }
-    const R *Wj = Wst + 10 * (size_t)j + k0;
+    R Wj[KH];
+    load_n<R, KH>(Wst + 10 * (size_t)j + k0, Wj);
 #pragma unroll
     for (int k = 0; k < KH; k++) {
       const R wj = Wj[k];

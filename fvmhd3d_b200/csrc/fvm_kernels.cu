@@ -313,6 +313,16 @@ __device__ __forceinline__ void load_n(const R *__restrict__ p, R *v) {
   }
 }
 
+// A face's 14 contributions as seven 2-wide stores (records of 112 bytes in
+// FP64, 56 in FP32).
+template <typename R>
+__device__ __forceinline__ void store_contrib(R *__restrict__ o, const R *v) {
+  using V = typename Vec2<R>::T;
+  V *o2 = reinterpret_cast<V *>(o);
+#pragma unroll
+  for (int h = 0; h < 7; h++) { V x; x.x = v[2 * h]; x.y = v[2 * h + 1]; o2[h] = x; }
+}
+
 template <typename R, int KH>
 __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double t_global,
     const int *__restrict__ off, const int *__restrict__ lnk, const int2 *__restrict__ lfj, const int2 *__restrict__ s12,
@@ -660,7 +670,8 @@ __device__ __forceinline__ void corr_face(int f, int slot, double t_global, cons
   {  // issued with the face record, before the boundary tests
     const R *fs = fst + 20 * (size_t)f;
 #pragma unroll
-    for (int k = 0; k < NF; k++) { Wi[k] = fs[k]; Wj[k] = fs[10 + k]; }
+    load_n<R, NF>(fs, Wi);
+    load_n<R, NF>(fs + 10, Wj);
   }
   int i = e.x, j = e.y;
   const double area = g.w;
@@ -697,12 +708,13 @@ __device__ __forceinline__ void corr_face(int f, int slot, double t_global, cons
     return;
   }
   const double tarea = dt * area;
-  R *o = fcon + 14 * (size_t)f;
+  R o[14];
 #pragma unroll
   for (int k = 0; k < NF; k++) o[k] = R(double(flux[k]) * tarea);
   const double pt = double(psi) * tarea;
   o[10] = R(nrm[0] * pt); o[11] = R(nrm[1] * pt); o[12] = R(nrm[2] * pt);
   o[13] = R(double(Bn) * tarea);
+  store_contrib<R>(fcon + 14 * (size_t)f, o);
   fcode[f] = code;
 }
 
@@ -1481,7 +1493,8 @@ __device__ __forceinline__ void pred_face(int f, int slot, const Params &P,
   R Wi[NF], Wj[NF];
   const R *wi = Wst + 10 * (size_t)i, *wj = Wst + 10 * (size_t)(jb == NO_BOUNDARY ? j : i);
 #pragma unroll
-  for (int k = 0; k < NF; k++) { Wi[k] = wi[k]; Wj[k] = wj[k]; }
+  load_n<R, NF>(wi, Wi);
+  load_n<R, NF>(wj, Wj);
   const double *vi = vel + 3 * (size_t)i, *vj = vel + 3 * (size_t)j;
   const double fij[3] = {dri[0] - nrm[0] * dsh, dri[1] - nrm[1] * dsh, dri[2] - nrm[2] * dsh};
   const double fdv = (vj[0] - vi[0]) * fij[0] + (vj[1] - vi[1]) * fij[1] + (vj[2] - vi[2]) * fij[2];
@@ -1499,12 +1512,13 @@ __device__ __forceinline__ void pred_face(int f, int slot, const Params &P,
       return;
     }
   }
-  R *o = fcon + 14 * (size_t)f;
+  R o[14];
 #pragma unroll
   for (int k = 0; k < NF; k++) o[k] = R(double(flux[k]) * area);
   const double pa2 = double(psi) * area;
   o[10] = R(nrm[0] * pa2); o[11] = R(nrm[1] * pa2); o[12] = R(nrm[2] * pa2);
   o[13] = R(double(Bn) * area);
+  store_contrib<R>(fcon + 14 * (size_t)f, o);
   fcode[f] = code;
 }
 

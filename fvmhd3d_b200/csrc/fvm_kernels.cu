@@ -313,6 +313,19 @@ __device__ __forceinline__ void load_n(const R *__restrict__ p, R *v) {
   }
 }
 
+template <typename R, int N>
+__device__ __forceinline__ void store_n(R *__restrict__ p, const R *v) {
+  if constexpr (N % 2 == 0) {
+    using V = typename Vec2<R>::T;
+    V *p2 = reinterpret_cast<V *>(p);
+#pragma unroll
+    for (int h = 0; h < N / 2; h++) { V x; x.x = v[2 * h]; x.y = v[2 * h + 1]; p2[h] = x; }
+  } else {
+#pragma unroll
+    for (int k = 0; k < N; k++) p[k] = v[k];
+  }
+}
+
 // A face's 14 contributions as seven 2-wide stores (records of 112 bytes in
 // FP64, 56 in FP32).
 template <typename R>
@@ -444,9 +457,10 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
     const double dsl = own ? 0.0 : 2.0 * d.w;
     const R dr[3] = {R(d.x - g.x * dsl), R(d.y - g.y * dsl), R(d.z - g.z * dsl)};
     const R dtt = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
-    R *o = fst + 20 * (size_t)f + (own ? 0 : 10) + k0;
+    R o[KH];
 #pragma unroll
     for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2]) + gt[k] * dtt);
+    store_n<R, KH>(fst + 20 * (size_t)f + (own ? 0 : 10) + k0, o);
   }
 }
 
@@ -556,9 +570,10 @@ __device__ __forceinline__ void limiter_st_block(int cb, int n, bool reuse, doub
     const int fk = sfk[l];
     if (!(fk & 1) || (fk & 2)) continue;
     const R d0 = sdx[l], d1 = sdy[l], d2 = sdz[l], dtt = st3[l];
-    R *o = fst + 20 * (size_t)(fk >> 3) + ((fk & 4) ? 0 : 10) + k0;
+    R o[KH];
 #pragma unroll
     for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * d0 + gy[k] * d1 + gz[k] * d2) + gt[k] * dtt);
+    store_n<R, KH>(fst + 20 * (size_t)(fk >> 3) + ((fk & 4) ? 0 : 10) + k0, o);
   }
 }
 
@@ -815,65 +830,63 @@ __device__ __forceinline__ void corr_cell_body(int c, double t_global, const Par
   if (!(ac & (A_ACTIVE | A_LNGB))) return;
   double s[14];
   gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, true, s);
-  double *d0 = dU + 14 * (size_t)c;
+  double *d0p = dU + 14 * (size_t)c;  // rows of 14 doubles: 2-wide loads and stores
+  double d0[14];
+  load_n<double, 14>(d0p, d0);
+  const double zero14[14] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
   if (!(ac & A_ACTIVE)) {
     // inactive neighbour: accumulate until its own step (collect_results,
     // MPI/distribute_work.cpp:714-720)
-    if (stepdU) {
-#pragma unroll
-      for (int k = 0; k < 14; k++) stepdU[14 * (size_t)c + k] = s[k];
-    }
+    if (stepdU) store_n<double, 14>(stepdU + 14 * (size_t)c, s);
     if (bnd[c] == NO_BOUNDARY) {
 #pragma unroll
       for (int k = 0; k < NF; k++) d0[k] += s[k];
       d0[13] += s[13];
       d0[10] = d0[10] + s[10]; d0[11] = d0[11] + s[11]; d0[12] = d0[12] + s[12];
+      store_n<double, 14>(d0p, d0);
     }
     return;
   }
   const double V = cvol[c];
   if (bnd[c] != NO_BOUNDARY) {
     volp[c] = V;
-#pragma unroll
-    for (int k = 0; k < 14; k++) d0[k] = 0.0;
-    if (stepdU) {
-#pragma unroll
-      for (int k = 0; k < 14; k++) stepdU[14 * (size_t)c + k] = s[k];
-    }
+    store_n<double, 14>(d0p, zero14);
+    if (stepdU) store_n<double, 14>(stepdU + 14 * (size_t)c, s);
     return;
   }
   double Uc[NF];
-  const double *Ui = U + 10 * (size_t)c;
+  load_n<double, NF>(U + 10 * (size_t)c, Uc);
 #pragma unroll
-  for (int k = 0; k < NF; k++) Uc[k] = Ui[k] + (d0[k] + s[k]);
+  for (int k = 0; k < NF; k++) Uc[k] = Uc[k] + (d0[k] + s[k]);
   const double divB = d0[13] + s[13];
   const double dPsi[3] = {d0[10] + s[10], d0[11] + s[11], d0[12] + s[12]};
   const double dt = t_global - tlast[c];
   divb[c] = float(dt > 0.0 ? divB / dt / V : divB);  // divBi (MPI/distribute_work.cpp:681)
-#pragma unroll
-  for (int k = 0; k < 14; k++) d0[k] = 0.0;  // dU_local = 0 (collect_results)
+  store_n<double, 14>(d0p, zero14);  // dU_local = 0 (collect_results)
   if (stepdU) {
     double *sd = stepdU + 14 * (size_t)c;
 #pragma unroll
     for (int k = 0; k < 13; k++) sd[k] = 0.0;
     sd[13] = dt > 0.0 ? divB / dt / V : divB;
   }
-  const R *r = Wrec + 50 * (size_t)c;
-  const R *tc = tau + 10 * (size_t)c;
+  R r[NF], rt[NF], tc[NF];  // w and t blocks of the record, tau
+  load_n<R, NF>(Wrec + 50 * (size_t)c, r);
+  load_n<R, NF>(Wrec + 50 * (size_t)c + 40, rt);
+  load_n<R, NF>(tau + 10 * (size_t)c, tc);
   double W1[NF];
   if (Uc[MASS] <= 0.0) {
     // failed-mass fallback (MPI/compute_update.cpp:438-468)
     atomicAdd(&counters[0], 1ULL);
     double Ut[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) W1[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dt;
+    for (int k = 0; k < NF; k++) W1[k] = double(r[k]) + double(rt[k] * tc[k]) * dt;
     to_conservative(W1, volp[c], Ut);
     to_primitive(Ut, V, W1);
   } else {
     const double dth = 0.5 * dt;
     double Wh[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) Wh[k] = double(r[k]) + double(r[40 + k] * tc[k]) * dth;
+    for (int k = 0; k < NF; k++) Wh[k] = double(r[k]) + double(rt[k] * tc[k]) * dth;
     Uc[WBX] -= Wh[VELX] * divB;
     Uc[WBY] -= Wh[VELY] * divB;
     Uc[WBZ] -= Wh[VELZ] * divB;
@@ -900,9 +913,7 @@ __device__ __forceinline__ void corr_cell_body(int c, double t_global, const Par
   }
   double Un[NF];
   to_conservative(W1, V, Un);
-  double *Uo = U + 10 * (size_t)c;
-#pragma unroll
-  for (int k = 0; k < NF; k++) Uo[k] = Un[k];
+  store_n<double, NF>(U + 10 * (size_t)c, Un);
 }
 
 // One thread per cell; in partial steps a fixed grid strides over the
@@ -1455,10 +1466,13 @@ __global__ void k_wst(int n, const unsigned char *__restrict__ act, const double
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
     const int i = lst ? clist[t] : t;
     if (!(act[i] & (A_ACTIVE | A_LNGB))) continue;
-    double W[NF];
-    to_primitive(U + 10 * (size_t)i, volp[i], W);
+    double u[NF], W[NF];
+    load_n<double, NF>(U + 10 * (size_t)i, u);
+    to_primitive(u, volp[i], W);
+    R w[NF];
 #pragma unroll
-    for (int k = 0; k < NF; k++) Wst[10 * (size_t)i + k] = R(W[k]);
+    for (int k = 0; k < NF; k++) w[k] = R(W[k]);
+    store_n<R, NF>(Wst + 10 * (size_t)i, w);
   }
 }
 
@@ -1559,10 +1573,8 @@ __device__ __forceinline__ void pred_cell_body(int c, double t_global, int min_r
   const double V = cvol[c];
   double dot[14];
   gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, false, dot);
-  const double *U0 = U + 10 * (size_t)c;
   double u0[NF], W0[NF];
-#pragma unroll
-  for (int k = 0; k < NF; k++) u0[k] = U0[k];
+  load_n<double, NF>(U + 10 * (size_t)c, u0);
   to_primitive(u0, V, W0);
   int rg = rung[c];
   while (rg < RUNGMAX - 1 && u0[MASS] + dot[MASS] * get_dt(P, rg) <= 0.0 * u0[MASS]) rg++;
@@ -1592,9 +1604,10 @@ __device__ __forceinline__ void pred_cell_body(int c, double t_global, int min_r
   if (W1[ETHM] <= 0.0) W1[ETHM] = W0[ETHM];
   else W1[ENTR] = entropy_from_ethm(P, W1);
   const double idt = 1.0 / dt;
-  R *r = Wrec + 50 * (size_t)c;
+  R rt[NF];
 #pragma unroll
-  for (int k = 0; k < NF; k++) r[40 + k] = R((W1[k] - W0[k]) * idt);
+  for (int k = 0; k < NF; k++) rt[k] = R((W1[k] - W0[k]) * idt);
+  store_n<R, NF>(Wrec + 50 * (size_t)c + 40, rt);
   // collect_reconstruction: rung = max(rung, get_rung(dt)), tend = t + dt(rung)
   int rf = rung[c];
   const int rb = get_rung(P, dt, min_rung);
@@ -1633,8 +1646,7 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
   R *r = Wrec + 50 * (size_t)c + k0;
   const R *wsi = Wst + 10 * (size_t)c + k0;
   R Wi[KH];
-#pragma unroll
-  for (int k = 0; k < KH; k++) Wi[k] = wsi[k];
+  load_n<R, KH>(wsi, Wi);
   if (bnd[c] != NO_BOUNDARY) {
 #pragma unroll
     for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = R(0); r[20 + k] = R(0); r[30 + k] = R(0); r[40 + k] = R(0); }
@@ -1672,7 +1684,7 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
   {
     R *mm = mnmx + 20 * (size_t)c + k0;
 #pragma unroll
-    for (int k = 0; k < KH; k++) { mm[k] = mn[k]; mm[10 + k] = mx[k]; }
+    { store_n<R, KH>(mm, mn); store_n<R, KH>(mm + 10, mx); }
     if (k0 == 0) mz[c] = zero ? 1 : 0;
   }
   if (zero) {
@@ -1716,8 +1728,11 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
       Wx[0] *= alpha; Wy[0] *= alpha; Wz[0] *= alpha; tt[0] *= alpha;
     }
   }
-#pragma unroll
-  for (int k = 0; k < KH; k++) { r[k] = Wi[k]; r[10 + k] = Wx[k]; r[20 + k] = Wy[k]; r[30 + k] = Wz[k]; r[40 + k] = tt[k]; }
+  store_n<R, KH>(r, Wi);
+  store_n<R, KH>(r + 10, Wx);
+  store_n<R, KH>(r + 20, Wy);
+  store_n<R, KH>(r + 30, Wz);
+  store_n<R, KH>(r + 40, tt);
 }
 
 // TPC threads per cell; in partial steps a fixed grid strides over clist.

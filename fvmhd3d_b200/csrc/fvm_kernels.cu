@@ -684,7 +684,6 @@ __device__ __forceinline__ void corr_face(int f, int slot, double t_global, cons
   R Wi[NF], Wj[NF];
   {  // issued with the face record, before the boundary tests
     const R *fs = fst + 20 * (size_t)f;
-#pragma unroll
     load_n<R, NF>(fs, Wi);
     load_n<R, NF>(fs + 10, Wj);
   }
@@ -1506,7 +1505,6 @@ __device__ __forceinline__ void pred_face(int f, int slot, const Params &P,
   const double dsh = d.w;
   R Wi[NF], Wj[NF];
   const R *wi = Wst + 10 * (size_t)i, *wj = Wst + 10 * (size_t)(jb == NO_BOUNDARY ? j : i);
-#pragma unroll
   load_n<R, NF>(wi, Wi);
   load_n<R, NF>(wj, Wj);
   const double *vi = vel + 3 * (size_t)i, *vj = vel + 3 * (size_t)j;
@@ -1683,7 +1681,6 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
   // the next step's limiter pass 1 (neighbour min/max of the same states)
   {
     R *mm = mnmx + 20 * (size_t)c + k0;
-#pragma unroll
     { store_n<R, KH>(mm, mn); store_n<R, KH>(mm + 10, mx); }
     if (k0 == 0) mz[c] = zero ? 1 : 0;
   }

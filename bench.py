@@ -72,12 +72,12 @@ def kernel_bytes(name, N, F, prec_bytes=8):
 # its face count.
 NCU_FACES_64 = 2085347
 NCU_TRAFFIC_64 = {
-    ("limiter", 8): 339.943424e6 + 310.681344e6, ("limiter", 4): 260.643328e6 + 141.116928e6,
-    ("corr_flux", 8): 495.774464e6 + 205.144320e6, ("corr_flux", 4): 328.350976e6 + 95.120896e6,
-    ("corr_cell", 8): 585.743360e6 + 31.117312e6, ("corr_cell", 4): 276.538368e6 + 36.321280e6,
-    ("pred_flux", 8): 181.332992e6 + 183.806464e6, ("pred_flux", 4): 170.044160e6 + 78.530304e6,
-    ("pred_cell", 8): 351.534336e6 + 24.011264e6, ("pred_cell", 4): 192.738048e6 + 15.876608e6,
-    ("recon", 8): 415.059200e6 + 132.006400e6, ("recon", 4): 243.856896e6 + 49.254144e6,
+    ("limiter", 8): 339.128064e6 + 307.197184e6, ("limiter", 4): 260.304384e6 + 140.282112e6,
+    ("corr_flux", 8): 495.820800e6 + 205.820416e6, ("corr_flux", 4): 328.371456e6 + 95.500288e6,
+    ("corr_cell", 8): 456.339200e6 + 41.685248e6, ("corr_cell", 4): 275.797504e6 + 34.937856e6,
+    ("pred_flux", 8): 181.456384e6 + 183.178240e6, ("pred_flux", 4): 170.108672e6 + 83.547904e6,
+    ("pred_cell", 8): 348.580096e6 + 25.229824e6, ("pred_cell", 4): 192.539136e6 + 16.604416e6,
+    ("recon", 8): 415.765504e6 + 126.286080e6, ("recon", 4): 243.889408e6 + 48.472320e6,
 }
 # FP64 floating-point operations per launch on the same 64^3 launches (ncu
 # thread-instruction counts: 2 per DFMA, 1 per DADD and DMUL; this includes

@@ -288,7 +288,10 @@ __global__ void k_link_recon(int n, Params P, const int *__restrict__ off, const
 // the FP32 reconstruction is faster with five per thread.
 template <typename R> struct CellTune;
 template <> struct CellTune<double> {
-  static constexpr int KH_LIM = 2, MINB_LIM = 6, KH_REC = 2, MINB_REC = 8;
+#ifndef FVM_RECON_MINB_D
+#define FVM_RECON_MINB_D 8
+#endif
+  static constexpr int KH_LIM = 2, MINB_LIM = 6, KH_REC = 2, MINB_REC = FVM_RECON_MINB_D;
 };
 template <> struct CellTune<float> {
   static constexpr int KH_LIM = 2, MINB_LIM = 8, KH_REC = 5, MINB_REC = 6;

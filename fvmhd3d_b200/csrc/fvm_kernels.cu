@@ -98,6 +98,7 @@ struct Dev {
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
   int *flist, *fbcount; // ordered active-face list and its block offsets (partial steps)
   int *clist, *cbcount; // ordered list of the step's active and neighbour cells, block offsets (partial steps)
+  unsigned char *bnb;   // per cell: 1 when a neighbour is a boundary cell (set with the boundary codes)
   int2 *lfj;            // per link: face id, neighbour (~j when the cell is s2)
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
   double *rdv, *wrv, *dt0;  // adjust_timesteps replay state (per link, per link, per cell)
@@ -1642,7 +1643,8 @@ template <typename R, int KH>
 __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const int *__restrict__ off,
     const int2 *__restrict__ lfj, const double *__restrict__ cvol, const unsigned char *__restrict__ act,
     const int *__restrict__ bnd, const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec,
-    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw, const R *__restrict__ lrd) {
+    R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw, const R *__restrict__ lrd,
+    const unsigned char *__restrict__ bnb) {
   if (!(act[c] & A_ACTIVE)) return;
   R *r = Wrec + 50 * (size_t)c + k0;
   const R *wsi = Wst + 10 * (size_t)c + k0;
@@ -1658,15 +1660,15 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
   R Wx[KH], Wy[KH], Wz[KH], mn[KH], mx[KH];
 #pragma unroll
   for (int k = 0; k < KH; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = R(0); }
-  bool zero = false;
+  // a boundary neighbour zeroes the reconstruction (its min/max are then unused)
+  const bool zero = bnb[c] != 0;
   FVM_CELL_LOOP
-  for (int q = q0; q < q1; q++) {
+  for (int q = q0; q < (zero ? q0 : q1); q++) {
     const int2 fj = lfj[q];
     const int j = fj.y >= 0 ? fj.y : ~fj.y;
     R w6[6];
     load_n<R, 6>(lrw + 6 * (size_t)q, w6);
     const R a0 = w6[0], a1 = w6[1], a2 = w6[2], b0 = w6[3], b1 = w6[4], b2 = w6[5];
-    if (bnd[j] != NO_BOUNDARY) { zero = true; break; }
     R Wj[KH];
     load_n<R, KH>(Wst + 10 * (size_t)j + k0, Wj);
 #pragma unroll
@@ -1742,7 +1744,7 @@ __global__ void __launch_bounds__(128, MINB) k_recon(int n, Params P, const Sche
     const double *__restrict__ cvol, const unsigned char *__restrict__ act, const int *__restrict__ bnd,
     const R *__restrict__ Wst, const int *__restrict__ rung, R *__restrict__ Wrec, const int *__restrict__ perm,
     R *__restrict__ mnmx, unsigned char *__restrict__ mz, const R *__restrict__ lrw,
-    const R *__restrict__ lrd, const int *__restrict__ clist) {
+    const R *__restrict__ lrd, const int *__restrict__ clist, const unsigned char *__restrict__ bnb) {
   constexpr int TPC = 10 / KH;
   const long long cnt = (long long)TPC * (clist ? S->ninv : n);
   const bool lst = clist && S->ninv != n;  // every cell involved: the list is the identity
@@ -1750,13 +1752,29 @@ __global__ void __launch_bounds__(128, MINB) k_recon(int n, Params P, const Sche
        t += (long long)gridDim.x * blockDim.x) {
     const int u = (int)(t / TPC);
     recon_body<R, KH>(lst ? clist[u] : perm[u], (int)(t % TPC) * KH, P, off, lfj, cvol, act, bnd, Wst, rung, Wrec,
-                      mnmx, mz, lrw, lrd);
+                      mnmx, mz, lrw, lrd, bnb);
   }
 }
 
 // Per link (a cell's entry in its face list, i.e. one side of a face), in the
 // order the cell walks its faces: the face id and the neighbour j, stored as
 // ~j when the cell is s2.  The mesh is fixed while it is installed.
+// Cells with a boundary neighbour, whose reconstruction is zero (the
+// reference's face loop stops at such a neighbour,
+// MPI/compute_reconstruction.cpp:103-106,121); boundary codes are fixed
+// after the state is installed.
+__global__ void k_bnd_neighbours(int n, const int *__restrict__ off, const int2 *__restrict__ lfj,
+                                 const int *__restrict__ bnd, unsigned char *__restrict__ bnb) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  unsigned char b = 0;
+  for (int q = off[c]; q < off[c + 1]; q++) {
+    const int2 fj = lfj[q];
+    if (bnd[fj.y >= 0 ? fj.y : ~fj.y] != NO_BOUNDARY) b = 1;
+  }
+  bnb[c] = b;
+}
+
 __global__ void k_link_tables(int n, const int *__restrict__ off, const int *__restrict__ lnk,
                               const int2 *__restrict__ s12, int2 *__restrict__ lfj) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2180,6 +2198,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc(c, &d.fcode, nface); rc |= dalloc(c, &d.fcode2, nface);
   rc |= dalloc(c, &d.flist, nface); rc |= dalloc(c, &d.fbcount, (nface + CB - 1) / CB + 1);
   rc |= dalloc(c, &d.clist, ncell); rc |= dalloc(c, &d.cbcount, (ncell + CB - 1) / CB + 1);
+  rc |= dalloc(c, &d.bnb, ncell);
   rc |= dalloc_bytes(c, &d.tau, 10 * c->rb * (size_t)ncell);
   rc |= dalloc_bytes(c, &d.fcon, 14 * c->rb * (size_t)nface);
   rc |= dalloc_bytes(c, &d.fcon2, 14 * c->rb * (size_t)nface);
@@ -2301,6 +2320,8 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   CK(cudaMemcpyAsync(d.pos, pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, c->st));
   if (bnd) CK(cudaMemcpyAsync(d.bnd, bnd, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
   else CK(cudaMemsetAsync(d.bnd, 0, sizeof(int) * n, c->st));
+  k_bnd_neighbours<<<nblk(n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.bnd, d.bnb);
+  LAUNCH_CHECK();
   CK(cudaMemsetAsync(d.vel, 0, sizeof(double) * 3 * (size_t)n, c->st));
   CK(cudaMemsetAsync(d.tlast, 0, sizeof(double) * n, c->st));
   k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
@@ -2671,7 +2692,7 @@ static int enq_recon(fvm_ctx *c) {
   BULK(k_recon<R, CellTune<R>::KH_REC, CellTune<R>::MINB_REC>
        <<<sgrid(c, (long long)(10 / CellTune<R>::KH_REC) * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(
            c->n, c->P, d.S, d.off, d.lfj, d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung, (R *)d.Wrec, d.perm,
-           (R *)d.mnmx, d.mz, (const R *)d.lrw, (const R *)d.lrd, c->use_flist ? d.clist : nullptr));
+           (R *)d.mnmx, d.mz, (const R *)d.lrw, (const R *)d.lrd, c->use_flist ? d.clist : nullptr, d.bnb));
   LAUNCH_CHECK();
   kt_end(c, KT_RECON);
   return 0;

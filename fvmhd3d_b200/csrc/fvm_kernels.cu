@@ -107,6 +107,7 @@ struct Dev {
   void *mnmx;               // per cell: the reconstruction's neighbour min and max (20 of the bulk type)
   void *lrw;                // per link: the reconstruction's face weights (6, bulk type)
   void *lrd;                // per link: the face centroid's offset from the cell (3, bulk type)
+  void *lld;                // per link: the limiter's face-side offset dr (3, bulk type)
   unsigned char *mz;        // per cell: the reconstruction met a boundary (the limiter is zero)
   // learned-flux buffers (fvm_set_flux_mode)
   void *lX, *lY, *lface, *lcount, *lstats, *lhx, *lhy, *lhcount, *lnorm;
@@ -255,7 +256,8 @@ __device__ __forceinline__ double recon_ia(const double4 &g, double dsh) {
 template <typename R>
 __global__ void k_link_recon(int n, Params P, const int *__restrict__ off, const int2 *__restrict__ lfj,
                              const double4 *__restrict__ geo, const double4 *__restrict__ dr1,
-                             const double4 *__restrict__ dr2, R *__restrict__ lrw, R *__restrict__ lrd) {
+                             const double4 *__restrict__ dr2, R *__restrict__ lrw, R *__restrict__ lrd,
+                             R *__restrict__ lld) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
   for (int q = off[c]; q < off[c + 1]; q++) {
@@ -272,6 +274,12 @@ __global__ void k_link_recon(int n, Params P, const int *__restrict__ off, const
       w[3 + a] = R((d[a] - nrm[a] * dsh) * ia);
       o[a] = R(d[a]);
     }
+    // the limiter's offset of this side: dri for s1, dri - 2 dsh n for s2
+    // (MPI/compute_update.cpp:157-212; dr1 unwrapped, as the limiter uses it)
+    const double4 e = dr1[fj.x];
+    const double dsl = own ? 0.0 : 2.0 * e.w;
+    R *l3 = lld + 3 * (size_t)q;
+    l3[0] = R(e.x - g.x * dsl); l3[1] = R(e.y - g.y * dsl); l3[2] = R(e.z - g.z * dsl);
   }
 }
 
@@ -346,7 +354,7 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst,
-    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz, const R *__restrict__ lld) {
   if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
   const double ti = tlast[i];
   const R *ri = Wrec + 50 * (size_t)i + k0;
@@ -418,9 +426,8 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
       const bool own = e.x == i;
 #endif
       const double dth = 0.5 * smin(dtI, dtJ);
-      const double4 g = geo[f], d = dr1[f];
-      const double dsl = own ? 0.0 : 2.0 * d.w;
-      const R dr[3] = {R(d.x - g.x * dsl), R(d.y - g.y * dsl), R(d.z - g.z * dsl)};
+      const R *l3 = lld + 3 * (size_t)q;
+      const R dr[3] = {l3[0], l3[1], l3[2]};
       const R dtt = R(own ? dtI - dth : dtJ - dth);
 #pragma unroll
       for (int k = 0; k < KH; k++) {
@@ -457,9 +464,8 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
     const bool own = e.x == i;
 #endif
     const double dt = smin(dtI, dtJ);
-    const double4 g = geo[f], d = dr1[f];
-    const double dsl = own ? 0.0 : 2.0 * d.w;
-    const R dr[3] = {R(d.x - g.x * dsl), R(d.y - g.y * dsl), R(d.z - g.z * dsl)};
+    const R *l3 = lld + 3 * (size_t)q;
+    const R dr[3] = {l3[0], l3[1], l3[2]};
     const R dtt = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
     R o[KH];
 #pragma unroll
@@ -487,7 +493,7 @@ __device__ __forceinline__ void limiter_st_block(int cb, int n, bool reuse, doub
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
-    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz) {
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz, const R *__restrict__ lld) {
   constexpr int TPC = 10 / KH, CST = limiter_cst<KH>(), LCAP = limiter_lcap<KH>();
   const int tid = threadIdx.x;
   const int c0 = cb * CST;
@@ -513,11 +519,10 @@ __device__ __forceinline__ void limiter_st_block(int cb, int n, bool reuse, doub
       const double dtI = t_global - (own ? ti : tj), dtJ = t_global - (own ? tj : ti);
       const double dth = 0.5 * smin(dtI, dtJ);
       const double dt = smin(dtI, dtJ);
-      const double4 g = geo[f], d = dr1[f];
-      const double dsl = own ? 0.0 : 2.0 * d.w;
-      sdx[l] = R(d.x - g.x * dsl);
-      sdy[l] = R(d.y - g.y * dsl);
-      sdz[l] = R(d.z - g.z * dsl);
+      const R *l3 = lld + 3 * (size_t)(L0 + l);
+      sdx[l] = l3[0];
+      sdy[l] = l3[1];
+      sdz[l] = l3[2];
       st2[l] = R(own ? dtI - dth : dtJ - dth);
       st3[l] = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
       sfk[l] = (f << 3) | ((ff & FF_ACTIVE) ? 1 : 0) | ((ff & (FF_BND1 | FF_BND2)) ? 2 : 0) | (own ? 4 : 0);
@@ -528,7 +533,7 @@ __device__ __forceinline__ void limiter_st_block(int cb, int n, bool reuse, doub
   if (cl >= CST || c0 + cl >= n) return;
   if (!staged) {
     limiter_thread<R, KH>(perm[c0 + cl], k0, reuse, t_global, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast, Wrec, tau,
-                      fst, mnmx, mz);
+                          fst, mnmx, mz, lld);
     return;
   }
   const int i = c0 + cl;  // the staged blocks assume the identity thread-to-cell map
@@ -590,7 +595,7 @@ __global__ void __launch_bounds__(128, MINB) k_limiter_st(int n, Params P, const
     const double4 *__restrict__ geo, const double4 *__restrict__ dr1, const unsigned char *__restrict__ fflag,
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
-    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz, int only_all) {
+    const R *__restrict__ mnmx, const unsigned char *__restrict__ mz, int only_all, const R *__restrict__ lld) {
   constexpr int CST = limiter_cst<KH>();
   extern __shared__ __align__(16) unsigned char lsm[];
   __shared__ int soff[CST + 1];
@@ -598,7 +603,7 @@ __global__ void __launch_bounds__(128, MINB) k_limiter_st(int n, Params P, const
   const double t_global = S->t_global;
   const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
   limiter_st_block<R, KH>(blockIdx.x, n, reuse, t_global, soff, lsm, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
-                          Wrec, tau, fst, perm, mnmx, mz);
+                          Wrec, tau, fst, perm, mnmx, mz, lld);
 }
 template <typename R, int KH, int MINB>
 __global__ void __launch_bounds__(128, MINB) k_limiter(int n, Params P, const Sched *__restrict__ S,
@@ -607,7 +612,7 @@ __global__ void __launch_bounds__(128, MINB) k_limiter(int n, Params P, const Sc
     const unsigned char *__restrict__ act, const double *__restrict__ tlast,
     const R *__restrict__ Wrec, R *__restrict__ tau, R *__restrict__ fst, const int *__restrict__ perm,
     const R *__restrict__ mnmx, const unsigned char *__restrict__ mz, const int *__restrict__ clist,
-    int skip_if_all) {
+    int skip_if_all, const R *__restrict__ lld) {
   if (skip_if_all && S->iscal[1] == n) return;  // the staged limiter has this step
   const double t_global = S->t_global;
   // every cell steps and every cell was reconstructed by the last step: the
@@ -622,7 +627,7 @@ __global__ void __launch_bounds__(128, MINB) k_limiter(int n, Params P, const Sc
        t += (long long)gridDim.x * blockDim.x) {
     const int u = (int)(t / TPC);
     limiter_thread<R, KH>(lst ? clist[u] : perm[u], (int)(t % TPC) * KH, reuse, t_global, off, lnk, lfj, s12, geo,
-                          dr1, fflag, act, tlast, Wrec, tau, fst, mnmx, mz);
+                          dr1, fflag, act, tlast, Wrec, tau, fst, mnmx, mz, lld);
   }
 }
 
@@ -2185,6 +2190,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   rc |= dalloc_bytes(c, &d.mnmx, 20 * c->rb * (size_t)ncell); rc |= dalloc(c, &d.mz, ncell);
   rc |= dalloc_bytes(c, &d.lrw, 6 * c->rb * (size_t)nl);
   rc |= dalloc_bytes(c, &d.lrd, 3 * c->rb * (size_t)nl);
+  rc |= dalloc_bytes(c, &d.lld, 3 * c->rb * (size_t)nl);
   rc |= dalloc(c, &d.alist, ncell); rc |= dalloc(c, &d.bcount, (ncell + CB - 1) / CB + 1);
   if ((ncell + CB - 1) / CB > CB * 16) { c->err = "fvm_set_mesh: more than 16M cells"; return FVM_ERANGE; }
   rc |= dalloc(c, &d.pos, 3 * (size_t)ncell); rc |= dalloc(c, &d.vel, 3 * (size_t)ncell);
@@ -2327,7 +2333,7 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
   LAUNCH_CHECK();
   BULK(k_link_recon<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.off, d.lfj, d.geo, d.dr1, d.dr2, (R *)d.lrw,
-                                                        (R *)d.lrd));
+                                                        (R *)d.lrd, (R *)d.lld));
   LAUNCH_CHECK();
 
   BULK(k_init_state<R><<<nblk(n, 128), 128, 0, c->st>>>(n, dW, d.cvol, d.U, d.dU, (R *)d.Wrec, d.volp));
@@ -2485,7 +2491,7 @@ static int enq_limiter(fvm_ctx *c) {
           <<<nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>()), 128,
              limiter_stage_bytes<R, CellTune<R>::KH_LIM>(), c->st>>>(
           c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
-          (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, c->use_flist);
+          (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, c->use_flist, (const R *)d.lld);
     }));
     LAUNCH_CHECK();
   }
@@ -2496,7 +2502,7 @@ static int enq_limiter(fvm_ctx *c) {
                                                               d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
                                                               (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx,
                                                               d.mz, c->use_flist ? d.clist : nullptr,
-                                                              staged && c->use_flist));
+                                                              staged && c->use_flist, (const R *)d.lld));
   }
   LAUNCH_CHECK();
   kt_end(c, KT_LIMITER);

@@ -72,19 +72,19 @@ def kernel_bytes(name, N, F, prec_bytes=8):
 # its face count.
 NCU_FACES_64 = 2085347
 NCU_TRAFFIC_64 = {
-    ("limiter", 8): 339.128064e6 + 307.197184e6, ("limiter", 4): 260.304384e6 + 140.282112e6,
-    ("corr_flux", 8): 495.820800e6 + 205.820416e6, ("corr_flux", 4): 328.371456e6 + 95.500288e6,
-    ("corr_cell", 8): 456.339200e6 + 41.685248e6, ("corr_cell", 4): 275.797504e6 + 34.937856e6,
-    ("pred_flux", 8): 181.456384e6 + 183.178240e6, ("pred_flux", 4): 170.108672e6 + 83.547904e6,
-    ("pred_cell", 8): 348.580096e6 + 25.229824e6, ("pred_cell", 4): 192.539136e6 + 16.604416e6,
-    ("recon", 8): 415.765504e6 + 126.286080e6, ("recon", 4): 243.889408e6 + 48.472320e6,
+    ("limiter", 8): 293.388800e6 + 305.387264e6, ("limiter", 4): 168.422656e6 + 129.603584e6,
+    ("corr_flux", 8): 495.818752e6 + 205.004032e6, ("corr_flux", 4): 328.471296e6 + 95.712000e6,
+    ("corr_cell", 8): 460.649728e6 + 42.046464e6, ("corr_cell", 4): 275.880960e6 + 34.968064e6,
+    ("pred_flux", 8): 181.350912e6 + 183.134720e6, ("pred_flux", 4): 170.220032e6 + 84.814848e6,
+    ("pred_cell", 8): 353.519104e6 + 24.941824e6, ("pred_cell", 4): 192.598272e6 + 16.507392e6,
+    ("recon", 8): 416.417024e6 + 127.086336e6, ("recon", 4): 243.891968e6 + 49.104128e6,
 }
 # FP64 floating-point operations per launch on the same 64^3 launches (ncu
 # thread-instruction counts: 2 per DFMA, 1 per DADD and DMUL; this includes
 # the FMAs inside the compiler's divide and square-root sequences).  The plain
 # FP64 path is compared with the measured FP64 FMA peak (fvm_fp64_peak).
 NCU_FP64_FLOPS_64 = {
-    "limiter": 0.8528e9, "corr_flux": 1.4451e9, "corr_cell": 0.2531e9, "pred_flux": 1.4389e9,
+    "limiter": 0.8236e9, "corr_flux": 1.4451e9, "corr_cell": 0.2531e9, "pred_flux": 1.4389e9,
     "pred_cell": 0.2497e9, "recon": 1.0849e9,
 }
 

@@ -5,9 +5,9 @@
 // 128 faces; the weights sit in shared memory as BF16 in the K-major
 // no-swizzle core-matrix layout the tcgen05 shared-memory descriptors
 // describe; one elected thread issues tcgen05.mma (kind::f16, BF16 inputs,
-// FP32 accumulation in tensor memory); after each layer four warps read their
-// 32 rows back with tcgen05.ld, add the bias, apply GELU, round to BF16 and
-// write the next layer's A operand.  Tensor-memory columns [0,128) and
+// FP32 accumulation in tensor memory); after each layer eight warps read
+// their 32 rows x 64 columns back with tcgen05.ld, add the bias, apply GELU,
+// round to BF16 and write the next layer's A operand.  Tensor-memory columns [0,128) and
 // [128,256) alternate between layers.
 //
 // Included by fvm_kernels.cu (it uses the context and its error macros).
@@ -88,20 +88,30 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
-  uint32_t r[32];
+// 64 columns of this warp's lane quarter, with the wait in the same asm block
+// (no register of the load is read before it completes).
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v) {
+  uint32_t r[64];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-      "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(taddr)
+      : "memory");
 #pragma unroll
-  for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
+  for (int k = 0; k < 64; k++) v[k] = __uint_as_float(r[k]);
+}
+
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
+  uint32_t r[8];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+      : "r"(taddr)
+      : "memory");
+#pragma unroll
+  for (int k = 0; k < 8; k++) v[k] = __uint_as_float(r[k]);
 }
 
 // The hardware tanh approximation (one MUFU instruction).
@@ -118,6 +128,16 @@ __device__ __forceinline__ float gelu(float x) {
   return 0.5f * x * (1.0f + tanh_hw(u));
 }
 
+// Twice the GELU, x (1 + tanh(u)) with u = sqrt(2/pi) x (1 + 0.044715 x^2),
+// in four FP32 operations and one tanh.  The inference epilogue stores it and
+// the image of the next layer's weights carries the factor 1/2 (an exact
+// power-of-two scaling of the BF16 weights), so the layer's products are those
+// of gelu(x) and W.
+__device__ __forceinline__ float gelu2(float x) {
+  const float u = x * fmaf(x * x, 0.7978845608028654f * 0.044715f, 0.7978845608028654f);
+  return fmaf(x, tanh_hw(u), x);
+}
+
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<const uint32_t *>(&h);
@@ -125,24 +145,23 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
 
 // Hidden-layer epilogue: warp w takes rows 32 (w % 4) .. +31 (its
 // tensor-memory lane quarter) and columns 64 (w / 4) .. +63 of the
-// accumulator at col0; bias, GELU, BF16, into the A operand.
+// accumulator at col0; bias, twice the GELU, BF16, into the A operand.
 __device__ __forceinline__ void epilogue_hidden(uint32_t tmem, int col0, const float *bias, unsigned char *A,
                                                 int warp, int lane) {
   const int q = warp & 3, h = warp >> 2, r = 32 * q + lane;
-#pragma unroll 1
-  for (int c = 2 * h; c < 2 * h + 2; c++) {
-    float v[32];
-    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(col0 + 32 * c), v);
+  float v[64];
+  tmem_ld64(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(col0 + 64 * h), v);
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      uint4 w;
-      const int k = 32 * c + 8 * q;
-      w.x = pack_bf16(gelu(v[8 * q + 0] + bias[k + 0]), gelu(v[8 * q + 1] + bias[k + 1]));
-      w.y = pack_bf16(gelu(v[8 * q + 2] + bias[k + 2]), gelu(v[8 * q + 3] + bias[k + 3]));
-      w.z = pack_bf16(gelu(v[8 * q + 4] + bias[k + 4]), gelu(v[8 * q + 5] + bias[k + 5]));
-      w.w = pack_bf16(gelu(v[8 * q + 6] + bias[k + 6]), gelu(v[8 * q + 7] + bias[k + 7]));
-      *reinterpret_cast<uint4 *>(A + kmajor_off(r, k, TILE)) = w;
-    }
+  for (int j = 0; j < 8; j++) {
+    const int k = 64 * h + 8 * j;
+    const float4 b0 = *reinterpret_cast<const float4 *>(bias + k);
+    const float4 b1 = *reinterpret_cast<const float4 *>(bias + k + 4);
+    uint4 w;
+    w.x = pack_bf16(gelu2(v[8 * j + 0] + b0.x), gelu2(v[8 * j + 1] + b0.y));
+    w.y = pack_bf16(gelu2(v[8 * j + 2] + b0.z), gelu2(v[8 * j + 3] + b0.w));
+    w.z = pack_bf16(gelu2(v[8 * j + 4] + b1.x), gelu2(v[8 * j + 5] + b1.y));
+    w.w = pack_bf16(gelu2(v[8 * j + 6] + b1.z), gelu2(v[8 * j + 7] + b1.w));
+    *reinterpret_cast<uint4 *>(A + kmajor_off(r, k, TILE)) = w;
   }
 }
 
@@ -185,14 +204,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__re
   uint32_t parity = 0;
   bool ok = true;
   const int ntiles = (n + TILE - 1) / TILE;
+  // layer-1 input: thread t holds half a row of X (8 BF16, 16 bytes); the
+  // next tile's half row is loaded while this tile's layers run
+  const int xr = t & (TILE - 1), xhalf = t >> 7;
+  auto load_x = [&](int tile) {
+    uint4 x = make_uint4(0, 0, 0, 0);
+    const int row = tile * TILE + xr;
+    if (tile < ntiles && row < n) x = reinterpret_cast<const uint4 *>(X + (size_t)row * NIN)[xhalf];
+    return x;
+  };
+  uint4 xnext = load_x(blockIdx.x);
   for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    // layer-1 input: thread t loads half a row of X (8 BF16, 16 bytes)
-    {
-      const int r = t & (TILE - 1), half = t >> 7, row = tile * TILE + r;
-      uint4 x = make_uint4(0, 0, 0, 0);
-      if (row < n) x = reinterpret_cast<const uint4 *>(X + (size_t)row * NIN)[half];
-      *reinterpret_cast<uint4 *>(A + kmajor_off(r, 8 * half, TILE)) = x;
-    }
+    *reinterpret_cast<uint4 *>(A + kmajor_off(xr, 8 * xhalf, TILE)) = xnext;
+    xnext = load_x(tile + gridDim.x);
     // four layers; layer L reads A (and weights), writes tensor-memory columns dcol
 #pragma unroll 1
     for (int L = 0; L < 4 && ok; L++) {
@@ -225,8 +249,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__re
       if (L < 3) {
         epilogue_hidden(tmem, (L & 1) ? 128 : 0, bias + NH * L, A, warp, t & 31);
       } else if (warp < 4) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + 128u, v);
+        float v[8];
+        tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + 128u, v);
         const int row = tile * TILE + t;
         if (row < n) {
           float4 *yo = reinterpret_cast<float4 *>(Y + (size_t)row * NOUT);
@@ -252,7 +276,8 @@ __global__ void k_f32_to_bf16(long long n, const float *__restrict__ x, __nv_bfl
 
 // Parameters (W1[NH x NIN], b1, W2[NH x NH], b2, W3, b3, W4[NOUT x NH], b4)
 // -> shared-memory image of the BF16 weights (W4 padded to NOUTP rows with
-// zeros) and the FP32 biases (b4 padded likewise).
+// zeros) and the FP32 biases (b4 padded likewise).  W2, W3 and W4 are stored
+// halved: the epilogue hands them twice the GELU.
 __global__ void k_mlp_pack(const float *__restrict__ p, unsigned char *__restrict__ img, float *__restrict__ bias) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const float *W1 = p, *b1 = W1 + NH * NIN, *W2 = b1 + NH, *b2 = W2 + NH * NH, *W3 = b2 + NH, *b3 = W3 + NH * NH,
@@ -263,13 +288,13 @@ __global__ void k_mlp_pack(const float *__restrict__ p, unsigned char *__restric
   }
   if (i < NH * NH) {
     const int r = i / NH, k = i % NH;
-    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W2 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(W2[i]);
-    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W3 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(W3[i]);
+    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W2 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(0.5f * W2[i]);
+    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W3 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(0.5f * W3[i]);
   }
   if (i < NOUTP * NH) {
     const int r = i / NH, k = i % NH;
     *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W4 + kmajor_off(r, k, NOUTP)) =
-        __float2bfloat16_rn(r < NOUT ? W4[r * NH + k] : 0.0f);
+        __float2bfloat16_rn(r < NOUT ? 0.5f * W4[r * NH + k] : 0.0f);
   }
   if (i < NH) {
     bias[i] = b1[i];

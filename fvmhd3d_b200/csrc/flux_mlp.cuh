@@ -5,10 +5,10 @@
 // 128 faces; the weights sit in shared memory as BF16 in the K-major
 // no-swizzle core-matrix layout the tcgen05 shared-memory descriptors
 // describe; one elected thread issues tcgen05.mma (kind::f16, BF16 inputs,
-// FP32 accumulation in tensor memory); after each layer eight warps read
-// their 32 rows x 64 columns back with tcgen05.ld, add the bias, apply GELU,
-// round to BF16 and write the next layer's A operand.  Tensor-memory columns [0,128) and
-// [128,256) alternate between layers.
+// FP32 accumulation in tensor memory); after each layer eight warps read the
+// accumulator back with tcgen05.ld (32 rows x 64 columns each), add the bias,
+// apply GELU, round to BF16 and write the next layer's A operand.  Four such
+// tile chains share a CTA (one per SM) and its one copy of the weights.
 //
 // Included by fvm_kernels.cu (it uses the context and its error macros).
 
@@ -26,12 +26,18 @@ constexpr int OFF_W2 = OFF_W1 + NH * NIN * 2;      // [NH x NH]   32768 B
 constexpr int OFF_W3 = OFF_W2 + NH * NH * 2;       // [NH x NH]   32768 B
 constexpr int OFF_W4 = OFF_W3 + NH * NH * 2;       // [NOUTP x NH] 4096 B
 constexpr int IMG_BYTES = OFF_W4 + NOUTP * NH * 2;  // weights image copied from global
-constexpr int OFF_A = IMG_BYTES;                   // [TILE x NH]  32768 B activations
-constexpr int OFF_BIAS = OFF_A + TILE * NH * 2;    // f32 b1, b2, b3 (3 x NH), b4 (NOUTP)
+// GROUPS independent tile chains per CTA, each with its own activations
+// buffer, mbarrier and 128 tensor-memory columns; they share the weights.
+constexpr int GROUPS = 4, GTHREADS = 256;
+constexpr int A_BYTES = TILE * NH * 2;             // [TILE x NH]  32768 B activations of one group
+constexpr int OFF_A = IMG_BYTES;                   // GROUPS activations buffers
+constexpr int OFF_BIAS = OFF_A + GROUPS * A_BYTES; // f32 b1, b2, b3 (3 x NH), b4 (NOUTP)
 constexpr int NBIAS = 3 * NH + NOUTP;
-constexpr int OFF_BAR = OFF_BIAS + NBIAS * 4;      // mbarrier (8 B) + tensor-memory address (4 B)
-constexpr int SMEM_BYTES = OFF_BAR + 16;
-constexpr int TMEM_COLS = 256;
+constexpr int OFF_BAR = OFF_BIAS + NBIAS * 4;      // GROUPS mbarriers (8 B each), tensor-memory address (4 B)
+constexpr int SMEM_BYTES = OFF_BAR + GROUPS * 8 + 8;
+constexpr int TMEM_COLS = GROUPS * NH;             // 512: the whole tensor memory, one CTA per SM
+static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
+static_assert(OFF_BAR % 8 == 0, "mbarrier alignment");
 static_assert(OFF_W2 % 1024 == 0 && OFF_W3 % 1024 == 0 && OFF_W4 % 1024 == 0 && OFF_A % 1024 == 0, "align");
 
 // Element (row, k) of a K-major no-swizzle operand with `rows` rows: core
@@ -88,18 +94,18 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {
   return false;
 }
 
-// 64 columns of this warp's lane quarter, with the wait in the same asm block
+// 32 columns of this warp's lane quarter, with the wait in the same asm block
 // (no register of the load is read before it completes).
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, float *v) {
-  uint32_t r[64];
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float *v) {
+  uint32_t r[32];
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31, %32, %33, %34, %35, %36, %37, %38, %39, %40, %41, %42, %43, %44, %45, %46, %47, %48, %49, %50, %51, %52, %53, %54, %55, %56, %57, %58, %59, %60, %61, %62, %63}, [%64];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];\n\t"
       "tcgen05.wait::ld.sync.aligned;"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
       : "r"(taddr)
       : "memory");
 #pragma unroll
-  for (int k = 0; k < 64; k++) v[k] = __uint_as_float(r[k]);
+  for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
 }
 
 __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float *v) {
@@ -143,44 +149,71 @@ __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   return *reinterpret_cast<const uint32_t *>(&h);
 }
 
-// Hidden-layer epilogue: warp w takes rows 32 (w % 4) .. +31 (its
-// tensor-memory lane quarter) and columns 64 (w / 4) .. +63 of the
-// accumulator at col0; bias, twice the GELU, BF16, into the A operand.
-__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, int col0, const float *bias, unsigned char *A,
-                                                int warp, int lane) {
-  const int q = warp & 3, h = warp >> 2, r = 32 * q + lane;
-  float v[64];
-  tmem_ld64(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(col0 + 64 * h), v);
+// Hidden-layer epilogue of one group: warp w (0..7 within the group) takes
+// rows 32 (w % 4) .. +31 (its tensor-memory lane quarter q) and columns
+// 64 (w / 4) .. +63 (half h) of the group's accumulator, 32 at a time; bias,
+// twice the GELU, BF16, into the group's A operand.
+__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, const float *bias, unsigned char *A, int q, int h,
+                                                int lane) {
+  const int r = 32 * q + lane;
+#pragma unroll 1
+  for (int c = 2 * h; c < 2 * h + 2; c++) {
+    float v[32];
+    tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
 #pragma unroll
-  for (int j = 0; j < 8; j++) {
-    const int k = 64 * h + 8 * j;
-    const float4 b0 = *reinterpret_cast<const float4 *>(bias + k);
-    const float4 b1 = *reinterpret_cast<const float4 *>(bias + k + 4);
-    uint4 w;
-    w.x = pack_bf16(gelu2(v[8 * j + 0] + b0.x), gelu2(v[8 * j + 1] + b0.y));
-    w.y = pack_bf16(gelu2(v[8 * j + 2] + b0.z), gelu2(v[8 * j + 3] + b0.w));
-    w.z = pack_bf16(gelu2(v[8 * j + 4] + b1.x), gelu2(v[8 * j + 5] + b1.y));
-    w.w = pack_bf16(gelu2(v[8 * j + 6] + b1.z), gelu2(v[8 * j + 7] + b1.w));
-    *reinterpret_cast<uint4 *>(A + kmajor_off(r, k, TILE)) = w;
+    for (int j = 0; j < 4; j++) {
+      const int k = 32 * c + 8 * j;
+      const float4 b0 = *reinterpret_cast<const float4 *>(bias + k);
+      const float4 b1 = *reinterpret_cast<const float4 *>(bias + k + 4);
+      uint4 w;
+      w.x = pack_bf16(gelu2(v[8 * j + 0] + b0.x), gelu2(v[8 * j + 1] + b0.y));
+      w.y = pack_bf16(gelu2(v[8 * j + 2] + b0.z), gelu2(v[8 * j + 3] + b0.w));
+      w.z = pack_bf16(gelu2(v[8 * j + 4] + b1.x), gelu2(v[8 * j + 5] + b1.y));
+      w.w = pack_bf16(gelu2(v[8 * j + 6] + b1.z), gelu2(v[8 * j + 7] + b1.w));
+      *reinterpret_cast<uint4 *>(A + kmajor_off(r, k, TILE)) = w;
+    }
   }
 }
 
+// Barrier over the 256 threads of group g (named barrier 1 + g).
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(1 + g), "r"(GTHREADS) : "memory");
+}
+// The same barrier, returning whether v holds on every thread of the group.
+__device__ __forceinline__ bool group_all(bool v, int g) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.u32 p, %1, 0;\n\t"
+      "bar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(1 + g), "r"(GTHREADS)
+      : "memory");
+  return r != 0;
+}
+
 // Y[n x 8] = MLP(X[n x 16]) (n read from n_dev when given); X in BF16, Y in
-// FP32.  256 threads per CTA: the eight warps share each epilogue (a
-// tensor-memory lane quarter and half the columns each).  err bit 1: an
-// mbarrier wait gave up.
-constexpr int THREADS = 256;
+// FP32.  One CTA per SM (the shared memory holds one copy of the weights and
+// four activations buffers); its four groups of eight warps run independent
+// 128-row tiles, so one group's epilogue overlaps another's matrix products.
+// The first four warps of a group load the inputs and write the outputs (warp
+// q: rows 32 q .. +31); thread 0 of the group issues the group's tcgen05.mma
+// and commits them to the group's mbarrier.  err bit 1: an mbarrier wait gave
+// up.
+constexpr int THREADS = GROUPS * GTHREADS;
 __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__restrict__ n_dev,
                                                       const __nv_bfloat16 *__restrict__ X, float *__restrict__ Y,
                                                       const uint4 *__restrict__ wimg, const float *__restrict__ bias_g,
                                                       int *__restrict__ err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   if (n_dev) n = *n_dev;  // row count produced on the device
-  const int t = threadIdx.x, warp = t >> 5;
-  uint64_t *bar = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
-  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + 8);
+  const int t = threadIdx.x, warp = t >> 5, g = warp >> 3, q = warp & 3, hq = (warp >> 2) & 1,
+            gt = t & (GTHREADS - 1);
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + GROUPS * 8);
   float *bias = reinterpret_cast<float *>(sm + OFF_BIAS);
-  unsigned char *A = sm + OFF_A;
+  unsigned char *A = sm + OFF_A + g * A_BYTES;
   for (int i = t; i < IMG_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4 *>(sm)[i] = wimg[i];
   for (int i = t; i < NBIAS; i += blockDim.x) bias[i] = bias_g[i];
   if (warp == 0) {
@@ -189,14 +222,15 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__re
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (t == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(1));
+    for (int i = 0; i < GROUPS; i++) asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bars + i)), "r"(1));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   fence_before();
   __syncthreads();
   fence_after();
-  const uint32_t tmem = *tslot;
-  const uint32_t bar_a = smem_u32(bar);
+  const uint32_t tbase = *tslot;
+  const uint32_t tmem = tbase + (uint32_t)(g * NH);  // this group's 128 columns
+  const uint32_t bar_a = smem_u32(bars + g);
   const uint32_t a_addr = smem_u32(A);
   const uint32_t w_addr = smem_u32(sm);
   const uint32_t id_h = instr_desc(TILE, NH), id_o = instr_desc(TILE, NOUTP);
@@ -204,54 +238,64 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__re
   uint32_t parity = 0;
   bool ok = true;
   const int ntiles = (n + TILE - 1) / TILE;
-  // layer-1 input: thread t holds half a row of X (8 BF16, 16 bytes); the
-  // next tile's half row is loaded while this tile's layers run
-  const int xr = t & (TILE - 1), xhalf = t >> 7;
-  auto load_x = [&](int tile) {
-    uint4 x = make_uint4(0, 0, 0, 0);
-    const int row = tile * TILE + xr;
-    if (tile < ntiles && row < n) x = reinterpret_cast<const uint4 *>(X + (size_t)row * NIN)[xhalf];
-    return x;
+  const int stride = gridDim.x * GROUPS;
+  // layer-1 input: thread gt of the group holds row gt of X (16 BF16, two
+  // 16-byte halves); the next tile's row is loaded while this tile's layers run
+  auto load_x = [&](int tile, uint4 &x0, uint4 &x1) {
+    x0 = x1 = make_uint4(0, 0, 0, 0);
+    if (tile < ntiles && gt < TILE) {
+      const int row = tile * TILE + gt;
+      if (row < n) {
+        const uint4 *src = reinterpret_cast<const uint4 *>(X + (size_t)row * NIN);
+        x0 = src[0];
+        x1 = src[1];
+      }
+    }
   };
-  uint4 xnext = load_x(blockIdx.x);
-  for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    *reinterpret_cast<uint4 *>(A + kmajor_off(xr, 8 * xhalf, TILE)) = xnext;
-    xnext = load_x(tile + gridDim.x);
-    // four layers; layer L reads A (and weights), writes tensor-memory columns dcol
+  int tile = blockIdx.x * GROUPS + g;
+  uint4 x0, x1;
+  load_x(tile, x0, x1);
+  for (; tile < ntiles && ok; tile += stride) {
+    if (gt < TILE) {
+      *reinterpret_cast<uint4 *>(A + kmajor_off(gt, 0, TILE)) = x0;
+      *reinterpret_cast<uint4 *>(A + kmajor_off(gt, 8, TILE)) = x1;
+    }
+    load_x(tile + stride, x0, x1);
+    // four layers; each reads the group's A (and the weights) and overwrites
+    // the group's accumulator, whose previous contents the group has read
 #pragma unroll 1
     for (int L = 0; L < 4 && ok; L++) {
       fence_async_smem();
       fence_before();
-      __syncthreads();
-      if (t == 0) {
+      group_sync(g);
+      if (gt == 0) {
         fence_after();
-        const uint32_t dcol = (L & 1) ? 128u : 0u;
         if (L == 0) {
-          mma_bf16(tmem + dcol, smem_desc(a_addr, LBO_128, SBO), smem_desc(w_addr + OFF_W1, LBO_128, SBO), id_h, 0);
+          mma_bf16(tmem, smem_desc(a_addr, LBO_128, SBO), smem_desc(w_addr + OFF_W1, LBO_128, SBO), id_h, 0);
         } else {
           const uint32_t wb = w_addr + (L == 1 ? OFF_W2 : L == 2 ? OFF_W3 : OFF_W4);
           const uint32_t lbo_b = L == 3 ? LBO_OUT : LBO_128;
 #pragma unroll 1
           for (int kk = 0; kk < NH / 16; kk++)
-            mma_bf16(tmem + dcol, smem_desc(a_addr + 2 * kk * LBO_128, LBO_128, SBO),
+            mma_bf16(tmem, smem_desc(a_addr + 2 * kk * LBO_128, LBO_128, SBO),
                      smem_desc(wb + 2 * kk * lbo_b, lbo_b, SBO), L == 3 ? id_o : id_h, kk > 0 ? 1u : 0u);
         }
         mma_commit(bar_a);
       }
       const bool waited = bar_wait(bar_a, parity);
-      if (!__syncthreads_and(waited)) {  // every thread leaves together
-        if (t == 0) atomicOr(err, 1);
+      if (!group_all(waited, g)) {  // the group leaves together
+        if (gt == 0) atomicOr(err, 1);
         ok = false;
         break;
       }
       parity ^= 1;
       fence_after();
       if (L < 3) {
-        epilogue_hidden(tmem, (L & 1) ? 128 : 0, bias + NH * L, A, warp, t & 31);
-      } else if (warp < 4) {
+        epilogue_hidden(tmem, bias + NH * L, A, q, hq, t & 31);
+      } else if (gt < TILE) {
         float v[8];
-        tmem_ld8(tmem + ((uint32_t)(32 * warp) << 16) + 128u, v);
-        const int row = tile * TILE + t;
+        tmem_ld8(tmem + ((uint32_t)(32 * q) << 16), v);
+        const int row = tile * TILE + gt;
         if (row < n) {
           float4 *yo = reinterpret_cast<float4 *>(Y + (size_t)row * NOUT);
           const float *b4 = bias + 3 * NH;
@@ -265,7 +309,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__re
   __syncthreads();
   if (warp == 0) {
     fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(TMEM_COLS));
   }
 }
 

@@ -3215,7 +3215,7 @@ int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const doub
 // ============================ learned flux network ============================
 
 // The network on n rows (or on *n_dev rows, at most nmax, counted on the
-// device): persistent CTAs, two per SM (shared memory allows two).
+// device): persistent CTAs, one per SM, four 128-row tiles in flight in each.
 static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfloat16 *X, float *Y) {
   if (nmax <= 0) return 0;
   static bool attr_set = false;
@@ -3225,8 +3225,8 @@ static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfl
   }
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
-  const int ntiles = (nmax + mlp::TILE - 1) / mlp::TILE;
-  const int grid = ntiles < 2 * nsm ? ntiles : 2 * nsm;
+  const int nchains = (nmax + mlp::TILE * mlp::GROUPS - 1) / (mlp::TILE * mlp::GROUPS);
+  const int grid = nchains < nsm ? nchains : nsm;
   mlp::k_mlp_infer<<<grid, mlp::THREADS, mlp::SMEM_BYTES, c->st>>>(nmax, n_dev, X, Y, (const uint4 *)c->mlp_img,
                                                           c->mlp_bias, c->mlp_err);
   LAUNCH_CHECK();

@@ -33,6 +33,23 @@ def test_bf16_rounding():
     assert M.bf16(x).tolist() == [1.0, 1.0, 1.0 + 2 ** -7, -3.5, 0.0]
 
 
+def test_twice_gelu_with_halved_weights_is_the_same_rounded_network():
+    """The inference kernel stores 2 gelu(z) as the next layer's BF16 input
+    and halves W2, W3 and W4 in its weights image.  Power-of-two scaling
+    commutes with BF16 rounding and cancels in each product, so the rounded
+    network is unchanged: outputs equal the oracle's bit for bit."""
+    rng = np.random.default_rng(4)
+    p = M.init_params(9)
+    X = rng.normal(size=(257, M.NIN))
+    W1, b1, W2, b2, W3, b3, W4, b4 = M.unpack(p)
+    a = M.bf16(X).astype(np.float64)
+    z = a @ M.bf16(W1).astype(np.float64).T + b1
+    for W, b in ((W2, b2), (W3, b3), (W4, b4)):
+        a = M.bf16(2.0 * M.gelu(z)).astype(np.float64)
+        z = a @ M.bf16(0.5 * W).astype(np.float64).T + b
+    assert np.array_equal(z, M.forward(p, X))
+
+
 @pytest.mark.gpu
 @pytest.mark.parametrize("n", [1, 1000, 128 * 400 + 17])
 def test_tensor_core_inference_matches_oracle(n):

@@ -155,13 +155,14 @@ class ClockSampler:
 # ---------------------------------------------------------------- CPU legs --
 
 def _cpu_worker(args):
-    """One single-rank reference (or oracle port) process on its own replica."""
-    nside, problem, steps, warmup, kind, seed = args
+    """One single-rank reference (or oracle port) process on its own replica
+    of the shared host-built mesh: `warmup` untimed and `steps` timed global
+    steps of `problem`."""
+    mesh_path, problem, steps, warmup, kind = args
     sys.path.insert(0, ROOT)
     import fvmhd3d_b200 as F
     from oracle import pyoracle
-    pos = F.jittered_lattice(nside, 0.1, seed=seed)
-    m = F.build_periodic(pos[F.sort_local_data(pos, 1.0)], 1.0, nthreads=1)
+    m = F.mesh.Mesh.load(mesh_path)
     W = getattr(F.problems, problem)(m.pos)
     S = pyoracle.RefSystem() if kind == "reference" else pyoracle.OracleSystem()
     S.set_mesh(m)
@@ -174,25 +175,70 @@ def _cpu_worker(args):
     return m.nface * steps, time.perf_counter() - t0
 
 
-def cpu_leg(nside, problem, steps, warmup, procs=None):
-    """Aggregate face-updates/s of P concurrent single-rank CPU processes (one
-    per host core), each on its own replica mesh.  Uses the reference's own
-    code (oracle/_ref/libfvmref.so) when it was built, else the C oracle."""
+# Host memory one single-rank reference process holds per cell (its system
+# arrays plus the loaded mesh; measured 4.9 KB per cell on the 64^3 blast).
+CPU_BYTES_PER_CELL = 5000
+
+
+def host_memory_available():
+    """Bytes the host can still give: MemAvailable, capped by a cgroup limit."""
+    avail = None
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    avail = int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    for path in ("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory/memory.limit_in_bytes"):
+        try:
+            with open(path) as f:
+                v = f.read().strip()
+            if v.isdigit():
+                lim = int(v)
+                usage = 0
+                for up in ("/sys/fs/cgroup/memory.current", "/sys/fs/cgroup/memory/memory.usage_in_bytes"):
+                    if os.path.exists(up):
+                        with open(up) as g:
+                            usage = int(g.read().strip())
+                        break
+                avail = lim - usage if avail is None else min(avail, lim - usage)
+        except (OSError, ValueError):
+            pass
+    return avail
+
+
+def cpu_leg(m, problem, steps, warmup, procs=None):
+    """Aggregate face-updates/s of P concurrent single-rank CPU processes,
+    each on its own replica of the mesh m (the workload's own mesh, built
+    once on the host and shared through a file).  Uses the reference's own
+    code (oracle/_ref/libfvmref.so) when it was built, else the C oracle.  P
+    is the host's core count, lowered when host memory cannot hold that many
+    replicas."""
     import multiprocessing as mp
     from oracle import pyoracle
     kind = "reference" if os.path.exists(pyoracle.REF_SO) else "port"
     if not os.path.exists(pyoracle.REF_SO if kind == "reference" else pyoracle.ORACLE_SO):
         raise RuntimeError("CPU checkers are not built (run __graft_entry__.build())")
     P = procs or os.cpu_count() or 1
-    ctx = mp.get_context("spawn")
-    with ctx.Pool(P) as pool:
-        res = pool.map(_cpu_worker, [(nside, problem, steps, warmup, kind, 100 + r) for r in range(P)])
+    avail = host_memory_available()
+    if avail:
+        P = max(1, min(P, int(0.6 * avail // (CPU_BYTES_PER_CELL * m.ncell))))
+    fd, path = tempfile.mkstemp(suffix=".npz")
+    os.close(fd)
+    try:
+        m.save(path)
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(P) as pool:
+            res = pool.map(_cpu_worker, [(path, problem, steps, warmup, kind)] * P)
+    finally:
+        os.unlink(path)
     faces = sum(r[0] for r in res)
     t = max(r[1] for r in res)
     return {"value": faces / t, "unit": UNIT, "cores": P, "kind": kind,
-            "sample": f"{P} concurrent single-rank processes, each {steps} global steps of the {problem} "
-                      f"on its own {nside}^3 jittered-lattice replica in Peano-Hilbert order ({faces // (P * steps)} faces); "
-                      f"no halo exchange"}
+            "sample": f"{P} concurrent single-rank processes, each {steps} global step(s) of the {problem} on its "
+                      f"own replica of the workload's mesh ({m.ncell} cells, {m.nface} faces, Peano-Hilbert "
+                      f"order) after {warmup} untimed; no halo exchange"}
 
 
 # ---------------------------------------------------------------- GPU leg ---
@@ -224,6 +270,176 @@ def barrier(ws):
         dist.barrier()
 
 
+def make_workload(F, problem, nside, ncell, order, rank=0):
+    """(mesh, primitives, boundary codes, System arguments, global timestep)
+    of a workload.  The lattice problems (blast, alfven, orszag_tang) run on
+    nside^3 jittered generators with a global timestep; the Keplerian disk on
+    ncell generators with individual power-of-two timesteps, isothermal EOS
+    and static generators (the mesh is built once; generators that followed
+    the flow would need the mesh rebuilt every step).  Cells in
+    Peano-Hilbert order (the reference's sort_local_data) unless order is
+    "native"."""
+    if problem == "disk":
+        pos, box = F.problems.disk_generators(ncell, seed=3 + rank)
+        if order == "hilbert":
+            pos = pos[F.sort_local_data(pos, box)]
+        m = F.build_periodic(pos, box)
+        W, bnd = F.problems.disk(pos, box)
+        sysargs = dict(gamma=1.0, courant=0.4, box=tuple(box), dtmax=1.0 / 16, eos=1, iso_GM=1.0, iso_cfac=0.05,
+                       static_mesh=True)
+        return m, W, bnd, sysargs, False
+    pos = F.jittered_lattice(nside, 0.1, seed=1 + rank)
+    if order == "hilbert":
+        pos = pos[F.sort_local_data(pos, 1.0)]
+    m = F.build_periodic(pos, 1.0)
+    return m, getattr(F.problems, problem)(m.pos), None, {}, True
+
+
+def timed_run(torch, S, steps, shared):
+    """(cells, faces, ms) of `steps` steps replayed from the captured step
+    graph (captured beforehand), CUDA events on the context's stream."""
+    stream = torch.cuda.ExternalStream(S.stream_ptr)
+    S.run(1, shared=shared)  # capture outside the timed region
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    cells, faces = S.run(steps, shared=shared)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return cells, faces, e0.elapsed_time(e1)
+
+
+def device_bytes_of(torch, local, build):
+    """(object, device bytes it holds) of build() by cudaMemGetInfo."""
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info(local)[0]
+    obj = build()
+    torch.cuda.synchronize()
+    return obj, free0 - torch.cuda.mem_get_info(local)[0]
+
+
+def rel_l1(Ub, Ua):
+    rel = np.abs(Ub - Ua).sum(axis=0) / np.maximum(np.abs(Ua).sum(axis=0), 1e-300)
+    return {"density": float(rel[0]), "energy": float(rel[4]), "momentum": float(rel[1:4].max()),
+            "magnetic": float(rel[5:8].max())}
+
+
+def config2_leg(F, torch, steps=50):
+    """The mixed-precision configuration: the blast on 64^3 generators, 50
+    global steps, FP32 bulk (reconstruction, limiter, flux) with FP64
+    geometry and compensated accumulation: face-updates/s of both paths and
+    the FP32 path's relative L1 error per conserved variable against the
+    plain FP64 path over the same steps."""
+    m, W, _, _, _ = make_workload(F, "blast", 64, 0, "hilbert")
+    out = {"workload": "blast 64^3 jittered Voronoi (Peano-Hilbert order), 50 global steps",
+           "ncell": m.ncell, "nface": m.nface}
+    U = {}
+    for name, prec in (("plain_fp64", F.FVM_PREC_FP64), ("fp32_bulk", F.FVM_PREC_FP32)):
+        S = F.System(precision=prec)
+        S.set_mesh(m)
+        S.init_problem(W)
+        _, faces, ms = timed_run(torch, S, steps, True)
+        U[name] = S.get_state()["U"]
+        out[name] = {"value": faces / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps}
+        S.close()
+    # the first (untimed) step of timed_run is part of both runs alike
+    out["fp32_bulk"]["rel_l1_vs_plain_fp64"] = rel_l1(U["fp32_bulk"], U["plain_fp64"])
+    out["steps"] = steps + 1
+    return out
+
+
+def config3_leg(F, torch, local, steps=64):
+    """The rung-batching configuration: the Keplerian disk on 1,048,576
+    generators, individual power-of-two timesteps, FP32 bulk, launch choices
+    by the autotuner, each step one replay of the captured step graph."""
+    m, W, bnd, sysargs, _ = make_workload(F, "disk", 0, 1 << 20, "hilbert")
+
+    def build():
+        S = F.System(precision=F.FVM_PREC_FP32, device=local, **sysargs)
+        S.set_mesh(m)
+        S.init_problem(W, bnd=bnd)
+        return S
+    S, dev_bytes = device_bytes_of(torch, local, build)
+    for _ in range(8):
+        S.step(shared=False)
+    tuned = S.autotune(shared=False, steps=3)
+    cells, faces, ms = timed_run(torch, S, steps, False)
+    rung = S.get_state()["rung"]
+    used, counts = np.unique(rung, return_counts=True)
+    out = {"workload": f"Keplerian disk {m.ncell} static generators, individual timesteps, FP32 bulk",
+           "value": faces / (ms / 1e3), "unit": UNIT, "steps": steps, "ms_per_step": ms / steps,
+           "mean_active_cells": cells / steps, "mean_active_faces": faces / steps, "nface": m.nface,
+           "rungs": {int(r): int(c) for r, c in zip(used, counts)}, "device_bytes": int(dev_bytes),
+           "autotuned": tuned}
+    S.close()
+    return out
+
+
+def config5_leg(F, torch, local, steps=24):
+    """The combined configuration: the Orszag-Tang vortex on 160^3
+    generators with individual power-of-two timesteps, plain FP64 against
+    learned flux + FP32 bulk, the same steps from the same start: face-updates/s,
+    rungs in use, device bytes and the learned path's relative L1 error per
+    conserved variable."""
+    from fvmhd3d_b200 import learned as L
+    m, W, _, _, _ = make_workload(F, "orszag_tang", 160, 0, "hilbert")
+    model = L.load_model()
+    out = {"workload": "Orszag-Tang vortex 160^3 jittered Voronoi (Peano-Hilbert order), individual timesteps",
+           "ncell": m.ncell, "nface": m.nface, "steps": steps}
+    U, T = {}, {}
+    for name, prec, learned in (("plain_fp64", F.FVM_PREC_FP64, False), ("learned_fp32", F.FVM_PREC_FP32, True)):
+        def build():
+            S = F.System(precision=prec, device=local)
+            S.set_mesh(m)
+            S.init_problem(W)
+            if learned:
+                L.apply(S, model)
+                S.set_flux_mode(1, judge=1024, **L.GATE)
+            return S
+        S, dev_bytes = device_bytes_of(torch, local, build)
+        cells, faces, ms = timed_run(torch, S, steps, False)
+        st = S.get_state()
+        U[name], T[name] = st["U"], S.time
+        used, counts = np.unique(st["rung"], return_counts=True)
+        r = {"value": faces / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+             "mean_active_faces": faces / steps, "rungs": {int(a): int(b) for a, b in zip(used, counts)},
+             "device_bytes": int(dev_bytes)}
+        if learned:
+            ls = S.learn_stats()
+            r["network_faces_fraction"] = ls["deferred"] / max(2 * faces, 1)
+            r["fallback_fraction"] = ls["fallback"] / max(ls["deferred"], 1)
+            r["judged_rel_l1"] = ls["judged_rel_l1"]
+        out[name] = r
+        S.close()
+    out["same_time"] = T["plain_fp64"] == T["learned_fp32"]
+    out["learned_fp32"]["rel_l1_vs_plain_fp64"] = rel_l1(U["learned_fp32"], U["plain_fp64"])
+    out["speedup_learned_vs_plain_fp64"] = out["learned_fp32"]["value"] / out["plain_fp64"]["value"]
+    return out
+
+
+def remesh_leg(F, S, m, e2e):
+    """The mesh installation the reference repeats every step
+    (MPI/iterate.cpp:150 rebuilds the mesh; the fluid path then starts from
+    the new face and cell lists): fvm_set_mesh from host arrays, with the
+    per-link tables it builds on the device, timed by the host clock around
+    the call (it synchronises).  With the host's own mesh build excluded, as
+    for the reference, the end-to-end rate of a step that also reinstalls
+    the mesh is faces / (e2e step time + this time)."""
+    import torch
+    torch.cuda.synchronize()
+    ts = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        S.set_mesh(m)
+        ts.append(time.perf_counter() - t0)
+    out = {"set_mesh_ms": round(1e3 * min(ts), 2), "ncell": m.ncell, "nface": m.nface,
+           "path": "fvm_set_mesh from host arrays (upload, validation, link tables), host clock"}
+    if e2e:
+        step_s = m.nface / e2e["value"]
+        out["e2e_with_remesh"] = {"value": m.nface / (step_s + min(ts)), "unit": UNIT}
+    return out
+
+
 def run_gpu(args):
     import torch
     import fvmhd3d_b200 as F
@@ -232,27 +448,7 @@ def run_gpu(args):
     torch.cuda.set_device(local)
     t0 = time.perf_counter()
     prec = F.FVM_PREC_FP32 if args.precision == "fp32" else F.FVM_PREC_FP64
-    bnd = None
-    if args.problem == "disk":
-        # Keplerian disk, isothermal EOS, individual power-of-two timesteps, on
-        # static generators (the mesh is built once; generators that followed
-        # the flow would need the mesh rebuilt every step)
-        pos, box = F.problems.disk_generators(args.ncell, seed=3 + rank)
-        if args.order == "hilbert":  # the reference's sort_local_data
-            pos = pos[F.sort_local_data(pos, box)]
-        m = F.build_periodic(pos, box)
-        W, bnd = F.problems.disk(pos, box)
-        sysargs = dict(gamma=1.0, courant=0.4, box=tuple(box), dtmax=1.0 / 16, eos=1, iso_GM=1.0, iso_cfac=0.05,
-                       static_mesh=True)
-        shared = False
-    else:
-        pos = F.jittered_lattice(args.nside, 0.1, seed=1 + rank)
-        if args.order == "hilbert":
-            pos = pos[F.sort_local_data(pos, 1.0)]
-        m = F.build_periodic(pos, 1.0)
-        W = getattr(F.problems, args.problem)(m.pos)
-        sysargs = {}
-        shared = True
+    m, W, bnd, sysargs, shared = make_workload(F, args.problem, args.nside, args.ncell, args.order, rank)
     mesh_s = time.perf_counter() - t0
     torch.cuda.synchronize()
     free0 = torch.cuda.mem_get_info(local)[0]
@@ -396,10 +592,23 @@ def run_gpu(args):
     # run, same mesh and steps (relative L1 error per conserved variable)
     weights = os.path.join(ROOT, "fvmhd3d_b200", "data", "flux_mlp.npz")
     if (not args.no_learned and shared and args.problem == "blast" and pb == 8 and os.path.exists(weights)):
-        line["learned_fp32"] = learned_leg(F, m, W, S, 100, weights, stream_of=torch.cuda.ExternalStream)
+        line["learned_fp32"] = learned_leg(F, m, W, 100, weights, stream_of=torch.cuda.ExternalStream)
+    if not args.no_remesh:
+        line["e2e_remesh"] = remesh_leg(F, S, m, e2e)
+    S.close()
+    # the other configurations of the target, each on its own mesh (parity
+    # cases of the headline are in tests/); rank 0 of a single-GPU run only
+    if rank == 0 and ws == 1 and not args.no_configs and args.problem == "blast" and pb == 8:
+        for key, fn in (("config2_blast64_fp32", lambda: config2_leg(F, torch)),
+                        ("config3_disk1m_fp32_rungs", lambda: config3_leg(F, torch, local)),
+                        ("config5_orszag_tang160_learned", lambda: config5_leg(F, torch, local))):
+            try:
+                line[key] = fn()
+            except Exception as e:  # the headline stands without them
+                line[key] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and ws == 1 and not args.no_cpu:
         try:
-            line["cpu_baseline"] = cpu_leg(args.cpu_nside, args.problem, args.cpu_steps, 1)
+            line["cpu_baseline"] = cpu_leg(m, args.problem, args.cpu_steps, 0)
         except Exception as e:  # the GPU number stands without it
             line["cpu_baseline"] = {"error": str(e)}
     if rank == 0:
@@ -409,62 +618,97 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
-def learned_leg(F, m, W, plain, steps, weights, stream_of):
+def learned_leg(F, m, W, steps, weights, stream_of):
     """The learned-flux + FP32 bulk path on the same mesh and initial state
-    for `steps` global steps: face-updates/s (CUDA events) and its relative
-    L1 error per conserved variable against the plain FP64 context `plain`
-    advanced by the same number of steps from the same start."""
+    for `steps` global steps: face-updates/s (CUDA events), its relative L1
+    error per conserved variable against a plain FP64 run of the same steps
+    from the same start, and the judge's error of the network on the faces it
+    serves.  The same steps are repeated with the gated faces taking the
+    central flux alone (no dissipation) and the local Lax-Friedrichs
+    dissipation instead of the network: the network earns its place when its
+    error is below both."""
     import torch
     from fvmhd3d_b200 import learned as L
-    z = np.load(weights)
-    model = {k: z[k] for k in ("params", "mu_x", "sd_x", "mu_y", "sd_y")}
+    model = L.load_model(weights)
     ref = F.System(precision=F.FVM_PREC_FP64)
     ref.set_mesh(m)
     ref.init_problem(W)
     ref.run(steps, shared=True)
-    s = F.System(precision=F.FVM_PREC_FP32)
-    s.set_mesh(m)
-    s.init_problem(W)
-    L.apply(s, model)
-    s.set_flux_mode(1, **L.GATE)
-    st = stream_of(s.stream_ptr)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    e0.record(st)
-    _, faces = s.run(steps, shared=True)
-    e1.record(st)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1)
-    Ua, Ub = ref.get_state()["U"], s.get_state()["U"]
-    rel = np.abs(Ub - Ua).sum(axis=0) / np.maximum(np.abs(Ua).sum(axis=0), 1e-300)
-    stats = s.learn_stats()
-    out = {"value": faces / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
-           "rel_l1_vs_plain_fp64": {"density": float(rel[0]), "energy": float(rel[4]),
-                                    "momentum": float(rel[1:4].max()), "magnetic": float(rel[5:8].max())},
-           "network_faces_fraction": stats["deferred"] / max(2 * faces, 1),
-           "fallback_fraction": stats["fallback"] / max(stats["deferred"], 1),
-           "judged_mean_abs_scaled": stats["judged_mean_abs"], "judged_max_abs_scaled": stats["judged_max_abs"],
-           "judged_rel_l1": stats["judged_rel_l1"],
-           "dtype": "f32 bulk + bf16 network", "weights": "fvmhd3d_b200/data/flux_mlp.npz"}
+    Ua = ref.get_state()["U"]
     ref.close()
-    s.close()
+
+    def rel_l1(Ub):
+        rel = np.abs(Ub - Ua).sum(axis=0) / np.maximum(np.abs(Ua).sum(axis=0), 1e-300)
+        return {"density": float(rel[0]), "energy": float(rel[4]), "momentum": float(rel[1:4].max()),
+                "magnetic": float(rel[5:8].max())}
+
+    out = {}
+    for sur in ("network", "central", "llf"):
+        s = F.System(precision=F.FVM_PREC_FP32)
+        s.set_mesh(m)
+        s.init_problem(W)
+        L.apply(s, model)
+        s.set_flux_mode(1, judge=1024, **L.GATE)
+        s.set_flux_surrogate(sur)
+        st = stream_of(s.stream_ptr)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(st)
+        _, faces = s.run(steps, shared=True)
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        stats = s.learn_stats()
+        r = {"rel_l1_vs_plain_fp64": rel_l1(s.get_state()["U"]), "judged_rel_l1": stats["judged_rel_l1"]}
+        if sur == "network":
+            r.update({"value": faces / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
+                      "network_faces_fraction": stats["deferred"] / max(2 * faces, 1),
+                      "fallback_fraction": stats["fallback"] / max(stats["deferred"], 1),
+                      "positivity_fallback_fraction": stats["positivity_fallback"] / max(stats["deferred"], 1),
+                      "judged_faces": stats["judged"],
+                      "judged_mean_abs_scaled": stats["judged_mean_abs"],
+                      "judged_max_abs_scaled": stats["judged_max_abs"],
+                      "dtype": "f32 bulk + bf16 network", "weights": "fvmhd3d_b200/data/flux_mlp.npz"})
+            out.update(r)
+        else:
+            out[f"gated_faces_{sur}"] = r
+        s.close()
     return out
 
 
 def run_reference(args):
+    """The reference arm: the reference's own hot path (oracle/_ref, compiled
+    from its sources) on the host cores, on this arm's workload and mesh.  A
+    step is one full global step of one single-rank process on its own
+    replica of the mesh; the K timed and W warm-up steps are spread over P
+    concurrent processes (ceil(K/P) and ceil(W/P) each)."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
+    import fvmhd3d_b200 as F
     steps = max(1, args.steps)
     t0 = time.perf_counter()
-    cb = cpu_leg(args.cpu_nside, args.problem, steps, max(1, min(args.warmup, 2)))
+    m, _, _, _, shared = make_workload(F, args.problem, args.nside, args.ncell, args.order)
+    if not shared:
+        print(json.dumps({"impl": "reference", "unavailable": "the CPU sample runs the global-timestep workloads"}))
+        return
+    mesh_s = time.perf_counter() - t0
+    P = os.cpu_count() or 1
+    avail = host_memory_available()
+    if avail:
+        P = max(1, min(P, int(0.6 * avail // (CPU_BYTES_PER_CELL * m.ncell))))
+    per = math.ceil(steps / P)
+    wper = math.ceil(max(0, args.warmup) / P)
+    cb = cpu_leg(m, args.problem, per, wper, procs=P)
     wall = time.perf_counter() - t0
     line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": ws,
             "steps": steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"{args.problem} {args.nside}^3 jittered Voronoi, global timestep, plain FP64 "
-                                   f"(bounded CPU sample: {args.cpu_nside}^3 replicas)"},
+            "config": {"workload": f"{args.problem} {args.nside}^3 jittered Voronoi, global timestep, plain FP64",
+                       "ncell": m.ncell, "nface_per_step": m.nface, "cell_order": args.order,
+                       "mesh_build_s": round(mesh_s, 2),
+                       "steps_run": f"{cb['cores']} processes x {per} timed step(s) after {wper} warm-up"},
             "cpu_baseline": {"value": cb["value"], "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
                              "sample": cb["sample"]},
             "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -484,11 +728,12 @@ def main():
     ap.add_argument("--order", default="hilbert", choices=["hilbert", "native"],
                     help="cell order: Peano-Hilbert (the reference's sort_local_data) or as generated")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
-    ap.add_argument("--cpu-nside", type=int, default=32)
-    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--cpu-steps", type=int, default=1, help="timed steps per process of the CPU sample")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-flux + FP32 comparison leg")
+    ap.add_argument("--no-remesh", action="store_true", help="skip timing the per-step mesh installation")
+    ap.add_argument("--no-configs", action="store_true", help="skip the 64^3, disk and 160^3 configurations")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "fvm":
         args.warmup = 3

@@ -60,6 +60,8 @@ SIGNATURES = {
     "fvm_get_counters": (c_int, [c_void_p, c_void_p]),
     "fvm_mlp_set_weights": (c_int, [c_void_p, c_void_p]),
     "fvm_mlp_eval": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "fvm_mlp_eval_counted": (c_int, [c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "fvm_set_flux_surrogate": (c_int, [c_void_p, c_int]),
     "fvm_mlp_get_weights": (c_int, [c_void_p, c_void_p]),
     "fvm_mlp_grad": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "fvm_mlp_train": (c_int, [c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int, c_int, c_float, c_ull,
@@ -70,6 +72,7 @@ SIGNATURES = {
     "fvm_harvest_count": (c_ll, [c_void_p]),
     "fvm_get_harvest": (c_int, [c_void_p, c_ll, c_void_p, c_void_p]),
     "fvm_autotune": (c_int, [c_void_p, c_int, c_int, c_void_p]),
+    "fvm_set_tuning": (c_int, [c_void_p, c_void_p]),
     "fvm_compute_flux": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_compute_flux_static": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_last_step_ms": (c_float, [c_void_p]),

@@ -200,7 +200,8 @@ __device__ __forceinline__ bool group_all(bool v, int g) {
 // The first four warps of a group load the inputs and write the outputs (warp
 // q: rows 32 q .. +31); thread 0 of the group issues the group's tcgen05.mma
 // and commits them to the group's mbarrier.  err bit 1: an mbarrier wait gave
-// up.
+// up; bit 2: the wait for that group's last commit before the tensor memory
+// is released gave up as well.
 constexpr int THREADS = GROUPS * GTHREADS;
 __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__restrict__ n_dev,
                                                       const __nv_bfloat16 *__restrict__ X, float *__restrict__ Y,
@@ -305,6 +306,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__re
       }
     }
   }
+  // A group that gave up on its mbarrier may still have matrix products in
+  // flight that write its tensor-memory columns: wait once more (bounded) for
+  // that commit before the columns are released; err bit 2 records that this
+  // wait gave up too (the columns are then released with the products
+  // possibly still running, and the launch reports the error).
+  if (!ok && !bar_wait(bar_a, parity) && gt == 0) atomicOr(err, 2);
   fence_before();
   __syncthreads();
   if (warp == 0) {

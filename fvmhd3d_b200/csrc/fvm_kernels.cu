@@ -46,6 +46,9 @@ using namespace fvm;
 #ifndef FVM_CELL_UNROLL
 #define FVM_CELL_UNROLL 1  // unroll factor of the cell kernels' face loops (1 and 2 time the same within 1%)
 #endif
+#ifndef FVM_RECON_PIPE
+#define FVM_RECON_PIPE 0  // the reconstruction's face loop as a software pipeline (loads one link ahead)
+#endif
 #ifndef FVM_REUSE_MINMAX
 #define FVM_REUSE_MINMAX 1  // the limiter reuses the reconstruction's neighbour min/max when every cell steps
 #endif
@@ -640,8 +643,9 @@ __global__ void __launch_bounds__(128, MINB) k_limiter(int n, Params P, const Sc
 // exact with harvesting (LM_HARVEST), gate and defer to the network
 // (LM_DEFER: returns false for a deferred face), or the deferred face's flux
 // from the network output (LM_FINISH), falling back to the exact solver when
-// the face would move more than half of either cell's mass within its step
-// (tdt_i, tdt_j: area times each side's step) or the result is not finite.
+// the state either cell reaches from this face's flux alone over its step
+// (tdt_i, tdt_j: area times each side's step) keeps less than half of its
+// mass or of its thermal energy, or the result is not finite.
 enum { LM_EXACT = 0, LM_HARVEST = 1, LM_DEFER = 2, LM_FINISH = 3 };
 
 template <typename R, int MODE>
@@ -669,13 +673,16 @@ __device__ __forceinline__ bool learned_flux(const Params &P, const Sched *S, co
   y[0] = y0.x; y[1] = y0.y; y[2] = y0.z; y[3] = y0.w; y[4] = y1.x; y[5] = y1.y; y[6] = y1.z; y[7] = y1.w;
   LearnedSolver h{lb, y, lb.judge != 0 && face_hash((unsigned)f, salt) % lb.judge == 0};
   compute_flux_with<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux, h);
-  const double dm = fabs(double(flux[MASS]));
-  bool ok = dm * tdt_i <= 0.5 * lb.U[10 * (size_t)i + MASS] && dm * tdt_j <= 0.5 * lb.U[10 * (size_t)j + MASS];
+  bool ok = true;
 #pragma unroll
   for (int k = 0; k < NF; k++) ok = ok && isfinite(double(flux[k]));
   if (!ok) {
     compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
     atomicAdd(&lb.stats[LSTAT_FALLBACK], 1.0);
+  } else if (!keeps_positive<R>(lb, i, -tdt_i, flux) || !keeps_positive<R>(lb, j, tdt_j, flux)) {
+    compute_flux<R>(P, wij, Wi, Wj, jb, nr, psi, Bn, flux);
+    atomicAdd(&lb.stats[LSTAT_FALLBACK], 1.0);
+    atomicAdd(&lb.stats[LSTAT_POSFALL], 1.0);
   }
   return true;
 }
@@ -1667,15 +1674,8 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
   for (int k = 0; k < KH; k++) { Wx[k] = Wy[k] = Wz[k] = mn[k] = mx[k] = R(0); }
   // a boundary neighbour zeroes the reconstruction (its min/max are then unused)
   const bool zero = bnb[c] != 0;
-  FVM_CELL_LOOP
-  for (int q = q0; q < (zero ? q0 : q1); q++) {
-    const int2 fj = lfj[q];
-    const int j = fj.y >= 0 ? fj.y : ~fj.y;
-    R w6[6];
-    load_n<R, 6>(lrw + 6 * (size_t)q, w6);
-    const R a0 = w6[0], a1 = w6[1], a2 = w6[2], b0 = w6[3], b1 = w6[4], b2 = w6[5];
-    R Wj[KH];
-    load_n<R, KH>(Wst + 10 * (size_t)j + k0, Wj);
+  const int qe = zero ? q0 : q1;
+  auto face_term = [&](const R *w6, const R *Wj) {
 #pragma unroll
     for (int k = 0; k < KH; k++) {
       const R wj = Wj[k];
@@ -1683,11 +1683,49 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
       const R diff = wj - Wi[k];
       mn[k] = smin(mn[k], diff);
       mx[k] = smax(mx[k], diff);
-      Wx[k] += sum * a0 + diff * b0;
-      Wy[k] += sum * a1 + diff * b1;
-      Wz[k] += sum * a2 + diff * b2;
+      Wx[k] += sum * w6[0] + diff * w6[3];
+      Wy[k] += sum * w6[1] + diff * w6[4];
+      Wz[k] += sum * w6[2] + diff * w6[5];
+    }
+  };
+#if FVM_RECON_PIPE
+  // Software pipeline: the next link's weights and neighbour state are in
+  // flight while this link's terms are summed, and the link after next's
+  // (face, neighbour) entry is loaded one step earlier still, so no
+  // iteration waits on a dependent pair of loads.
+  if (q0 < qe) {
+    int2 fjn = lfj[q0];
+    R w6n[6], Wjn[KH];
+    load_n<R, 6>(lrw + 6 * (size_t)q0, w6n);
+    load_n<R, KH>(Wst + 10 * (size_t)(fjn.y >= 0 ? fjn.y : ~fjn.y) + k0, Wjn);
+    int2 fj2 = q0 + 1 < qe ? lfj[q0 + 1] : fjn;
+#pragma unroll 1
+    for (int q = q0; q < qe; q++) {
+      R w6[6], Wj[KH];
+#pragma unroll
+      for (int k = 0; k < 6; k++) w6[k] = w6n[k];
+#pragma unroll
+      for (int k = 0; k < KH; k++) Wj[k] = Wjn[k];
+      if (q + 1 < qe) {
+        load_n<R, 6>(lrw + 6 * (size_t)(q + 1), w6n);
+        load_n<R, KH>(Wst + 10 * (size_t)(fj2.y >= 0 ? fj2.y : ~fj2.y) + k0, Wjn);
+        if (q + 2 < qe) fj2 = lfj[q + 2];
+      }
+      face_term(w6, Wj);
     }
   }
+#else
+  FVM_CELL_LOOP
+  for (int q = q0; q < qe; q++) {
+    const int2 fj = lfj[q];
+    const int j = fj.y >= 0 ? fj.y : ~fj.y;
+    R w6[6];
+    load_n<R, 6>(lrw + 6 * (size_t)q, w6);
+    R Wj[KH];
+    load_n<R, KH>(Wst + 10 * (size_t)j + k0, Wj);
+    face_term(w6, Wj);
+  }
+#endif
   // the next step's limiter pass 1 (neighbour min/max of the same states)
   {
     R *mm = mnmx + 20 * (size_t)c + k0;
@@ -1932,6 +1970,10 @@ enum KernelId { KT_FLAGS = 0, KT_LIMITER, KT_CORR_FLUX, KT_CORR_CELL, KT_PVEL, K
                 KT_WST, KT_PRED_FLUX, KT_PRED_CELL, KT_RECON, KT_SYNC, KT_COUNT };
 static const char *kKernelNames[KT_COUNT] = {"flags", "limiter", "corr_flux", "corr_cell", "pvel", "timestep",
                                              "rungs", "wst", "pred_flux", "pred_cell", "recon", "sync"};
+
+// Per-device one-time settings (kernel attributes) are kept for device
+// indices below this bound.
+constexpr int kMaxDevices = 64;
 
 struct fvm_ctx {
   int device;
@@ -2480,12 +2522,14 @@ static int enq_limiter(fvm_ctx *c) {
   const bool staged = c->tune.lim_staged != 0;
   if (staged) {
     BULK(({
-      static bool attr = false;
-      if (!attr) {
+      // the attribute is per device: set once on each device a context uses
+      static bool attr[kMaxDevices] = {};
+      if (c->device < 0 || c->device >= kMaxDevices) { c->err = "device index out of range"; return FVM_EINVAL; }
+      if (!attr[c->device]) {
         CK(cudaFuncSetAttribute(k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 limiter_stage_bytes<R, CellTune<R>::KH_LIM>()));
-        attr = true;
+        attr[c->device] = true;
       }
       k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
           <<<nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>()), 128,
@@ -3218,10 +3262,11 @@ int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const doub
 // device): persistent CTAs, one per SM, four 128-row tiles in flight in each.
 static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfloat16 *X, float *Y) {
   if (nmax <= 0) return 0;
-  static bool attr_set = false;
-  if (!attr_set) {
+  static bool attr_set[kMaxDevices] = {};  // per device, like the attribute itself
+  if (c->device < 0 || c->device >= kMaxDevices) { c->err = "device index out of range"; return FVM_EINVAL; }
+  if (!attr_set[c->device]) {
     CK(cudaFuncSetAttribute(mlp::k_mlp_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, mlp::SMEM_BYTES));
-    attr_set = true;
+    attr_set[c->device] = true;
   }
   int nsm = 148;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, c->device);
@@ -3404,6 +3449,38 @@ int fvm_mlp_train(fvm_ctx *c, long long n, const float *X, const float *T, const
   return 0;
 }
 
+int fvm_mlp_eval_counted(fvm_ctx *c, int nmax, int n, const float *X, float *Y) {
+  if (!c || nmax < 0 || n < 0 || n > nmax || (nmax > 0 && (!X || !Y))) return FVM_EINVAL;
+  if (!c->mlp_img) { c->err = "fvm_mlp_eval_counted: no weights (fvm_mlp_set_weights)"; return FVM_EINVAL; }
+  if (nmax == 0) return 0;
+  CK(cudaSetDevice(c->device));
+  const size_t nx = (size_t)nmax * mlp::NIN, ny = (size_t)nmax * mlp::NOUT;
+  float *dx = nullptr, *dy = nullptr;
+  __nv_bfloat16 *db = nullptr;
+  int *dn = nullptr;
+  CK(cudaMallocAsync(&dx, nx * sizeof(float), c->st));
+  CK(cudaMallocAsync(&db, nx * sizeof(__nv_bfloat16), c->st));
+  CK(cudaMallocAsync(&dy, ny * sizeof(float), c->st));
+  CK(cudaMallocAsync(&dn, sizeof(int), c->st));
+  CK(cudaMemcpyAsync(dx, X, nx * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dy, Y, ny * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(dn, &n, sizeof(int), cudaMemcpyHostToDevice, c->st));
+  mlp::k_f32_to_bf16<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>((long long)nx, dx, db);
+  LAUNCH_CHECK();
+  int rc = mlp_launch_dev(c, nmax, dn, db, dy);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(Y, dy, ny * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  int herr = 0;
+  CK(cudaMemcpyAsync(&herr, c->mlp_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaFreeAsync(dx, c->st));
+  CK(cudaFreeAsync(db, c->st));
+  CK(cudaFreeAsync(dy, c->st));
+  CK(cudaFreeAsync(dn, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (herr) { c->err = "fvm_mlp_eval_counted: tensor-core pipeline wait timed out"; return FVM_ECUDA; }
+  return 0;
+}
+
 int fvm_mlp_eval(fvm_ctx *c, int n, const float *X, float *Y) {
   if (!c || n < 0 || (n > 0 && (!X || !Y))) return FVM_EINVAL;
   if (!c->mlp_img) { c->err = "fvm_mlp_eval: no weights (fvm_mlp_set_weights)"; return FVM_EINVAL; }
@@ -3476,6 +3553,7 @@ int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, in
   lb.hstride = (unsigned)hstride;
   lb.judge = (unsigned)judge;
   lb.U = d.U;
+  lb.vol = d.cvol;
   lb.norm = (const float *)d.lnorm;
   CK(cudaMemcpy(d.lnorm, c->h_norm, sizeof(c->h_norm), cudaMemcpyHostToDevice));
   lb.drho = drho;
@@ -3486,6 +3564,15 @@ int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, in
   CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));
   CK(cudaStreamSynchronize(c->st));
   c->learn_mode = mode;
+  return 0;
+}
+
+int fvm_set_flux_surrogate(fvm_ctx *c, int kind) {
+  if (!c || kind < SUR_NETWORK || kind > SUR_LLF) return FVM_EINVAL;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  drop_graphs(c);  // captured steps hold the flux settings by value
+  c->lb.surrogate = kind;
   return 0;
 }
 
@@ -3569,6 +3656,23 @@ int state_copy(fvm_ctx *c, StateCopy &sc, bool save) {
 }  // namespace
 
 extern "C" {
+
+int fvm_set_tuning(fvm_ctx *c, const int *choice) {
+  if (!c || !choice) return FVM_EINVAL;
+  auto block_ok = [](int b) { return b == 32 || b == 64 || b == 128; };
+  if ((choice[0] != 0 && choice[0] != 1) || !block_ok(choice[1]) || !block_ok(choice[2]) || !block_ok(choice[3])) {
+    c->err = "fvm_set_tuning: staged limiter must be 0 or 1 and block sizes 32, 64 or 128";
+    return FVM_EINVAL;
+  }
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  drop_graphs(c);  // captured steps hold the launch shapes
+  c->tune.lim_staged = choice[0];
+  c->tune.bs_face = choice[1];
+  c->tune.bs_cell = choice[2];
+  c->tune.bs_cell2 = choice[3];
+  return 0;
+}
 
 int fvm_autotune(fvm_ctx *c, int shared, int steps, int *choice) {
   if (!c || steps < 1) return FVM_EINVAL;

@@ -3,9 +3,12 @@
 The network (16 -> 128 -> 128 -> 128 -> 8, GELU, BF16 weights, FP32
 accumulation) predicts, on smooth faces, the dissipative part of the HLLD
 flux in the face frame (the HLLD flux minus the mean of the two sides'
-physical fluxes); csrc/flux_learn.cuh describes the features, the gate and
-the exact fallback.  This module runs the pipeline with the library's own
-kernels:
+physical fluxes) divided by the size m of the face's scaled jump; the flux
+pass multiplies the output by m in FP32, so the network's error is relative
+to the dissipation on every face.  csrc/flux_learn.cuh describes the
+features, the gate and the exact fallback.  Harvested rows hold the features
+(x[14] = m) and the scaled dissipation y itself; the training target is y / m.
+This module runs the pipeline with the library's own kernels:
 
 1. ``harvest``: exact runs of the Alfven-wave (32^3, 10 global steps) and
    blast-wave (64^3, 50 global steps) workloads in harvesting mode collect
@@ -23,6 +26,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import time
 
 import numpy as np
@@ -96,17 +100,48 @@ def harvest(scale=1.0):
     return np.concatenate(Xs), np.concatenate(Ys)
 
 
-def standardisation(X, Y):
-    """Per-feature and per-output mean and spread of a harvested set (the
+M_COL = 14  # feature column holding the jump size m
+
+
+def targets(X, Y):
+    """Training targets: the scaled dissipation divided by the jump size m
+    (rows with m = 0 have zero dissipation and are dropped by the caller)."""
+    m = np.asarray(X[:, M_COL], np.float64)[:, None]
+    return (np.asarray(Y, np.float64) / np.where(m > 0, m, 1.0)).astype(np.float32)
+
+
+def usable(X):
+    """Rows that carry a jump (m > 0)."""
+    return X[:, M_COL] > 0
+
+
+def standardisation(X, T):
+    """Per-feature and per-target mean and spread of a harvested set (the
     unlearned normal induction output keeps spread 1)."""
     mu_x = X.mean(axis=0, dtype=np.float64)
     sd_x = X.std(axis=0, dtype=np.float64)
     sd_x = np.maximum(sd_x, 1e-3)  # features nearly constant in training keep a usable spread
-    mu_y = Y.mean(axis=0, dtype=np.float64)
-    sd_y = Y.std(axis=0, dtype=np.float64)
+    mu_y = T.mean(axis=0, dtype=np.float64)
+    sd_y = T.std(axis=0, dtype=np.float64)
     sd_y = np.where((sd_y > 1e-12) & (OUTPUT_WEIGHTS > 0), sd_y, 1.0)
     mu_y = np.where(OUTPUT_WEIGHTS > 0, mu_y, 0.0)
     return {k: v.astype(np.float32) for k, v in (("mu_x", mu_x), ("sd_x", sd_x), ("mu_y", mu_y), ("sd_y", sd_y))}
+
+
+# Version tag of the network's input and output definition, stored with the
+# weights; weights of another form would be fed the wrong features.
+FORM = "jump-scaled dissipation, features v2"
+DEFAULT_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "flux_mlp.npz")
+
+
+def load_model(path=DEFAULT_WEIGHTS):
+    """Parameters and standardisation of a trained network (.npz written by
+    main); raises if the file holds another form of the network."""
+    z = np.load(path)
+    form = str(z["form"]) if "form" in z else "(none)"
+    if form != FORM:
+        raise ValueError(f"{path}: network form {form!r}, expected {FORM!r}")
+    return {k: z[k] for k in ("params", "mu_x", "sd_x", "mu_y", "sd_y")}
 
 
 def apply(sys, model):
@@ -116,18 +151,21 @@ def apply(sys, model):
 
 
 def predict(sys, model, X):
-    """Scaled dissipation the loaded model predicts for raw features X."""
+    """Scaled dissipation the loaded model predicts for raw features X
+    (m times the unstandardised network output, as the flux pass forms it)."""
     Xn = (X - model["mu_x"]) / model["sd_x"]
-    return model["mu_y"] + model["sd_y"] * sys.mlp_eval(Xn)
+    return X[:, [M_COL]] * (model["mu_y"] + model["sd_y"] * sys.mlp_eval(Xn))
 
 
 def train(X, Y, steps=12000, batch=8192, seed=0, lr_schedule=(2e-3, 1e-3, 3e-4, 1e-4), sys=None):
-    """Train from init_params(seed) on the GPU on the standardised set;
-    returns (model dict, loss history)."""
+    """Train from init_params(seed) on the GPU on the standardised set of
+    targets y / m; returns (model dict, loss history)."""
     s = sys or System()
-    model = standardisation(X, Y)
+    keep = usable(X)
+    X, T = X[keep], targets(X[keep], Y[keep])
+    model = standardisation(X, T)
     Xn = ((X - model["mu_x"]) / model["sd_x"]).astype(np.float32)
-    Yn = ((Y - model["mu_y"]) / model["sd_y"]).astype(np.float32)
+    Yn = ((T - model["mu_y"]) / model["sd_y"]).astype(np.float32)
     s.mlp_set_weights(init_params(seed))
     hist = []
     per = max(1, steps // len(lr_schedule))
@@ -140,10 +178,13 @@ def train(X, Y, steps=12000, batch=8192, seed=0, lr_schedule=(2e-3, 1e-3, 3e-4, 
 def llf_dissipation(X):
     """Scaled face-frame dissipation of the local Lax-Friedrichs (Rusanov)
     flux, -(max wave speed)/2 times the jump of the conserved state, in the
-    network's output units: the method without the network."""
+    network's output units, from the features to first order in the jump
+    (the flux pass evaluates it exactly from the side states): the method
+    without the network."""
     x = np.asarray(X, np.float64)
     u, v, w, p, bx, by, bz = (x[:, k] for k in range(7))
-    dr, du, dv, dw, dpr, dby, dbz = (x[:, 7 + k] for k in range(7))
+    jump = x[:, 7:14] * x[:, [M_COL]]
+    dr, du, dv, dw, dpr, dby, dbz = (jump[:, k] for k in range(7))
     smax = np.abs(u) + np.abs(du) / 2 + 1.0  # |u| + c (c = 1 in these units)
     # conserved jumps with rho = 1 + dr/2 on the right, 1 - dr/2 on the left
     dmom = [u * dr + du, v * dr + dv, w * dr + dw]
@@ -183,20 +224,26 @@ def holdout(model, problem="blast", nside=128, steps=20, hstride=64, order="hilb
 def evaluate(model, nside=128, steps=100, judge=1024, order="hilbert"):
     """The blast with the learned flux + FP32 bulk path against the plain
     FP64 path after `steps` global steps: relative L1 error per conserved
-    variable, fallback and judged statistics, and face-updates/s of both."""
+    variable, fallback and judged statistics, and face-updates/s.  The same
+    run is repeated with the gated faces taking the central flux alone (no
+    dissipation) and the local Lax-Friedrichs dissipation in place of the
+    network, and with the exact solver everywhere (FP32 bulk)."""
     import torch
     m = _lattice_mesh(nside, 1, order)
     W = problems.blast(m.pos)
     out = {"cell_order": order}
     states = {}
-    for name, prec, mode in (("plain_fp64", FVM_PREC_FP64, 0), ("fp32", FVM_PREC_FP32, 0),
-                             ("learned_fp32", FVM_PREC_FP32, 1)):
+    runs = (("plain_fp64", FVM_PREC_FP64, 0, None), ("fp32", FVM_PREC_FP32, 0, None),
+            ("learned_fp32", FVM_PREC_FP32, 1, "network"), ("central_fp32", FVM_PREC_FP32, 1, "central"),
+            ("llf_fp32", FVM_PREC_FP32, 1, "llf"))
+    for name, prec, mode, sur in runs:
         s = System(precision=prec)
         s.set_mesh(m)
         s.init_problem(W)
         if mode == 1:
             apply(s, model)
             s.set_flux_mode(1, judge=judge, **GATE)
+            s.set_flux_surrogate(sur)
         stream = torch.cuda.ExternalStream(s.stream_ptr)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
@@ -209,12 +256,12 @@ def evaluate(model, nside=128, steps=100, judge=1024, order="hilbert"):
         out[name] = {"face_updates_per_s": faces / (ms / 1e3), "ms_per_step": ms / steps}
         if mode == 1:
             st = s.learn_stats()
-            st["deferred_fraction"] = st["deferred"] / max(faces, 1)
+            st["deferred_fraction"] = st["deferred"] / max(2 * faces, 1)
             st["fallback_fraction"] = st["fallback"] / max(st["deferred"], 1)
             out[name]["learned"] = st
         s.close()
     ref = states["plain_fp64"]
-    for name in ("fp32", "learned_fp32"):
+    for name, *_ in runs[1:]:
         d = np.abs(states[name] - ref).sum(axis=0) / np.maximum(np.abs(ref).sum(axis=0), 1e-300)
         out[name]["rel_l1_vs_fp64"] = {k: float(d[i]) for i, k in
                                        enumerate(["mass", "momx", "momy", "momz", "energy", "bx", "by", "bz",
@@ -248,8 +295,7 @@ def main():
                           "finite": bool(np.isfinite(Y).all())}))
         return
     if args.weights:
-        z = np.load(args.weights)
-        model = {k: z[k] for k in ("params", "mu_x", "sd_x", "mu_y", "sd_y")}
+        model = load_model(args.weights)
     else:
         t0 = time.perf_counter()
         X, Y = harvest()
@@ -262,13 +308,16 @@ def main():
         apply(s, model)
         pred = predict(s, model, X[idx])
         w = OUTPUT_WEIGHTS.astype(bool)
-        err_mlp = np.abs(pred - Y[idx])[:, w].mean()
-        err_llf = np.abs(llf_dissipation(X[idx]) - Y[idx])[:, w].mean()
+        e_mlp = np.abs(pred - Y[idx])[:, w]
+        e_llf = np.abs(llf_dissipation(X[idx]) - Y[idx])[:, w]
+        ref = np.abs(Y[idx])[:, w]
         print(json.dumps({"pairs": int(X.shape[0]), "harvest_s": t1 - t0, "train_s": t2 - t1,
-                          "final_loss": float(hist[-200:].mean()), "mean_abs_err_network": float(err_mlp),
-                          "mean_abs_err_llf": float(err_llf), "mean_abs_target": float(np.abs(Y[idx])[:, w].mean())}))
+                          "final_loss": float(hist[-200:].mean()), "mean_abs_err_network": float(e_mlp.mean()),
+                          "mean_abs_err_llf": float(e_llf.mean()), "mean_abs_target": float(ref.mean()),
+                          "rel_l1_network": float(e_mlp.sum() / ref.sum()),
+                          "rel_l1_llf": float(e_llf.sum() / ref.sum())}))
         if args.out:
-            np.savez_compressed(args.out, loss=hist, gate=json.dumps(GATE), **model)
+            np.savez_compressed(args.out, loss=hist, gate=json.dumps(GATE), form=FORM, **model)
     if args.evaluate:
         print(json.dumps({"holdout_blast128": holdout(model, order=args.eval_order)}))
         print(json.dumps(evaluate(model, nside=args.eval_nside, steps=args.eval_steps, order=args.eval_order)))

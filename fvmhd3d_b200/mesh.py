@@ -74,10 +74,22 @@ class Mesh:
     def closure_error(self) -> np.ndarray:
         """|sum of outward area vectors| / V^(2/3) per cell (the reference's
         closure check, MPI/compute_update.cpp:307-320)."""
-        acc = np.zeros((self.ncell, 3))
-        np.add.at(acc, self.s1, self.n)
-        np.add.at(acc, self.s2, -self.n)
+        acc = np.stack([np.bincount(self.s1, self.n[:, k], self.ncell) - np.bincount(self.s2, self.n[:, k], self.ncell)
+                        for k in range(3)], axis=1)
         return np.linalg.norm(acc, axis=1) / self.volume ** (2.0 / 3.0)
+
+    def save(self, path) -> None:
+        """Write the mesh arrays to an uncompressed .npz (for processes that
+        share one host-built mesh)."""
+        np.savez(path, box=self.box, pos=self.pos, s1=self.s1, s2=self.s2, n=self.n, centroid=self.centroid,
+                 volume=self.volume, cell_centroid=self.cell_centroid, cell_face_off=self.cell_face_off,
+                 cell_face_ids=self.cell_face_ids)
+
+    @staticmethod
+    def load(path) -> "Mesh":
+        z = np.load(path)
+        return Mesh(z["box"], z["pos"], z["s1"], z["s2"], z["n"], z["centroid"], z["volume"], z["cell_centroid"],
+                    z["cell_face_off"], z["cell_face_ids"])
 
 
 def build_periodic(pos: np.ndarray, box, nthreads: int = 0) -> Mesh:

@@ -193,6 +193,20 @@ class System:
         self._check(self.L.fvm_mlp_eval(self.h, X.shape[0], _p(X), _p(Y)), "fvm_mlp_eval")
         return Y
 
+    def mlp_eval_counted(self, X, n, Y0=None) -> np.ndarray:
+        """The network with its row count n read on the device (the form the
+        flux passes launch): rows n.. of the result keep Y0 (zeros)."""
+        X = np.ascontiguousarray(X, np.float32)
+        Y = np.zeros((X.shape[0], 8), np.float32) if Y0 is None else np.array(Y0, np.float32, copy=True)
+        self._check(self.L.fvm_mlp_eval_counted(self.h, X.shape[0], int(n), _p(X), _p(Y)), "fvm_mlp_eval_counted")
+        return Y
+
+    def set_flux_surrogate(self, kind) -> None:
+        """What stands in for the dissipation on gated faces: "network" (the
+        default), "central" (none) or "llf" (local Lax-Friedrichs)."""
+        k = {"network": 0, "central": 1, "llf": 2}[kind] if isinstance(kind, str) else int(kind)
+        self._check(self.L.fvm_set_flux_surrogate(self.h, k), "fvm_set_flux_surrogate")
+
     def set_flux_mode(self, mode, drho=0.05, dp=0.05, mach=1.0, judge=1024, hstride=1, hcap=0) -> None:
         """Learned-flux mode of the flux passes: 0 exact, 1 network on gated
         faces, 2 exact with harvesting (see fvm_set_flux_mode)."""
@@ -210,7 +224,8 @@ class System:
         self._check(self.L.fvm_learn_stats(self.h, _p(s)), "fvm_learn_stats")
         return {"deferred": int(s[0]), "fallback": int(s[1]), "judged": int(s[2]),
                 "judged_rel_l1": float(s[3] / s[4]) if s[4] > 0 else 0.0,
-                "judged_mean_abs": float(s[3] / (8 * s[2])) if s[2] > 0 else 0.0, "judged_max_abs": float(s[5])}
+                "judged_mean_abs": float(s[3] / (7 * s[2])) if s[2] > 0 else 0.0, "judged_max_abs": float(s[5]),
+                "positivity_fallback": int(s[6])}
 
     def harvest(self):
         """(X, Y) pairs harvested in mode 2 so far."""
@@ -256,6 +271,11 @@ class System:
         self._check(self.L.fvm_autotune(self.h, 1 if shared else 0, int(steps), _p(ch)), "fvm_autotune")
         return {"staged_limiter": int(ch[0]), "face_block": int(ch[1]), "cell_block": int(ch[2]),
                 "cell2_block": int(ch[3])}
+
+    def set_tuning(self, staged_limiter, face_block, cell_block, cell2_block) -> None:
+        """Set the launch choices the autotuner picks (see autotune)."""
+        ch = np.array([staged_limiter, face_block, cell_block, cell2_block], np.int32)
+        self._check(self.L.fvm_set_tuning(self.h, _p(ch)), "fvm_set_tuning")
 
     def clock(self):
         """(tsysU, dt_global, iteration): the scheduler clock after the last

@@ -207,6 +207,12 @@ int fvm_mlp_set_weights(fvm_ctx *c, const float *params);
  * buffers in and out (X rounded to BF16). */
 int fvm_mlp_eval(fvm_ctx *c, int n, const float *X, float *Y);
 
+/* The same network with the row count read on the device, as the flux
+ * passes launch it: the grid is sized for nmax rows (X and Y hold nmax rows),
+ * the kernel reads n (0 <= n <= nmax) from device memory and leaves rows n..
+ * of Y as they were passed in. */
+int fvm_mlp_eval_counted(fvm_ctx *c, int nmax, int n, const float *X, float *Y);
+
 /* The FP32 master parameters (FVM_MLP_NPARAM floats). */
 int fvm_mlp_get_weights(fvm_ctx *c, float *params);
 
@@ -229,21 +235,32 @@ int fvm_mlp_train(fvm_ctx *c, long long n, const float *X, const float *T, const
  * sampled) appends its (features, targets) to a device harvest buffer of
  * hcap rows.  Gate: ideal-gas EOS, no boundary neighbour, relative density
  * and pressure jumps at most drho and dp, normal Mach number in the face
- * frame at most mach.  In mode 1 a face whose network flux would move more
- * than half of either cell's mass within its step falls back to the exact
- * solver, and one deferred face in `judge` (0: none) is also solved exactly
- * to record the network's error.  Resets the statistics. */
+ * frame at most mach.  In mode 1 a face falls back to the exact solver when
+ * the state either of its cells reaches from that face's network flux alone,
+ * over the cell's step, keeps less than half of the cell's mass or thermal
+ * energy (positivity of the updated state); one deferred face in `judge`
+ * (0: none) is also solved exactly to record the network's error.  Resets
+ * the statistics. */
 int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, int judge, int hstride,
                       long long hcap);
 
-/* Standardisation of the network: inputs (features - mu_x) / sd_x, outputs
- * mu_y + sd_y * network (16, 16, 8, 8 floats; identity by default). */
+/* What stands in for the HLLD dissipation on the faces the gate passes, in
+ * mode 1: 0 the network (the default), 1 none (the central flux alone), 2 the
+ * local Lax-Friedrichs dissipation.  1 and 2 are comparisons for the
+ * network; gate, fallback and judge work as in mode 1.  Has no counterpart in
+ * the reference (an addition of the learned form). */
+int fvm_set_flux_surrogate(fvm_ctx *c, int kind);
+
+/* Standardisation of the network: inputs (features - mu_x) / sd_x; the scaled
+ * dissipation of a face is m (mu_y + sd_y * network), m the size of the
+ * face's scaled jump (16, 16, 8, 8 floats; identity by default). */
 int fvm_mlp_set_norm(fvm_ctx *c, const float *mu_x, const float *sd_x, const float *mu_y, const float *sd_y);
 
 /* Cumulative learned-flux statistics since fvm_set_flux_mode: [0] deferred
  * faces, [1] exact fallbacks, [2] judged faces, [3] sum over judged faces of
- * the L1 error of the 8 scaled outputs, [4] sum of their L1 norms, [5] the
- * largest single-output error. */
+ * the L1 error of the 7 predicted scaled outputs, [4] sum of their L1 norms,
+ * [5] the largest single-output error, [6] fallbacks of the positivity test
+ * (counted in [1] too). */
 int fvm_learn_stats(fvm_ctx *c, double *stats8);
 
 /* Rows harvested so far (capped at hcap), and a copy of the first n of them
@@ -258,6 +275,11 @@ int fvm_get_harvest(fvm_ctx *c, long long n, float *X, float *Y);
  * two-threads-per-cell kernels.  choice (4 ints, may be NULL) receives
  * {staged limiter, face block, cell block, two-thread cell block}. */
 int fvm_autotune(fvm_ctx *c, int shared, int steps, int *choice);
+
+/* Sets the launch choices fvm_autotune picks (same 4 ints: staged limiter
+ * 0/1, then block sizes 32, 64 or 128), e.g. to replay a tuned configuration
+ * on another run of the same mesh. */
+int fvm_set_tuning(fvm_ctx *c, const int *choice);
 
 /* Timing helper: CUDA-event time in ms of the last fvm_step's kernels. */
 float fvm_last_step_ms(const fvm_ctx *c);

@@ -25,13 +25,18 @@ REF_SO = os.path.join(HERE, "_ref", "libfvmref.so")
 ORACLE_SO = os.path.join(HERE, "_ref", "liboracle.so")
 
 
+# The reference's MPI-tree sources, read where they lie (the Makefile's
+# REF_DIR default); FVM_REF_DIR points the build elsewhere.
+REF_DIR = os.environ.get("FVM_REF_DIR", "/root/reference/MPI")
+
+
 def build(ref: bool = True) -> None:
     """Compile the checkers with oracle/Makefile (the reference build only when
     its sources are present)."""
     targets = ["oracle"]
-    if ref and os.path.isdir("/root/reference/MPI"):
+    if ref and os.path.isdir(REF_DIR):
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+    subprocess.run(["make", "-s", "-C", HERE, f"REF_DIR={REF_DIR}"] + targets, check=True)
 
 
 class _Params(ctypes.Structure):

@@ -10,9 +10,11 @@ from common import setup_case
 pytestmark = pytest.mark.gpu
 
 # Relative L1 error bound per conserved variable after the steps below
-# (sum |fp32 - oracle| / sum |oracle|): single precision carries ~1e-7
-# relative error into each flux.
-RTOL_L1_FP32 = 1e-4
+# (sum |fp32 - oracle| / sum |oracle|; a magnetic component against the L1
+# norm of the whole field, since one component can start at zero): single
+# precision carries ~1e-7 relative error into each flux, and the measured
+# errors are 1e-9 to 1e-6.
+RTOL_L1_FP32 = 1e-5
 
 
 def run(problem, nside, nsteps, precision):
@@ -42,7 +44,9 @@ def test_fp32_error_vs_fp64_oracle(problem, nside, nsteps):
     m, W, s = run(problem, nside, nsteps, F.FVM_PREC_FP32)
     o = oracle(m, W, nsteps)
     a, b = s.get_state()["U"], o.get_state()["U"]
-    l1 = np.abs(a - b).sum(axis=0) / np.maximum(np.abs(b).sum(axis=0), 1e-300)
+    den = np.abs(b).sum(axis=0)
+    den[5:8] = np.sqrt((b[:, 5:8] ** 2).sum(axis=1)).sum()
+    l1 = np.abs(a - b).sum(axis=0) / np.maximum(den, 1e-300)
     print(problem, "rel L1 per conserved variable:", " ".join("%.2e" % x for x in l1))
     for k in (0, 1, 2, 3, 4, 5, 6, 7):  # mass, momentum, energy, magnetic flux
         assert l1[k] <= RTOL_L1_FP32, (k, l1[k])

@@ -311,3 +311,49 @@ def test_mesh_input_validation_keeps_the_context_usable():
     o = oracle_system(m, W)
     assert s.step(shared=True) == o.step(shared=True)
     assert_state_close(s.get_state(), o.get_state())
+
+
+def hilbert_case(nside, problem, seed=1):
+    """The benchmark's mesh: jittered lattice with its cells in Peano-Hilbert
+    order (the reference's sort_local_data)."""
+    import fvmhd3d_b200 as F
+    pos = F.jittered_lattice(nside, 0.1, seed=seed)
+    m = F.build_periodic(pos[F.sort_local_data(pos, 1.0)], 1.0)
+    return m, getattr(F.problems, problem)(m.pos)
+
+
+@pytest.mark.slow
+def test_blast_128cubed_benchmark_configuration_vs_oracle():
+    """The benchmark's own workload at full size: the 128^3 blast on the
+    Peano-Hilbert-ordered mesh (2,097,152 cells, 16.7M faces), 2 global
+    steps replayed from the captured step graph, once with the autotuner's
+    choices and once with 32-thread blocks and the staged limiter forced,
+    against the oracle at 1e-12 with exact rungs, tlast and tend."""
+    m, W = hilbert_case(128, "blast")
+    o = oracle_system(m, W)
+    for _ in range(2):
+        assert o.step(shared=True) == m.ncell
+    ref, t_ref = o.get_state(), o.time
+    o.close()
+    for forced in (None, (1, 32, 32, 32)):
+        s = gpu_system(m, W)
+        if forced:
+            s.set_tuning(*forced)
+        else:
+            s.autotune(shared=True, steps=1)
+        cells, faces = s.run(2, shared=True)
+        assert cells == 2 * m.ncell and faces == 2 * m.nface
+        assert s.time == t_ref
+        assert_state_close(s.get_state(), ref)
+        s.close()
+
+
+def test_blast_64cubed_fp64_5_steps_vs_oracle():
+    """Configuration 2's mesh and problem on the plain FP64 path: the 64^3
+    blast (Peano-Hilbert order), 5 global steps."""
+    m, W = hilbert_case(64, "blast")
+    s, o = gpu_system(m, W), oracle_system(m, W)
+    for _ in range(5):
+        assert s.step(shared=True) == o.step(shared=True) == m.ncell
+    assert s.time == o.time
+    assert_state_close(s.get_state(), o.get_state())

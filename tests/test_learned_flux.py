@@ -34,10 +34,13 @@ def test_bf16_rounding():
 
 
 def test_twice_gelu_with_halved_weights_is_the_same_rounded_network():
-    """The inference kernel stores 2 gelu(z) as the next layer's BF16 input
-    and halves W2, W3 and W4 in its weights image.  Power-of-two scaling
-    commutes with BF16 rounding and cancels in each product, so the rounded
-    network is unchanged: outputs equal the oracle's bit for bit."""
+    """The algebra behind the inference kernel's weights image: storing
+    2 gelu(z) as the next layer's BF16 input and halving W2, W3 and W4 leaves
+    the oracle's rounded network unchanged, because power-of-two scaling
+    commutes with BF16 rounding and cancels in each product (checked here in
+    float64 with the oracle's own gelu).  It does not show that the kernel's
+    FP32 evaluation of 2 gelu (one fused multiply-add and the hardware tanh)
+    rounds like the oracle's; the GPU inference test bounds that difference."""
     rng = np.random.default_rng(4)
     p = M.init_params(9)
     X = rng.normal(size=(257, M.NIN))
@@ -50,8 +53,18 @@ def test_twice_gelu_with_halved_weights_is_the_same_rounded_network():
     assert np.array_equal(z, M.forward(p, X))
 
 
+# Tensor-core inference against the oracle's rounded network: largest error
+# per output over the rows, relative to that output's largest magnitude.  The
+# kernel differs from the oracle only by FP32 accumulation order and the
+# hardware tanh in its GELU epilogue (measured up to 4.0e-3 on 160,000 rows).
+INFER_RTOL = 6e-3
+
+
+# 148 SMs x 4 tile chains x 128 rows = 75,776 rows per wave: the larger
+# cases make every chain run several tiles (input prefetch, buffer and
+# tensor-memory reuse, mbarrier phases carried across tiles).
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [1, 1000, 128 * 400 + 17])
+@pytest.mark.parametrize("n", [1, 1000, 128 * 400 + 17, 160000, 303 * 512 + 5])
 def test_tensor_core_inference_matches_oracle(n):
     import fvmhd3d_b200 as F
     rng = np.random.default_rng(n)
@@ -64,14 +77,37 @@ def test_tensor_core_inference_matches_oracle(n):
     scale = np.abs(ref).max(axis=0)
     err = np.abs(got - ref).max(axis=0) / scale
     assert np.isfinite(got).all()
-    assert err.max() <= 2e-2, err
+    assert err.max() <= INFER_RTOL, err
+
+
+@pytest.mark.gpu
+def test_tensor_core_inference_with_a_device_row_count():
+    """The launch the flux passes make: grid sized for nmax rows, the row
+    count read on the device, well below nmax but spanning several tiles per
+    chain; rows past the count are left untouched."""
+    import fvmhd3d_b200 as F
+    nmax, n = 600000, 2 * 75776 + 4099
+    rng = np.random.default_rng(8)
+    p = M.init_params(6)
+    s = F.System()
+    s.mlp_set_weights(p)
+    X = rng.normal(size=(nmax, M.NIN)).astype(np.float32)
+    Y0 = np.full((nmax, M.NOUT), 7.0, np.float32)
+    got = s.mlp_eval_counted(X, n, Y0)
+    assert (got[n:] == 7.0).all()
+    ref = M.forward(p, X[:n])
+    err = np.abs(got[:n] - ref).max(axis=0) / np.abs(ref).max(axis=0)
+    assert err.max() <= INFER_RTOL, err
+
+
+GRAD_RTOL = 1e-2  # measured 1.6e-3 at most
 
 
 @pytest.mark.gpu
 def test_training_gradient_matches_oracle():
     """Backward kernels (BF16 tensor-core GEMMs, FP32 accumulation) against
     the oracle's backward pass of the same rounded network: loss to 1e-3,
-    each parameter block's gradient to 3e-2 in norm."""
+    each parameter block's gradient to GRAD_RTOL in norm."""
     import fvmhd3d_b200 as F
     rng = np.random.default_rng(11)
     p = M.init_params(7)
@@ -87,7 +123,7 @@ def test_training_gradient_matches_oracle():
     for shp in M.SHAPES:
         k = int(np.prod(shp))
         a, b = g[o:o + k], rg[o:o + k]
-        assert np.linalg.norm(a - b) <= 3e-2 * np.linalg.norm(b), shp
+        assert np.linalg.norm(a - b) <= GRAD_RTOL * np.linalg.norm(b), (shp, np.linalg.norm(a - b) / np.linalg.norm(b))
         o += k
 
 
@@ -153,6 +189,45 @@ def small_trained():
     X, Y = L.harvest(scale=0.1)
     model, hist = L.train(X, Y, steps=2000, batch=4096, seed=2)
     return X, Y, model, hist
+
+
+@pytest.mark.gpu
+def test_shipped_network_beats_central_and_llf_on_a_deployed_run():
+    """The shipped network on the faces a run actually hands it: the 32^3
+    blast, 10 global steps, FP32 bulk, every deferred face judged against the
+    exact solver.  Its dissipation error is under half the dissipation
+    itself (a central flux, i.e. no dissipation, scores 1), and the state
+    after the run is closer to the plain FP64 run than with the central flux
+    alone or the local Lax-Friedrichs dissipation on the same faces."""
+    import fvmhd3d_b200 as F
+    from fvmhd3d_b200 import learned as L
+    model = L.load_model()
+    pos = F.jittered_lattice(32, 0.1, seed=1)
+    m = F.build_periodic(pos[F.sort_local_data(pos, 1.0)], 1.0)
+    W = F.problems.blast(m.pos)
+    ref = F.System()
+    ref.set_mesh(m)
+    ref.init_problem(W)
+    ref.run(10, shared=True)
+    Ua = ref.get_state()["U"]
+    rel, judged = {}, {}
+    for sur in ("network", "central", "llf"):
+        s = F.System(precision=F.FVM_PREC_FP32)
+        s.set_mesh(m)
+        s.init_problem(W)
+        L.apply(s, model)
+        s.set_flux_mode(1, judge=1, **L.GATE)
+        s.set_flux_surrogate(sur)
+        s.run(10, shared=True)
+        Ub = s.get_state()["U"]
+        d = np.abs(Ub - Ua).sum(axis=0) / np.abs(Ua).sum(axis=0)
+        rel[sur] = d[[0, 4]].max()
+        st = s.learn_stats()
+        judged[sur] = st["judged_rel_l1"]
+        assert st["judged"] == st["deferred"] > 0
+    assert judged["network"] < 0.5, judged
+    assert abs(judged["central"] - 1.0) < 1e-6, judged
+    assert rel["network"] < rel["central"] and rel["network"] < rel["llf"], rel
 
 
 @pytest.mark.gpu

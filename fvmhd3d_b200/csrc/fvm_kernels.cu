@@ -46,9 +46,6 @@ using namespace fvm;
 #ifndef FVM_CELL_UNROLL
 #define FVM_CELL_UNROLL 1  // unroll factor of the cell kernels' face loops (1 and 2 time the same within 1%)
 #endif
-#ifndef FVM_RECON_PIPE
-#define FVM_RECON_PIPE 0  // the reconstruction's face loop as a software pipeline (loads one link ahead)
-#endif
 #ifndef FVM_REUSE_MINMAX
 #define FVM_REUSE_MINMAX 1  // the limiter reuses the reconstruction's neighbour min/max when every cell steps
 #endif
@@ -1688,33 +1685,6 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
       Wz[k] += sum * w6[2] + diff * w6[5];
     }
   };
-#if FVM_RECON_PIPE
-  // Software pipeline: the next link's weights and neighbour state are in
-  // flight while this link's terms are summed, and the link after next's
-  // (face, neighbour) entry is loaded one step earlier still, so no
-  // iteration waits on a dependent pair of loads.
-  if (q0 < qe) {
-    int2 fjn = lfj[q0];
-    R w6n[6], Wjn[KH];
-    load_n<R, 6>(lrw + 6 * (size_t)q0, w6n);
-    load_n<R, KH>(Wst + 10 * (size_t)(fjn.y >= 0 ? fjn.y : ~fjn.y) + k0, Wjn);
-    int2 fj2 = q0 + 1 < qe ? lfj[q0 + 1] : fjn;
-#pragma unroll 1
-    for (int q = q0; q < qe; q++) {
-      R w6[6], Wj[KH];
-#pragma unroll
-      for (int k = 0; k < 6; k++) w6[k] = w6n[k];
-#pragma unroll
-      for (int k = 0; k < KH; k++) Wj[k] = Wjn[k];
-      if (q + 1 < qe) {
-        load_n<R, 6>(lrw + 6 * (size_t)(q + 1), w6n);
-        load_n<R, KH>(Wst + 10 * (size_t)(fj2.y >= 0 ? fj2.y : ~fj2.y) + k0, Wjn);
-        if (q + 2 < qe) fj2 = lfj[q + 2];
-      }
-      face_term(w6, Wj);
-    }
-  }
-#else
   FVM_CELL_LOOP
   for (int q = q0; q < qe; q++) {
     const int2 fj = lfj[q];
@@ -1725,7 +1695,6 @@ __device__ __forceinline__ void recon_body(int c, int k0, const Params &P, const
     load_n<R, KH>(Wst + 10 * (size_t)j + k0, Wj);
     face_term(w6, Wj);
   }
-#endif
   // the next step's limiter pass 1 (neighbour min/max of the same states)
   {
     R *mm = mnmx + 20 * (size_t)c + k0;
@@ -3311,15 +3280,21 @@ int fvm_mlp_get_weights(fvm_ctx *c, float *params) {
 }
 
 // ---- training: forward + backward of one batch of `rows` rows ---------------
+// Largest K split of a training product (the weight gradients: M, N <= 128,
+// K = batch rows), and the partial tiles it needs.
+constexpr int kMaxSplit = 64;
+
 struct MlpWork {
   int rows = 0;
-  float *X, *T, *Z1, *Z2, *Z3, *Z4, *A1, *A2, *A3, *G, *dA, *dB, *grad, *loss, *wt, *m, *v;
+  float *X, *T, *Z1, *Z2, *Z3, *Z4, *A1, *A2, *A3, *G, *dA, *dB, *grad, *loss, *wt, *m, *v, *part;
   void *base = nullptr;
 };
 
 static int mlp_work(fvm_ctx *c, MlpWork &w, int rows) {
   using namespace mlp;
-  const size_t nf = (size_t)rows * (NIN + NOUT + 3 * NH + NOUT + 3 * NH + NOUT + 2 * NH) + 3 * (size_t)NPARAM + 1 + NOUT;
+  const size_t npart = (size_t)kMaxSplit * NH * NH;  // split-K partial tiles of the weight gradients
+  const size_t nf = (size_t)rows * (NIN + NOUT + 3 * NH + NOUT + 3 * NH + NOUT + 2 * NH) + 3 * (size_t)NPARAM + 1 + NOUT +
+                    npart;
   CK(cudaMallocAsync(&w.base, nf * sizeof(float), c->st));
   CK(cudaMemsetAsync(w.base, 0, nf * sizeof(float), c->st));
   float *p = (float *)w.base;
@@ -3331,13 +3306,35 @@ static int mlp_work(fvm_ctx *c, MlpWork &w, int rows) {
   w.A1 = take((size_t)rows * NH); w.A2 = take((size_t)rows * NH); w.A3 = take((size_t)rows * NH);
   w.G = take((size_t)rows * NOUT); w.dA = take((size_t)rows * NH); w.dB = take((size_t)rows * NH);
   w.grad = take(NPARAM); w.m = take(NPARAM); w.v = take(NPARAM); w.loss = take(1); w.wt = take(NOUT);
+  w.part = take(npart);
+  // the tensor-core product's shared memory, set once per device
+  static bool attr[kMaxDevices] = {};
+  if (c->device < 0 || c->device >= kMaxDevices) { c->err = "device index out of range"; return FVM_EINVAL; }
+  if (!attr[c->device]) {
+    CK(cudaFuncSetAttribute(mlpt::k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, mlpt::TC_SMEM));
+    attr[c->device] = true;
+  }
   return 0;
 }
 
-static void gemm(cudaStream_t s, int M, int N, int K, const float *A, long long sam, long long sak, const float *B,
-                 long long sbk, long long sbn, float *C, int ldc) {
-  dim3 grid((N + mlpt::GT - 1) / mlpt::GT, (M + mlpt::GT - 1) / mlpt::GT);
-  mlpt::k_gemm<<<grid, 128, 0, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, 0);
+// C = A B on the tensor cores (mlpt::k_gemm_tc).  Products with one output
+// tile and a long K are split over up to kMaxSplit CTAs of at least two
+// chunks each and summed in split order.
+static void gemm(fvm_ctx *c, const MlpWork &w, int M, int N, int K, const float *A, long long sam, long long sak,
+                 const float *B, long long sbk, long long sbn, float *C, int ldc) {
+  cudaStream_t s = c->st;
+  const int tiles_m = (M + mlpt::TM - 1) / mlpt::TM, tiles_n = (N + mlpt::TN - 1) / mlpt::TN;
+  const int nchunk = (K + mlpt::TK - 1) / mlpt::TK;
+  int nsplit = 1, cps = nchunk;
+  if (tiles_m * tiles_n == 1 && nchunk >= 4) {
+    nsplit = std::min(kMaxSplit, nchunk / 2);
+    cps = (nchunk + nsplit - 1) / nsplit;
+    nsplit = (nchunk + cps - 1) / cps;
+  }
+  dim3 grid(tiles_n, tiles_m, nsplit);
+  mlpt::k_gemm_tc<<<grid, 128, mlpt::TC_SMEM, s>>>(M, N, K, A, sam, sak, B, sbk, sbn, C, ldc, 0, cps, w.part,
+                                                   c->mlp_err);
+  if (nsplit > 1) mlpt::k_splitk_sum<<<(M * N + 255) / 256, 256, 0, s>>>(M, N, nsplit, w.part, C, ldc, 0);
 }
 
 // Loss (added to *w.loss) and gradient (w.grad) of the batch in w.X / w.T at
@@ -3354,28 +3351,28 @@ static int mlp_fwd_bwd(fvm_ctx *c, MlpWork &w, const float *P) {
   const long long nh = (long long)B * NH;
   const unsigned eb = (unsigned)((nh + 255) / 256);
   // forward
-  gemm(s, B, NH, NIN, w.X, NIN, 1, W1, 1, NIN, w.Z1, NH);
+  gemm(c, w, B, NH, NIN, w.X, NIN, 1, W1, 1, NIN, w.Z1, NH);
   mlpt::k_bias_gelu<<<eb, 256, 0, s>>>(B, NH, w.Z1, b1, w.A1);
-  gemm(s, B, NH, NH, w.A1, NH, 1, W2, 1, NH, w.Z2, NH);
+  gemm(c, w, B, NH, NH, w.A1, NH, 1, W2, 1, NH, w.Z2, NH);
   mlpt::k_bias_gelu<<<eb, 256, 0, s>>>(B, NH, w.Z2, b2, w.A2);
-  gemm(s, B, NH, NH, w.A2, NH, 1, W3, 1, NH, w.Z3, NH);
+  gemm(c, w, B, NH, NH, w.A2, NH, 1, W3, 1, NH, w.Z3, NH);
   mlpt::k_bias_gelu<<<eb, 256, 0, s>>>(B, NH, w.Z3, b3, w.A3);
-  gemm(s, B, NOUT, NH, w.A3, NH, 1, W4, 1, NH, w.Z4, NOUT);
+  gemm(c, w, B, NOUT, NH, w.A3, NH, 1, W4, 1, NH, w.Z4, NOUT);
   mlpt::k_out_loss<<<(B * NOUT + 255) / 256, 256, 0, s>>>(B, w.Z4, b4, w.T, w.wt, w.G, w.loss);
   // backward
-  gemm(s, NOUT, NH, B, w.G, 1, NOUT, w.A3, NH, 1, gW4, NH);
+  gemm(c, w, NOUT, NH, B, w.G, 1, NOUT, w.A3, NH, 1, gW4, NH);
   mlpt::k_colsum<<<1, 32, 0, s>>>(B, NOUT, w.G, gb4);
-  gemm(s, B, NH, NOUT, w.G, NOUT, 1, W4, NH, 1, w.dA, NH);
+  gemm(c, w, B, NH, NOUT, w.G, NOUT, 1, W4, NH, 1, w.dA, NH);
   mlpt::k_gelu_back<<<eb, 256, 0, s>>>(nh, w.dA, w.Z3);
-  gemm(s, NH, NH, B, w.dA, 1, NH, w.A2, NH, 1, gW3, NH);
+  gemm(c, w, NH, NH, B, w.dA, 1, NH, w.A2, NH, 1, gW3, NH);
   mlpt::k_colsum<<<1, NH, 0, s>>>(B, NH, w.dA, gb3);
-  gemm(s, B, NH, NH, w.dA, NH, 1, W3, NH, 1, w.dB, NH);
+  gemm(c, w, B, NH, NH, w.dA, NH, 1, W3, NH, 1, w.dB, NH);
   mlpt::k_gelu_back<<<eb, 256, 0, s>>>(nh, w.dB, w.Z2);
-  gemm(s, NH, NH, B, w.dB, 1, NH, w.A1, NH, 1, gW2, NH);
+  gemm(c, w, NH, NH, B, w.dB, 1, NH, w.A1, NH, 1, gW2, NH);
   mlpt::k_colsum<<<1, NH, 0, s>>>(B, NH, w.dB, gb2);
-  gemm(s, B, NH, NH, w.dB, NH, 1, W2, NH, 1, w.dA, NH);
+  gemm(c, w, B, NH, NH, w.dB, NH, 1, W2, NH, 1, w.dA, NH);
   mlpt::k_gelu_back<<<eb, 256, 0, s>>>(nh, w.dA, w.Z1);
-  gemm(s, NH, NIN, B, w.dA, 1, NH, w.X, NIN, 1, gW1, NIN);
+  gemm(c, w, NH, NIN, B, w.dA, 1, NH, w.X, NIN, 1, gW1, NIN);
   mlpt::k_colsum<<<1, NH, 0, s>>>(B, NH, w.dA, gb1);
   c->launches += 21;
   CK(cudaGetLastError());
@@ -3403,8 +3400,11 @@ int fvm_mlp_grad(fvm_ctx *c, int n, const float *X, const float *T, const float 
   if ((rc = mlp_fwd_bwd(c, w, c->mlp_param))) return rc;
   CK(cudaMemcpyAsync(grad, w.grad, mlp::NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->st));
   CK(cudaMemcpyAsync(loss, w.loss, sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  int herr = 0;
+  CK(cudaMemcpyAsync(&herr, c->mlp_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaFreeAsync(w.base, c->st));
   CK(cudaStreamSynchronize(c->st));
+  if (herr & 4) { c->err = "fvm_mlp_grad: tensor-core product wait timed out"; return FVM_ECUDA; }
   return 0;
 }
 
@@ -3441,11 +3441,14 @@ int fvm_mlp_train(fvm_ctx *c, long long n, const float *X, const float *T, const
   LAUNCH_CHECK();
   if (loss_out && steps > 0)
     CK(cudaMemcpyAsync(loss_out, hist, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost, c->st));
+  int herr = 0;
+  CK(cudaMemcpyAsync(&herr, c->mlp_err, sizeof(int), cudaMemcpyDeviceToHost, c->st));
   CK(cudaFreeAsync(dX, c->st));
   CK(cudaFreeAsync(dT, c->st));
   CK(cudaFreeAsync(hist, c->st));
   CK(cudaFreeAsync(w.base, c->st));
   CK(cudaStreamSynchronize(c->st));
+  if (herr & 4) { c->err = "fvm_mlp_train: tensor-core product wait timed out"; return FVM_ECUDA; }
   return 0;
 }
 

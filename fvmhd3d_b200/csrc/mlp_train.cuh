@@ -1,7 +1,7 @@
 // Training kernels of the learned face flux (the network of flux_mlp.cuh):
 // forward and backward passes built from one strided BF16 tensor-core GEMM
-// (mma.sync m16n8k16, FP32 accumulation), elementwise bias/GELU kernels, a
-// mean-squared loss and Adam.  Activations are stored in FP32 holding
+// (tcgen05.mma, FP32 accumulation in tensor memory), elementwise bias/GELU
+// kernels, a mean-squared loss and Adam.  Activations are stored in FP32 holding
 // BF16-rounded values, weights as an FP32 master copy rounded to BF16 where
 // they enter a product, as in inference.
 //
@@ -15,81 +15,158 @@ using mlp::NOUT;
 using mlp::NPARAM;
 
 // C[m, n] (+)= sum_k A(m, k) B(k, n), A(m, k) = A[m*sam + k*sak],
-// B(k, n) = B[k*sbk + n*sbn], C row-major with leading dimension ldc.
-// 64 x 64 tiles, K in steps of 16, four warps of 32 x 32.
-constexpr int GT = 64, GK = 16;
+// B(k, n) = B[k*sbk + n*sbn], C row-major with leading dimension ldc: every
+// product of the forward and backward passes, on the 5th-generation tensor
+// cores.  One CTA (four warps) owns a 128 x 128 tile of C in 128 columns of
+// tensor memory (FP32).  K runs in chunks of 64 through two shared-memory
+// stages: all threads load a chunk of each operand from global memory with
+// the operand's strides (so transposed operands need no copy), round it to
+// BF16 and store it in the K-major no-swizzle core-matrix layout; one thread
+// issues four tcgen05.mma (kind::f16, K = 16 each) on it and commits them to
+// the stage's mbarrier, which the chunk two steps later waits on before it
+// overwrites the stage.  Rows, columns and K past the operand's extent are
+// zero-filled.  With gridDim.z > 1 the K range is split: split z covers
+// chunks [z*cps, (z+1)*cps) and writes its partial tile to
+// Cpart[z][M][N] (reduced in a fixed order by k_splitk_sum), so the weight
+// gradients (M, N <= 128, K = batch rows) spread over many SMs and stay
+// deterministic.  err bit 4: an mbarrier wait gave up.
+constexpr int TM = 128, TN = 128, TK = 64;
+constexpr int TC_A = TM * TK * 2, TC_B = TN * TK * 2;  // bytes of one stage's operand tiles
+constexpr int TC_SMEM = 2 * (TC_A + TC_B) + 32;          // two stages, two mbarriers, tensor-memory slot
 
-__device__ __forceinline__ uint32_t pk(__nv_bfloat16 lo, __nv_bfloat16 hi) {
-  return (uint32_t)__bfloat16_as_ushort(lo) | ((uint32_t)__bfloat16_as_ushort(hi) << 16);
+__device__ __forceinline__ void tc_load_stage(unsigned char *sa, unsigned char *sb, int m0, int n0, int k0, int M,
+                                              int N, int K, const float *__restrict__ A, long long sam,
+                                              long long sak, const float *__restrict__ B, long long sbk,
+                                              long long sbn) {
+  const int t = threadIdx.x;
+  // the index order follows the operand's unit stride, so warps read runs
+  // of consecutive floats
+#pragma unroll 4
+  for (int e = t; e < TM * TK; e += 128) {
+    const int r = sak == 1 ? e / TK : e % TM, k = sak == 1 ? e % TK : e / TM;
+    const int gm = m0 + r, gk = k0 + k;
+    const float v = (gm < M && gk < K) ? A[gm * sam + gk * sak] : 0.0f;
+    *reinterpret_cast<__nv_bfloat16 *>(sa + mlp::kmajor_off(r, k, TM)) = __float2bfloat16_rn(v);
+  }
+#pragma unroll 4
+  for (int e = t; e < TN * TK; e += 128) {
+    const int r = sbk == 1 ? e / TK : e % TN, k = sbk == 1 ? e % TK : e / TN;
+    const int gn = n0 + r, gk = k0 + k;
+    const float v = (gn < N && gk < K) ? B[gk * sbk + gn * sbn] : 0.0f;
+    *reinterpret_cast<__nv_bfloat16 *>(sb + mlp::kmajor_off(r, k, TN)) = __float2bfloat16_rn(v);
+  }
 }
 
-__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const float *__restrict__ A, long long sam,
-                                              long long sak, const float *__restrict__ B, long long sbk,
-                                              long long sbn, float *__restrict__ C, int ldc, int accumulate) {
-  __shared__ __nv_bfloat16 As[GT][GK + 8];   // [m][k]
-  __shared__ __nv_bfloat16 Bs[GT][GK + 8];   // [n][k]
-  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-  const int m0 = blockIdx.y * GT, n0 = blockIdx.x * GT;
-  const int wm = (w >> 1) * 32, wn = (w & 1) * 32;
-  const int g = lane >> 2, q = lane & 3;
-  float acc[2][4][4];
-#pragma unroll
-  for (int i = 0; i < 2; i++)
-#pragma unroll
-    for (int j = 0; j < 4; j++)
-#pragma unroll
-      for (int r = 0; r < 4; r++) acc[i][j][r] = 0.0f;
-  for (int k0 = 0; k0 < K; k0 += GK) {
-    // 64 x 16 elements of each operand, 8 per thread
-#pragma unroll
-    for (int e = 0; e < 8; e++) {
-      const int idx = t + 128 * e, r = idx >> 4, k = idx & 15;
-      const int gm = m0 + r, gn = n0 + r, gk = k0 + k;
-      const float av = (gm < M && gk < K) ? A[gm * sam + gk * sak] : 0.0f;
-      const float bv = (gn < N && gk < K) ? B[gk * sbk + gn * sbn] : 0.0f;
-      As[r][k] = __float2bfloat16_rn(av);
-      Bs[r][k] = __float2bfloat16_rn(bv);
-    }
-    __syncthreads();
-    uint32_t af[2][4], bf[4][2];
-#pragma unroll
-    for (int i = 0; i < 2; i++) {
-      const int r = wm + 16 * i + g;
-      af[i][0] = pk(As[r][2 * q], As[r][2 * q + 1]);
-      af[i][1] = pk(As[r + 8][2 * q], As[r + 8][2 * q + 1]);
-      af[i][2] = pk(As[r][2 * q + 8], As[r][2 * q + 9]);
-      af[i][3] = pk(As[r + 8][2 * q + 8], As[r + 8][2 * q + 9]);
-    }
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int c = wn + 8 * j + g;
-      bf[j][0] = pk(Bs[c][2 * q], Bs[c][2 * q + 1]);
-      bf[j][1] = pk(Bs[c][2 * q + 8], Bs[c][2 * q + 9]);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; i++)
-#pragma unroll
-      for (int j = 0; j < 4; j++)
-        asm volatile(
-            "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0, %1, %2, %3}, {%4, %5, %6, %7}, {%8, %9}, "
-            "{%0, %1, %2, %3};"
-            : "+f"(acc[i][j][0]), "+f"(acc[i][j][1]), "+f"(acc[i][j][2]), "+f"(acc[i][j][3])
-            : "r"(af[i][0]), "r"(af[i][1]), "r"(af[i][2]), "r"(af[i][3]), "r"(bf[j][0]), "r"(bf[j][1]));
-    __syncthreads();
+__global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const float *__restrict__ A, long long sam,
+                                                 long long sak, const float *__restrict__ B, long long sbk,
+                                                 long long sbn, float *__restrict__ C, int ldc, int accumulate,
+                                                 int cps, float *__restrict__ Cpart, int *__restrict__ err) {
+  extern __shared__ __align__(1024) unsigned char sm[];
+  unsigned char *sa[2] = {sm, sm + TC_A + TC_B};
+  unsigned char *sb[2] = {sm + TC_A, sm + 2 * TC_A + TC_B};
+  uint64_t *bars = reinterpret_cast<uint64_t *>(sm + 2 * (TC_A + TC_B));
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(bars + 2);
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
+  const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+  const int nchunk_all = (K + TK - 1) / TK;
+  const int c_begin = gridDim.z > 1 ? blockIdx.z * cps : 0;
+  const int c_end = gridDim.z > 1 ? min(nchunk_all, c_begin + cps) : nchunk_all;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(mlp::smem_u32(tslot)),
+                 "r"(TN));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  if (t == 0) {
+    for (int i = 0; i < 2; i++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mlp::smem_u32(bars + i)), "r"(1));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  mlp::fence_before();
+  __syncthreads();
+  mlp::fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t idesc = mlp::instr_desc(TM, TN);
+  constexpr uint32_t LBO_A = (TM / 8) * 128, LBO_B = (TN / 8) * 128, SBO = 128;
+  bool ok = true;
+  int issued = 0;  // chunks whose products were issued and committed
+  for (int ch = c_begin; ch < c_end && ok; ch++) {
+    const int st = (ch - c_begin) & 1, use = (ch - c_begin) >> 1;
+    if (use > 0) {  // the products of this stage's previous chunk have read it
+      const bool w = mlp::bar_wait(mlp::smem_u32(bars + st), (uint32_t)((use - 1) & 1));
+      if (!__syncthreads_and(w)) { ok = false; break; }
+    }
+    tc_load_stage(sa[st], sb[st], m0, n0, ch * TK, M, N, K, A, sam, sak, B, sbk, sbn);
+    mlp::fence_async_smem();
+    mlp::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      mlp::fence_after();
+      const uint32_t a = mlp::smem_u32(sa[st]), b = mlp::smem_u32(sb[st]);
 #pragma unroll
-  for (int i = 0; i < 2; i++)
+      for (int kk = 0; kk < TK / 16; kk++)
+        mlp::mma_bf16(tmem, mlp::smem_desc(a + 2 * kk * LBO_A, LBO_A, SBO), mlp::smem_desc(b + 2 * kk * LBO_B, LBO_B, SBO),
+                      idesc, (ch > c_begin || kk > 0) ? 1u : 0u);
+      mlp::mma_commit(mlp::smem_u32(bars + st));
+    }
+    issued++;
+  }
+  const int nch = c_end - c_begin;
+  if (ok && nch > 0) {  // the last commit covers every product issued before it
+    const int st = (nch - 1) & 1, use = (nch - 1) >> 1;
+    ok = __syncthreads_and(mlp::bar_wait(mlp::smem_u32(bars + st), (uint32_t)(use & 1)));
+  }
+  if (!ok) {
+    if (t == 0) atomicOr(err, 4);
+    // a stage may still have products in flight: wait (bounded) for each
+    // stage's last issued commit before the tensor memory is released
+    for (int st = 0; st < 2 && st < issued; st++) {
+      const int last_use = (issued - 1 - st) >> 1;
+      mlp::bar_wait(mlp::smem_u32(bars + st), (uint32_t)(last_use & 1));
+    }
+  } else {
+    mlp::fence_after();
+    const int row = m0 + 32 * warp + lane;
+#pragma unroll 1
+    for (int cb = 0; cb < TN && n0 + cb < N; cb += 32) {
+      float v[32];
+      if (nch > 0) {
+        mlp::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)cb, v);
+      } else {
 #pragma unroll
-    for (int j = 0; j < 4; j++)
+        for (int j = 0; j < 32; j++) v[j] = 0.0f;
+      }
+      if (row < M) {
+        if (gridDim.z > 1) {
+          float *o = Cpart + ((size_t)blockIdx.z * M + row) * N + n0 + cb;
 #pragma unroll
-      for (int r = 0; r < 4; r++) {
-        const int gm = m0 + wm + 16 * i + g + (r >= 2 ? 8 : 0);
-        const int gn = n0 + wn + 8 * j + 2 * q + (r & 1);
-        if (gm < M && gn < N) {
-          float *cp = C + (size_t)gm * ldc + gn;
-          *cp = accumulate ? *cp + acc[i][j][r] : acc[i][j][r];
+          for (int j = 0; j < 32; j++)
+            if (n0 + cb + j < N) o[j] = v[j];
+        } else {
+          float *o = C + (size_t)row * ldc + n0 + cb;
+#pragma unroll
+          for (int j = 0; j < 32; j++)
+            if (n0 + cb + j < N) o[j] = accumulate ? o[j] + v[j] : v[j];
         }
       }
+    }
+  }
+  mlp::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    mlp::fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TN));
+  }
+}
+
+// C[m, n] (+)= sum over splits of Cpart[z][m][n], in split order.
+__global__ void k_splitk_sum(int M, int N, int nsplit, const float *__restrict__ Cpart, float *__restrict__ C,
+                             int ldc, int accumulate) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= M * N) return;
+  float s = 0.0f;
+  for (int z = 0; z < nsplit; z++) s += Cpart[(size_t)z * M * N + i];
+  float *o = C + (size_t)(i / N) * ldc + i % N;
+  *o = accumulate ? *o + s : s;
 }
 
 // Z += b (pre-activation kept), A = BF16(GELU(Z)).

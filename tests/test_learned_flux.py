@@ -103,16 +103,20 @@ def test_tensor_core_inference_with_a_device_row_count():
 GRAD_RTOL = 1e-2  # measured 1.6e-3 at most
 
 
+# 300 rows: one output tile per product and a two-way K split of the weight
+# gradients; 2500 rows: 20 row tiles and a ten-way split (the products run
+# on tcgen05 in 128 x 128 tiles with K in chunks of 64).
 @pytest.mark.gpu
-def test_training_gradient_matches_oracle():
+@pytest.mark.parametrize("rows", [300, 2500])
+def test_training_gradient_matches_oracle(rows):
     """Backward kernels (BF16 tensor-core GEMMs, FP32 accumulation) against
     the oracle's backward pass of the same rounded network: loss to 1e-3,
     each parameter block's gradient to GRAD_RTOL in norm."""
     import fvmhd3d_b200 as F
     rng = np.random.default_rng(11)
     p = M.init_params(7)
-    X = rng.normal(size=(300, M.NIN)).astype(np.float32)
-    T = rng.normal(size=(300, M.NOUT)).astype(np.float32)
+    X = rng.normal(size=(rows, M.NIN)).astype(np.float32)
+    T = rng.normal(size=(rows, M.NOUT)).astype(np.float32)
     wt = np.linspace(0.5, 2.0, M.NOUT)
     s = F.System()
     s.mlp_set_weights(p)

@@ -30,11 +30,12 @@ def _stale(out, srcs):
 
 def build_cuda(force=False):
     out = os.path.join(HERE, "libfvmhd3d_b200.so")
-    srcs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh"))]
+    srcs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cuh", ".h"))]
     srcs.append(os.path.join(HERE, "..", "include", "fvmhd3d_b200.h"))
     if force or _stale(out, srcs):
         _run([NVCC, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-shared",
-              "-diag-suppress", "177", "-o", out, os.path.join(CSRC, "fvm_kernels.cu")])
+              "-diag-suppress", "177", "-o", out, os.path.join(CSRC, "fvm_kernels.cu"),
+              os.path.join(CSRC, "fvm_fused.cu")])
     return out
 
 

@@ -18,6 +18,7 @@
 // face-frame flux maps back to the moving face's flux without approximation.
 //
 // Included by fvm_kernels.cu after fvm_math.cuh and flux_mlp.cuh.
+#pragma once
 
 namespace fvm {
 

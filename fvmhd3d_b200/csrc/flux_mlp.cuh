@@ -11,6 +11,7 @@
 // tile chains share a CTA (one per SM) and its one copy of the weights.
 //
 // Included by fvm_kernels.cu (it uses the context and its error macros).
+#pragma once
 
 #include <cuda_bf16.h>
 
@@ -203,7 +204,7 @@ __device__ __forceinline__ bool group_all(bool v, int g) {
 // up; bit 2: the wait for that group's last commit before the tensor memory
 // is released gave up as well.
 constexpr int THREADS = GROUPS * GTHREADS;
-__global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__restrict__ n_dev,
+static __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__restrict__ n_dev,
                                                       const __nv_bfloat16 *__restrict__ X, float *__restrict__ Y,
                                                       const uint4 *__restrict__ wimg, const float *__restrict__ bias_g,
                                                       int *__restrict__ err) {
@@ -320,7 +321,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__re
   }
 }
 
-__global__ void k_f32_to_bf16(long long n, const float *__restrict__ x, __nv_bfloat16 *__restrict__ y) {
+static __global__ void k_f32_to_bf16(long long n, const float *__restrict__ x, __nv_bfloat16 *__restrict__ y) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) y[i] = __float2bfloat16_rn(x[i]);
 }
@@ -329,7 +330,7 @@ __global__ void k_f32_to_bf16(long long n, const float *__restrict__ x, __nv_bfl
 // -> shared-memory image of the BF16 weights (W4 padded to NOUTP rows with
 // zeros) and the FP32 biases (b4 padded likewise).  W2, W3 and W4 are stored
 // halved: the epilogue hands them twice the GELU.
-__global__ void k_mlp_pack(const float *__restrict__ p, unsigned char *__restrict__ img, float *__restrict__ bias) {
+static __global__ void k_mlp_pack(const float *__restrict__ p, unsigned char *__restrict__ img, float *__restrict__ bias) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const float *W1 = p, *b1 = W1 + NH * NIN, *W2 = b1 + NH, *b2 = W2 + NH * NH, *W3 = b2 + NH, *b3 = W3 + NH * NH,
               *W4 = b3 + NH, *b4 = W4 + NOUT * NH;

@@ -6,6 +6,7 @@
 // they enter a product, as in inference.
 //
 // Included by fvm_kernels.cu.
+#pragma once
 
 namespace mlpt {
 

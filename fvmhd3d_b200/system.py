@@ -272,6 +272,16 @@ class System:
         return {"staged_limiter": int(ch[0]), "face_block": int(ch[1]), "cell_block": int(ch[2]),
                 "cell2_block": int(ch[3])}
 
+    def set_fused(self, max_cells) -> None:
+        """Replayed individual-timestep steps involving at most max_cells
+        cells run as one persistent kernel launch (0: never)."""
+        self._check(self.L.fvm_set_fused(self.h, int(max_cells)), "fvm_set_fused")
+
+    @property
+    def fused_steps(self) -> int:
+        """Steps the persistent rung kernel has run (as of the last run/step)."""
+        return int(self.L.fvm_fused_step_count(self.h))
+
     def set_tuning(self, staged_limiter, face_block, cell_block, cell2_block) -> None:
         """Set the launch choices the autotuner picks (see autotune)."""
         ch = np.array([staged_limiter, face_block, cell_block, cell2_block], np.int32)

@@ -276,6 +276,21 @@ int fvm_get_harvest(fvm_ctx *c, long long n, float *X, float *Y);
  * {staged limiter, face block, cell block, two-thread cell block}. */
 int fvm_autotune(fvm_ctx *c, int shared, int steps, int *choice);
 
+/* Persistent rung kernel: in steps replayed by fvm_run with individual
+ * timesteps, a step whose involved cells (the active ones and their
+ * neighbours) number at most max_cells runs every stage from the slope
+ * limiter to the reconstruction as one cooperative launch with grid-wide
+ * barriers between the stages; larger steps take the stage kernels.  The
+ * choice is made on the device each step; both give the same results.
+ * 0 (the default) turns it off.  Learned-flux mode and per-kernel profiling
+ * always take the stage kernels.  Has no counterpart in the reference (a
+ * GPU batching of its per-rung fluid_update sequence). */
+int fvm_set_fused(fvm_ctx *c, int max_cells);
+
+/* Steps the persistent rung kernel has run since the state was installed
+ * (as of the last fvm_run or fvm_step). */
+long long fvm_fused_step_count(const fvm_ctx *c);
+
 /* Sets the launch choices fvm_autotune picks (same 4 ints: staged limiter
  * 0/1, then block sizes 32, 64 or 128), e.g. to replay a tuned configuration
  * on another run of the same mesh. */

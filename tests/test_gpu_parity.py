@@ -322,10 +322,13 @@ def hilbert_case(nside, problem, seed=1):
     return m, getattr(F.problems, problem)(m.pos)
 
 
-def flat_neighbourhoods(m, U, rel=1e-9):
+def flat_neighbourhoods(m, U, rel=1e-6):
     """(ncell, 10) mask: primitive k of cell c differs from every neighbour's
-    by at most rel times the largest |W_k| over the mesh, i.e. it is flat to
-    round-off around the cell (primitives of the state U)."""
+    by at most rel times the largest |W_k| over the mesh (primitives of the
+    state U).  There the limiter's ratios are formed from differences of at
+    most 1e-6 of the primitive's scale, so round-off of order 1e-16 of the
+    scale moves them by up to 1e-10 relative, and more where the differences
+    are smaller still."""
     V = m.volume[:, None]
     W = np.empty_like(U)
     W[:, 0] = U[:, 0] / V[:, 0]
@@ -358,13 +361,13 @@ def test_blast_128cubed_benchmark_configuration_vs_oracle():
     1e-12 in face-state units.
 
     One documented exception: the time-derivative block of a primitive that
-    is flat to round-off around its cell (psi, Bz and entropy start at zero
-    or constant away from the blast).  Its limiter factor is then set by
-    round-off in the gradient and the neighbour differences (FMA contraction
-    and summation order differ from the reference build), and it multiplies
-    a predicted change that is not round-off (psi grows from the Dedner
-    source).  Those entries are held to 1e-6 and may be at most 1e-4 of the
-    cells."""
+    is flat around its cell to 1e-6 of its scale (psi, Bz and entropy start
+    at zero or constant away from the blast).  Its limiter factor is then set
+    by round-off in the gradient and the neighbour differences (FMA
+    contraction and summation order differ from the reference build), and it
+    multiplies a predicted change that is not round-off (psi grows from the
+    Dedner source).  Those entries are held to 1e-6 and may be at most 1e-4
+    of the cells."""
     m, W = hilbert_case(128, "blast")
     o = oracle_system(m, W)
     for _ in range(2):

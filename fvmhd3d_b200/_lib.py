@@ -66,7 +66,7 @@ SIGNATURES = {
     "fvm_mlp_grad": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "fvm_mlp_train": (c_int, [c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int, c_int, c_float, c_ull,
                               c_void_p]),
-    "fvm_set_flux_mode": (c_int, [c_void_p, c_int, c_float, c_float, c_float, c_int, c_int, c_ll]),
+    "fvm_set_flux_mode": (c_int, [c_void_p, c_int, c_float, c_float, c_float, c_float, c_int, c_int, c_ll]),
     "fvm_mlp_set_norm": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "fvm_learn_stats": (c_int, [c_void_p, c_void_p]),
     "fvm_harvest_count": (c_ll, [c_void_p]),

@@ -41,6 +41,7 @@ struct LearnBuf {
   const double *vol; // cell volumes (positivity gate: magnetic energy)
   const float *norm; // feature and output standardisation: mu_x[16], 1/sd_x[16], mu_y[8], sd_y[8]
   float drho, dp, mach;  // gate: relative density and pressure jumps, normal Mach number
+  float jmax;            // gate: size m of the scaled jump (the network's x[14])
   int surrogate;     // dissipation of gated faces: SUR_NETWORK, SUR_CENTRAL (none) or SUR_LLF
 };
 enum { LSTAT_DEFERRED = 0, LSTAT_FALLBACK, LSTAT_JUDGED, LSTAT_ERR, LSTAT_REF, LSTAT_ERRMAX, LSTAT_POSFALL,
@@ -68,6 +69,25 @@ __device__ __forceinline__ T flux_scale(int k, T rho, T c, T sr) {
   return k == 0 ? rho * c : (k <= 3 ? rho * c * c : (k == 4 ? rho * c * c * c : sr * c * c));
 }
 
+// The seven scaled jumps of a face (density by the mean density, velocities
+// by the larger fast speed c, pressure by rho c^2, tangential fields by
+// sqrt(rho) c) and their size m, which the function returns.
+__device__ __forceinline__ float scaled_jump(const FaceSides &s, float *j) {
+  const float rho = 0.5f * (s.dL + s.dR), c = fmaxf(s.chL, s.chR), sr = sqrtf(rho);
+  const float ic = 1.0f / c, iP = 1.0f / (rho * c * c), iB = 1.0f / (sr * c);
+  j[0] = (s.dR - s.dL) / rho;
+  j[1] = (s.vxR - s.vxL) * ic;
+  j[2] = (s.vyR - s.vyL) * ic;
+  j[3] = (s.vzR - s.vzL) * ic;
+  j[4] = (s.pR - s.pL) * iP;
+  j[5] = (s.ByR - s.ByL) * iB;
+  j[6] = (s.BzR - s.BzL) * iB;
+  float m2 = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 7; k++) m2 = fmaf(j[k], j[k], m2);
+  return sqrtf(m2);
+}
+
 // Features of a face (see the file comment): x[0..6] the side means of the
 // normal velocity in the face frame, the tangential velocities, the pressure
 // and the three field components; x[7..13] the direction of the scaled jump
@@ -85,12 +105,8 @@ __device__ __forceinline__ float face_features(const FaceSides &s, float *x) {
   x[4] = s.Bx * iB;
   x[5] = 0.5f * (s.ByL + s.ByR) * iB;
   x[6] = 0.5f * (s.BzL + s.BzR) * iB;
-  const float j[7] = {(s.dR - s.dL) / rho,   (s.vxR - s.vxL) * ic,  (s.vyR - s.vyL) * ic, (s.vzR - s.vzL) * ic,
-                      (s.pR - s.pL) * iP,     (s.ByR - s.ByL) * iB,  (s.BzR - s.BzL) * iB};
-  float m2 = 0.0f;
-#pragma unroll
-  for (int k = 0; k < 7; k++) m2 = fmaf(j[k], j[k], m2);
-  const float m = sqrtf(m2), im = m > 0.0f ? 1.0f / m : 0.0f;
+  float j[7];
+  const float m = scaled_jump(s, j), im = m > 0.0f ? 1.0f / m : 0.0f;
 #pragma unroll
   for (int k = 0; k < 7; k++) x[7 + k] = j[k] * im;
   x[14] = m;
@@ -199,8 +215,11 @@ __device__ __forceinline__ bool face_gated(const Params &P, const LearnBuf &lb, 
   if (P.eos != 0 || jbnd != NO_BOUNDARY) return false;
   const float rho = 0.5f * (s.dL + s.dR), pm = 0.5f * (s.pL + s.pR), c = fmaxf(s.chL, s.chR);
   const float un = 0.5f * (s.vxL + s.vxR) - s.w;
-  return fabsf(s.dR - s.dL) <= lb.drho * rho && fabsf(s.pR - s.pL) <= lb.dp * pm && fabsf(un) <= lb.mach * c &&
-         s.dL > 0.0f && s.dR > 0.0f && s.pL > 0.0f && s.pR > 0.0f;
+  if (!(fabsf(s.dR - s.dL) <= lb.drho * rho && fabsf(s.pR - s.pL) <= lb.dp * pm && fabsf(un) <= lb.mach * c &&
+        s.dL > 0.0f && s.dR > 0.0f && s.pL > 0.0f && s.pR > 0.0f))
+    return false;
+  float j[7];
+  return scaled_jump(s, j) <= lb.jmax;
 }
 
 template <typename T>

@@ -1852,12 +1852,15 @@ int fvm_mlp_eval(fvm_ctx *c, int n, const float *X, float *Y) {
 
 extern "C" {
 
-int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, int judge, int hstride,
+int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, float jmax, int judge, int hstride,
                       long long hcap) {
   if (!c || mode < 0 || mode > 2 || judge < 0 || hstride < 1 || hcap < 0) return FVM_EINVAL;
   if (!c->have_mesh) { c->err = "fvm_set_flux_mode: no mesh"; return FVM_ENOMESH; }
   if (mode == 1 && !c->mlp_img) { c->err = "fvm_set_flux_mode: no network weights"; return FVM_EINVAL; }
-  if (!(drho >= 0.0f) || !(dp >= 0.0f) || !(mach >= 0.0f)) { c->err = "fvm_set_flux_mode: bad gate"; return FVM_EINVAL; }
+  if (!(drho >= 0.0f) || !(dp >= 0.0f) || !(mach >= 0.0f) || !(jmax >= 0.0f)) {
+    c->err = "fvm_set_flux_mode: bad gate";
+    return FVM_EINVAL;
+  }
   CK(cudaSetDevice(c->device));
   CK(cudaStreamSynchronize(c->st));
   drop_graphs(c);
@@ -1899,6 +1902,7 @@ int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, in
   lb.drho = drho;
   lb.dp = dp;
   lb.mach = mach;
+  lb.jmax = jmax;
   CK(cudaMemsetAsync(lb.stats, 0, LSTAT_COUNT * sizeof(double), c->st));
   CK(cudaMemsetAsync(lb.hcount, 0, sizeof(unsigned long long), c->st));
   CK(cudaMemsetAsync(lb.count, 0, sizeof(int), c->st));

@@ -207,12 +207,13 @@ class System:
         k = {"network": 0, "central": 1, "llf": 2}[kind] if isinstance(kind, str) else int(kind)
         self._check(self.L.fvm_set_flux_surrogate(self.h, k), "fvm_set_flux_surrogate")
 
-    def set_flux_mode(self, mode, drho=0.05, dp=0.05, mach=1.0, judge=1024, hstride=1, hcap=0) -> None:
+    def set_flux_mode(self, mode, drho=0.05, dp=0.05, mach=1.0, jmax=float("inf"), judge=1024, hstride=1,
+                      hcap=0) -> None:
         """Learned-flux mode of the flux passes: 0 exact, 1 network on gated
         faces, 2 exact with harvesting (see fvm_set_flux_mode)."""
         self._check(self.L.fvm_set_flux_mode(self.h, int(mode), ctypes.c_float(drho), ctypes.c_float(dp),
-                                             ctypes.c_float(mach), int(judge), int(hstride), int(hcap)),
-                    "fvm_set_flux_mode")
+                                             ctypes.c_float(mach), ctypes.c_float(jmax), int(judge), int(hstride),
+                                             int(hcap)), "fvm_set_flux_mode")
 
     def mlp_set_norm(self, mu_x, sd_x, mu_y, sd_y) -> None:
         """Standardisation of the network's inputs and outputs."""

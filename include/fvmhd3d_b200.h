@@ -235,13 +235,15 @@ int fvm_mlp_train(fvm_ctx *c, long long n, const float *X, const float *T, const
  * sampled) appends its (features, targets) to a device harvest buffer of
  * hcap rows.  Gate: ideal-gas EOS, no boundary neighbour, relative density
  * and pressure jumps at most drho and dp, normal Mach number in the face
- * frame at most mach.  In mode 1 a face falls back to the exact solver when
+ * frame at most mach, and the size of the face's scaled jump (density by
+ * the mean density, velocities by the larger fast speed c, pressure by
+ * rho c^2, tangential fields by sqrt(rho) c) at most jmax.  In mode 1 a face falls back to the exact solver when
  * the state either of its cells reaches from that face's network flux alone,
  * over the cell's step, keeps less than half of the cell's mass or thermal
  * energy (positivity of the updated state); one deferred face in `judge`
  * (0: none) is also solved exactly to record the network's error.  Resets
  * the statistics. */
-int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, int judge, int hstride,
+int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, float jmax, int judge, int hstride,
                       long long hcap);
 
 /* What stands in for the HLLD dissipation on the faces the gate passes, in

@@ -35,27 +35,61 @@ constexpr int TM = 128, TN = 128, TK = 64;
 constexpr int TC_A = TM * TK * 2, TC_B = TN * TK * 2;  // bytes of one stage's operand tiles
 constexpr int TC_SMEM = 2 * (TC_A + TC_B) + 32;          // two stages, two mbarriers, tensor-memory slot
 
+// One operand tile (rows x TK, `rows` = TM or TN) of chunk k0 into shared
+// memory: element (r, k) = P[(base + r) * s_row + (k0 + k) * s_k], rounded to
+// BF16, zero outside rows < nrows and k < K.  The index order follows the
+// operand's unit stride, and where that stride is 1 and every run of four
+// starts on a 16-byte boundary the loads are float4: along K four elements
+// go out as one 8-byte store of two BF16 pairs (they are adjacent in a core
+// matrix row), along the rows as four 2-byte stores.
+template <int ROWS>
+__device__ __forceinline__ void tc_load_operand(unsigned char *sdst, int base, int nrows, int k0, int K,
+                                                const float *__restrict__ P, long long s_row, long long s_k) {
+  const int t = threadIdx.x;
+  const bool kvec = s_k == 1 && (s_row & 3) == 0 && (K & 3) == 0 && (reinterpret_cast<uintptr_t>(P) & 15) == 0;
+  const bool rvec = s_row == 1 && (s_k & 3) == 0 && (nrows & 3) == 0 && (base & 3) == 0 &&
+                    (reinterpret_cast<uintptr_t>(P) & 15) == 0;
+  if (kvec) {
+#pragma unroll 4
+    for (int e = t; e < ROWS * TK / 4; e += 128) {
+      const int r = e / (TK / 4), k = (e % (TK / 4)) * 4;
+      const int gr = base + r, gk = k0 + k;
+      float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (gr < nrows && gk < K) v = *reinterpret_cast<const float4 *>(P + gr * s_row + gk);
+      uint2 w;
+      w.x = mlp::pack_bf16(v.x, v.y);
+      w.y = mlp::pack_bf16(v.z, v.w);
+      *reinterpret_cast<uint2 *>(sdst + mlp::kmajor_off(r, k, ROWS)) = w;
+    }
+  } else if (rvec) {
+#pragma unroll 4
+    for (int e = t; e < ROWS * TK / 4; e += 128) {
+      const int r = (e % (ROWS / 4)) * 4, k = e / (ROWS / 4);
+      const int gr = base + r, gk = k0 + k;
+      float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (gr < nrows && gk < K) v = *reinterpret_cast<const float4 *>(P + gr + gk * s_k);
+      const float vv[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int q = 0; q < 4; q++)
+        *reinterpret_cast<__nv_bfloat16 *>(sdst + mlp::kmajor_off(r + q, k, ROWS)) = __float2bfloat16_rn(vv[q]);
+    }
+  } else {
+#pragma unroll 4
+    for (int e = t; e < ROWS * TK; e += 128) {
+      const int r = s_k == 1 ? e / TK : e % ROWS, k = s_k == 1 ? e % TK : e / ROWS;
+      const int gr = base + r, gk = k0 + k;
+      const float v = (gr < nrows && gk < K) ? P[gr * s_row + gk * s_k] : 0.0f;
+      *reinterpret_cast<__nv_bfloat16 *>(sdst + mlp::kmajor_off(r, k, ROWS)) = __float2bfloat16_rn(v);
+    }
+  }
+}
+
 __device__ __forceinline__ void tc_load_stage(unsigned char *sa, unsigned char *sb, int m0, int n0, int k0, int M,
                                               int N, int K, const float *__restrict__ A, long long sam,
                                               long long sak, const float *__restrict__ B, long long sbk,
                                               long long sbn) {
-  const int t = threadIdx.x;
-  // the index order follows the operand's unit stride, so warps read runs
-  // of consecutive floats
-#pragma unroll 4
-  for (int e = t; e < TM * TK; e += 128) {
-    const int r = sak == 1 ? e / TK : e % TM, k = sak == 1 ? e % TK : e / TM;
-    const int gm = m0 + r, gk = k0 + k;
-    const float v = (gm < M && gk < K) ? A[gm * sam + gk * sak] : 0.0f;
-    *reinterpret_cast<__nv_bfloat16 *>(sa + mlp::kmajor_off(r, k, TM)) = __float2bfloat16_rn(v);
-  }
-#pragma unroll 4
-  for (int e = t; e < TN * TK; e += 128) {
-    const int r = sbk == 1 ? e / TK : e % TN, k = sbk == 1 ? e % TK : e / TN;
-    const int gn = n0 + r, gk = k0 + k;
-    const float v = (gn < N && gk < K) ? B[gk * sbk + gn * sbn] : 0.0f;
-    *reinterpret_cast<__nv_bfloat16 *>(sb + mlp::kmajor_off(r, k, TN)) = __float2bfloat16_rn(v);
-  }
+  tc_load_operand<TM>(sa, m0, M, k0, K, A, sam, sak);  // A(m, k) = A[m sam + k sak]
+  tc_load_operand<TN>(sb, n0, N, k0, K, B, sbn, sbk);  // B(k, n) = B[k sbk + n sbn], as rows n
 }
 
 __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const float *__restrict__ A, long long sam,

@@ -281,11 +281,24 @@ def main():
     ap.add_argument("--evaluate", action="store_true")
     ap.add_argument("--weights", default=None, help="evaluate these parameters instead of training")
     ap.add_argument("--profile-rows", type=int, default=0, help="only run the network on N random rows")
+    ap.add_argument("--profile-train-steps", type=int, default=0,
+                    help="only run N training steps (batch 8192) on random pairs (for ncu)")
     ap.add_argument("--eval-nside", type=int, default=128, help="blast lattice size of --evaluate")
     ap.add_argument("--eval-steps", type=int, default=100, help="global steps of --evaluate")
     ap.add_argument("--eval-order", default="hilbert", choices=["hilbert", "native"],
                     help="cell order of the --evaluate mesh")
     args = ap.parse_args()
+    if args.profile_train_steps:
+        s = System()
+        s.mlp_set_weights(init_params(1))
+        rng = np.random.default_rng(0)
+        X = rng.normal(size=(200000, NIN)).astype(np.float32)
+        T = rng.normal(size=(200000, NOUT)).astype(np.float32)
+        t = time.perf_counter()
+        hist = s.mlp_train(X, T, batch=8192, steps=args.profile_train_steps, lr=1e-3, seed=1)
+        print(json.dumps({"train_steps": args.profile_train_steps, "wall_s": time.perf_counter() - t,
+                          "last_loss": float(hist[-1])}))
+        return
     if args.profile_rows:
         s = System()
         s.mlp_set_weights(init_params(1))

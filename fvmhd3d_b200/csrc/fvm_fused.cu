@@ -29,7 +29,8 @@ __device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
   return v;
 }
 
-// Grid-wide barrier over all blocks of the launch.  bar[0] counts arrivals
+// Grid-wide barrier over the nblocks working blocks of the launch (the
+// first nblocks; the others have returned).  bar[0] counts arrivals
 // (zero between barriers), bar[1] is the generation, which carries over from
 // launch to launch: each block reads it on entry, and no barrier can complete
 // before every block has arrived, so every block starts from the same value.
@@ -37,13 +38,13 @@ __device__ __forceinline__ unsigned load_acquire(const unsigned *p) {
 // bounded polls, for the generation its barrier completes; the last arrival
 // resets the count and publishes the generation.  Returns false on every
 // thread of the block if the wait gave up (err bit 1 set).
-__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &gen, int *err) {
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned &gen, int *err, unsigned nblocks) {
   __syncthreads();
   int ok = 1;
   if (threadIdx.x == 0) {
     const unsigned target = gen + 1;
     __threadfence();
-    if (atomicAdd(&bar[0], 1u) == gridDim.x - 1) {
+    if (atomicAdd(&bar[0], 1u) == nblocks - 1) {
       atomicExch(&bar[0], 0u);
       __threadfence();
       atomicExch(&bar[1], target);
@@ -102,10 +103,15 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   const Dev &d = a.d;
   Sched *S = d.S;
   const int n = a.n, nf = a.nf;
-  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+  // Every block works: the stages of a small step are bound by the latency
+  // of each thread's walk over its cell's faces, so more threads beat
+  // cheaper barriers (one block per 64 involved cells measured 0.20 ms per
+  // 200-cell step against 0.15 ms with the whole grid).
+  const unsigned nwork = gridDim.x;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = (int)nwork * blockDim.x;
   unsigned gen = load_acquire(&a.gbar[1]);
 #define FVM_GRID_SYNC() \
-  if (!grid_barrier(a.gbar, gen, a.gerr)) return
+  if (!grid_barrier(a.gbar, gen, a.gerr, nwork)) return
   // the work arrays of adjust_timesteps start cleared for the step's
   // involved cells (the separate-kernel step clears them for every cell).
   // Every entry this step writes or reads is an involved cell's: marks and

@@ -687,7 +687,7 @@ def learned_leg(F, m, W, steps, weights, stream_of):
                       "judged_faces": stats["judged"],
                       "judged_mean_abs_scaled": stats["judged_mean_abs"],
                       "judged_max_abs_scaled": stats["judged_max_abs"],
-                      "dtype": "f32 bulk + bf16 network", "weights": "fvmhd3d_b200/data/flux_mlp.npz"})
+                      "dtype": "f32 bulk + f16 network", "weights": "fvmhd3d_b200/data/flux_mlp.npz"})
             out.update(r)
         else:
             out[f"gated_faces_{sur}"] = r

@@ -27,7 +27,7 @@ namespace fvm {
 // pressure jumps, bounded normal Mach number in the face frame, and every
 // standardised network input within ZMAX spreads of its training mean.
 struct LearnBuf {
-  __nv_bfloat16 *X;  // [cap x 16] features of deferred faces
+  __half *X;  // [cap x 16] features of deferred faces (FP16, the network's input type)
   float *Y;          // [cap x 8] network outputs
   int *gface;        // [cap] face of each deferred slot
   int *count;        // deferred faces of the current pass
@@ -277,10 +277,10 @@ struct DeferSolver {
     if (face_gated(P, lb, s, jbnd) && net_inputs(lb, s, x)) {
       const int slot = atomicAdd(lb.count, 1);
       uint4 *o = reinterpret_cast<uint4 *>(lb.X + 16 * (size_t)slot);
-      o[0] = make_uint4(mlp::pack_bf16(x[0], x[1]), mlp::pack_bf16(x[2], x[3]), mlp::pack_bf16(x[4], x[5]),
-                        mlp::pack_bf16(x[6], x[7]));
-      o[1] = make_uint4(mlp::pack_bf16(x[8], x[9]), mlp::pack_bf16(x[10], x[11]), mlp::pack_bf16(x[12], x[13]),
-                        mlp::pack_bf16(x[14], x[15]));
+      o[0] = make_uint4(mlp::pack_f16(x[0], x[1]), mlp::pack_f16(x[2], x[3]), mlp::pack_f16(x[4], x[5]),
+                        mlp::pack_f16(x[6], x[7]));
+      o[1] = make_uint4(mlp::pack_f16(x[8], x[9]), mlp::pack_f16(x[10], x[11]), mlp::pack_f16(x[12], x[13]),
+                        mlp::pack_f16(x[14], x[15]));
       lb.gface[slot] = f;
       deferred = true;
       return false;

@@ -2,18 +2,23 @@
 // in for riemann_solver (MPI/compute_update.cpp:1109-1341) on smooth faces.
 //
 // Inference runs on the 5th-generation tensor cores: one CTA takes tiles of
-// 128 faces; the weights sit in shared memory as BF16 in the K-major
+// 128 faces; the weights sit in shared memory as FP16 in the K-major
 // no-swizzle core-matrix layout the tcgen05 shared-memory descriptors
-// describe; one elected thread issues tcgen05.mma (kind::f16, BF16 inputs,
-// FP32 accumulation in tensor memory); after each layer eight warps read the
-// accumulator back with tcgen05.ld (32 rows x 64 columns each), add the bias,
-// apply GELU, round to BF16 and write the next layer's A operand.  Four such
-// tile chains share a CTA (one per SM) and its one copy of the weights.
+// describe; one elected thread issues tcgen05.mma (kind::f16, FP16 inputs,
+// FP32 accumulation in tensor memory); each layer's bias enters the
+// accumulator through one more product (a constant ONES operand times the
+// bias split into two FP16 parts), so after each layer eight warps read the
+// accumulator back with tcgen05.ld (32 rows x 64 columns each), apply GELU in
+// packed half-precision pairs (one tanh.approx.f16x2 for two values) and
+// write the next layer's FP16 A operand.  Four such tile chains
+// share a CTA (one per SM) and its one copy of the weights.  The training
+// products (mlp_train.cuh) keep BF16 operands.
 //
 // Included by fvm_kernels.cu (it uses the context and its error macros).
 #pragma once
 
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 namespace mlp {
 
@@ -22,24 +27,34 @@ constexpr int NPARAM = NH * NIN + NH + NH * NH + NH + NH * NH + NH + NOUT * NH +
 static_assert(NPARAM == 36232, "parameter count");
 
 // byte offsets of the shared-memory image (each region 1024-byte aligned)
+constexpr int KB = 16;                             // K of one tcgen05.mma of kind::f16
 constexpr int OFF_W1 = 0;                          // [NH x NIN]   4096 B
 constexpr int OFF_W2 = OFF_W1 + NH * NIN * 2;      // [NH x NH]   32768 B
 constexpr int OFF_W3 = OFF_W2 + NH * NH * 2;       // [NH x NH]   32768 B
 constexpr int OFF_W4 = OFF_W3 + NH * NH * 2;       // [NOUTP x NH] 4096 B
-constexpr int IMG_BYTES = OFF_W4 + NOUTP * NH * 2;  // weights image copied from global
+// Bias operands: layer L's bias is the product ONES [TILE x KB] x BL^T
+// [KB x N], with columns 0 and 1 of ONES equal to 1 and of BL equal to the
+// high and low FP16 parts of the bias (every other entry 0).
+constexpr int OFF_B1 = OFF_W4 + NOUTP * NH * 2;    // [NH x KB]    4096 B
+constexpr int OFF_B2 = OFF_B1 + NH * KB * 2;       // [NH x KB]    4096 B
+constexpr int OFF_B3 = OFF_B2 + NH * KB * 2;       // [NH x KB]    4096 B
+constexpr int OFF_ONES = OFF_B3 + NH * KB * 2;     // [TILE x KB]  4096 B
+constexpr int OFF_B4 = OFF_ONES + TILE * KB * 2;   // [NOUTP x KB]  512 B
+constexpr int IMG_BYTES = OFF_B4 + NOUTP * KB * 2;  // weights image copied from global
 // GROUPS independent tile chains per CTA, each with its own activations
 // buffer, mbarrier and 128 tensor-memory columns; they share the weights.
 constexpr int GROUPS = 4, GTHREADS = 256;
 constexpr int A_BYTES = TILE * NH * 2;             // [TILE x NH]  32768 B activations of one group
-constexpr int OFF_A = IMG_BYTES;                   // GROUPS activations buffers
-constexpr int OFF_BIAS = OFF_A + GROUPS * A_BYTES; // f32 b1, b2, b3 (3 x NH), b4 (NOUTP)
-constexpr int NBIAS = 3 * NH + NOUTP;
-constexpr int OFF_BAR = OFF_BIAS + NBIAS * 4;      // GROUPS mbarriers (8 B each), tensor-memory address (4 B)
+constexpr int OFF_A = (IMG_BYTES + 1023) / 1024 * 1024;  // GROUPS activations buffers
+constexpr int OFF_BAR = OFF_A + GROUPS * A_BYTES;  // GROUPS mbarriers (8 B each), tensor-memory address (4 B)
 constexpr int SMEM_BYTES = OFF_BAR + GROUPS * 8 + 8;
 constexpr int TMEM_COLS = GROUPS * NH;             // 512: the whole tensor memory, one CTA per SM
 static_assert(SMEM_BYTES <= 227 * 1024, "shared memory");
 static_assert(OFF_BAR % 8 == 0, "mbarrier alignment");
-static_assert(OFF_W2 % 1024 == 0 && OFF_W3 % 1024 == 0 && OFF_W4 % 1024 == 0 && OFF_A % 1024 == 0, "align");
+static_assert(OFF_W2 % 1024 == 0 && OFF_W3 % 1024 == 0 && OFF_W4 % 1024 == 0 && OFF_B1 % 1024 == 0 &&
+                  OFF_B2 % 1024 == 0 && OFF_B3 % 1024 == 0 && OFF_ONES % 1024 == 0 && OFF_B4 % 1024 == 0 &&
+                  OFF_A % 1024 == 0 && IMG_BYTES % 16 == 0,
+              "align");
 
 // Element (row, k) of a K-major no-swizzle operand with `rows` rows: core
 // matrices of 8 rows x 16 bytes, 8-row groups 128 B apart (stride byte
@@ -57,12 +72,16 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
 __host__ __device__ constexpr uint32_t instr_desc(int M, int N) {
   return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
+// The same with FP16 A and B (A and B always share one type).
+__host__ __device__ constexpr uint32_t instr_desc_f16(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
 }
 
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+__device__ __forceinline__ void mma_f16kind(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                          uint32_t accumulate) {
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
@@ -135,27 +154,39 @@ __device__ __forceinline__ float gelu(float x) {
   return 0.5f * x * (1.0f + tanh_hw(u));
 }
 
-// Twice the GELU, x (1 + tanh(u)) with u = sqrt(2/pi) x (1 + 0.044715 x^2),
-// in four FP32 operations and one tanh.  The inference epilogue stores it and
-// the image of the next layer's weights carries the factor 1/2 (an exact
-// power-of-two scaling of the BF16 weights), so the layer's products are those
-// of gelu(x) and W.
-__device__ __forceinline__ float gelu2(float x) {
-  const float u = x * fmaf(x * x, 0.7978845608028654f * 0.044715f, 0.7978845608028654f);
-  return fmaf(x, tanh_hw(u), x);
+// Twice the GELU of two values, x (1 + tanh(u)) with
+// u = sqrt(2/pi) x (1 + 0.044715 x^2), in packed half precision: the FP32
+// sums a, b are rounded to an FP16 pair, and u, tanh and the result take one
+// instruction each for both values (the pair's tanh still takes two slots of
+// the XU pipe, as two FP32 tanh would).  The inference epilogue stores it and the
+// image of the next layer's weights carries the factor 1/2 (an exact
+// power-of-two scaling of the FP16 weights), so the layer's products are
+// those of gelu(x) and W.  Past |x| = 256 the square overflows to infinity,
+// tanh(u) to +-1 and the result to 2x or 0, the GELU's own limits.
+__device__ __forceinline__ uint32_t gelu2_h2(float a, float b) {
+  const __half2 x = __floats2half2_rn(a, b);
+  const __half2 c0 = __float2half2_rn(0.7978845608028654f), c1 = __float2half2_rn(0.7978845608028654f * 0.044715f);
+  const __half2 u = __hmul2(x, __hfma2(__hmul2(x, x), c1, c0));
+  uint32_t t;
+  asm("tanh.approx.f16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t *>(&u)));
+  const __half2 y = __hfma2(x, *reinterpret_cast<const __half2 *>(&t), x);
+  return *reinterpret_cast<const uint32_t *>(&y);
 }
 
 __device__ __forceinline__ uint32_t pack_bf16(float a, float b) {
   const __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
   return *reinterpret_cast<const uint32_t *>(&h);
 }
+__device__ __forceinline__ uint32_t pack_f16(float a, float b) {
+  const __half2 h = __floats2half2_rn(a, b);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
 
 // Hidden-layer epilogue of one group: warp w (0..7 within the group) takes
 // rows 32 (w % 4) .. +31 (its tensor-memory lane quarter q) and columns
-// 64 (w / 4) .. +63 (half h) of the group's accumulator, 32 at a time; bias,
-// twice the GELU, BF16, into the group's A operand.
-__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, const float *bias, unsigned char *A, int q, int h,
-                                                int lane) {
+// 64 (w / 4) .. +63 (half h) of the group's accumulator (bias included), 32
+// at a time; twice the GELU (FP16 pairs), into the group's A operand.
+__device__ __forceinline__ void epilogue_hidden(uint32_t tmem, unsigned char *A, int q, int h, int lane) {
   const int r = 32 * q + lane;
 #pragma unroll 1
   for (int c = 2 * h; c < 2 * h + 2; c++) {
@@ -163,15 +194,12 @@ __device__ __forceinline__ void epilogue_hidden(uint32_t tmem, const float *bias
     tmem_ld32(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(32 * c), v);
 #pragma unroll
     for (int j = 0; j < 4; j++) {
-      const int k = 32 * c + 8 * j;
-      const float4 b0 = *reinterpret_cast<const float4 *>(bias + k);
-      const float4 b1 = *reinterpret_cast<const float4 *>(bias + k + 4);
       uint4 w;
-      w.x = pack_bf16(gelu2(v[8 * j + 0] + b0.x), gelu2(v[8 * j + 1] + b0.y));
-      w.y = pack_bf16(gelu2(v[8 * j + 2] + b0.z), gelu2(v[8 * j + 3] + b0.w));
-      w.z = pack_bf16(gelu2(v[8 * j + 4] + b1.x), gelu2(v[8 * j + 5] + b1.y));
-      w.w = pack_bf16(gelu2(v[8 * j + 6] + b1.z), gelu2(v[8 * j + 7] + b1.w));
-      *reinterpret_cast<uint4 *>(A + kmajor_off(r, k, TILE)) = w;
+      w.x = gelu2_h2(v[8 * j + 0], v[8 * j + 1]);
+      w.y = gelu2_h2(v[8 * j + 2], v[8 * j + 3]);
+      w.z = gelu2_h2(v[8 * j + 4], v[8 * j + 5]);
+      w.w = gelu2_h2(v[8 * j + 6], v[8 * j + 7]);
+      *reinterpret_cast<uint4 *>(A + kmajor_off(r, 32 * c + 8 * j, TILE)) = w;
     }
   }
 }
@@ -194,30 +222,29 @@ __device__ __forceinline__ bool group_all(bool v, int g) {
   return r != 0;
 }
 
-// Y[n x 8] = MLP(X[n x 16]) (n read from n_dev when given); X in BF16, Y in
+// Y[n x 8] = MLP(X[n x 16]) (n read from n_dev when given); X in FP16, Y in
 // FP32.  One CTA per SM (the shared memory holds one copy of the weights and
 // four activations buffers); its four groups of eight warps run independent
 // 128-row tiles, so one group's epilogue overlaps another's matrix products.
 // The first four warps of a group load the inputs and write the outputs (warp
 // q: rows 32 q .. +31); thread 0 of the group issues the group's tcgen05.mma
-// and commits them to the group's mbarrier.  err bit 1: an mbarrier wait gave
-// up; bit 2: the wait for that group's last commit before the tensor memory
-// is released gave up as well.
+// and commits them to the group's mbarrier, on which the group's first warp
+// waits while the other seven sleep in the group's named barrier (no polling
+// that would take issue slots from the other groups' epilogues).  err bit 1:
+// an mbarrier wait gave up; bit 2: the wait for that group's last commit
+// before the tensor memory is released gave up as well.
 constexpr int THREADS = GROUPS * GTHREADS;
 static __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const int *__restrict__ n_dev,
-                                                      const __nv_bfloat16 *__restrict__ X, float *__restrict__ Y,
-                                                      const uint4 *__restrict__ wimg, const float *__restrict__ bias_g,
-                                                      int *__restrict__ err) {
+                                                      const __half *__restrict__ X, float *__restrict__ Y,
+                                                      const uint4 *__restrict__ wimg, int *__restrict__ err) {
   extern __shared__ __align__(1024) unsigned char sm[];
   if (n_dev) n = *n_dev;  // row count produced on the device
   const int t = threadIdx.x, warp = t >> 5, g = warp >> 3, q = warp & 3, hq = (warp >> 2) & 1,
             gt = t & (GTHREADS - 1);
   uint64_t *bars = reinterpret_cast<uint64_t *>(sm + OFF_BAR);
   uint32_t *tslot = reinterpret_cast<uint32_t *>(sm + OFF_BAR + GROUPS * 8);
-  float *bias = reinterpret_cast<float *>(sm + OFF_BIAS);
   unsigned char *A = sm + OFF_A + g * A_BYTES;
   for (int i = t; i < IMG_BYTES / 16; i += blockDim.x) reinterpret_cast<uint4 *>(sm)[i] = wimg[i];
-  for (int i = t; i < NBIAS; i += blockDim.x) bias[i] = bias_g[i];
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                  "r"(TMEM_COLS));
@@ -235,13 +262,14 @@ static __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const in
   const uint32_t bar_a = smem_u32(bars + g);
   const uint32_t a_addr = smem_u32(A);
   const uint32_t w_addr = smem_u32(sm);
-  const uint32_t id_h = instr_desc(TILE, NH), id_o = instr_desc(TILE, NOUTP);
+  const uint32_t id_h = instr_desc_f16(TILE, NH), id_o = instr_desc_f16(TILE, NOUTP);
   const uint32_t LBO_128 = (128 / 8) * 128, LBO_OUT = (NOUTP / 8) * 128, SBO = 128;
+  const uint64_t ones_desc = smem_desc(w_addr + OFF_ONES, LBO_128, SBO);
   uint32_t parity = 0;
   bool ok = true;
   const int ntiles = (n + TILE - 1) / TILE;
   const int stride = gridDim.x * GROUPS;
-  // layer-1 input: thread gt of the group holds row gt of X (16 BF16, two
+  // layer-1 input: thread gt of the group holds row gt of X (16 FP16, two
   // 16-byte halves); the next tile's row is loaded while this tile's layers run
   auto load_x = [&](int tile, uint4 &x0, uint4 &x1) {
     x0 = x1 = make_uint4(0, 0, 0, 0);
@@ -272,19 +300,22 @@ static __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const in
       group_sync(g);
       if (gt == 0) {
         fence_after();
+        const uint32_t lbo_b = L == 3 ? LBO_OUT : LBO_128, idesc = L == 3 ? id_o : id_h;
+        // the bias first (it initialises the accumulator), then the weights
+        const uint32_t bb = w_addr + (L == 0 ? OFF_B1 : L == 1 ? OFF_B2 : L == 2 ? OFF_B3 : OFF_B4);
+        mma_f16kind(tmem, ones_desc, smem_desc(bb, lbo_b, SBO), idesc, 0);
         if (L == 0) {
-          mma_bf16(tmem, smem_desc(a_addr, LBO_128, SBO), smem_desc(w_addr + OFF_W1, LBO_128, SBO), id_h, 0);
+          mma_f16kind(tmem, smem_desc(a_addr, LBO_128, SBO), smem_desc(w_addr + OFF_W1, LBO_128, SBO), id_h, 1);
         } else {
           const uint32_t wb = w_addr + (L == 1 ? OFF_W2 : L == 2 ? OFF_W3 : OFF_W4);
-          const uint32_t lbo_b = L == 3 ? LBO_OUT : LBO_128;
 #pragma unroll 1
-          for (int kk = 0; kk < NH / 16; kk++)
-            mma_bf16(tmem, smem_desc(a_addr + 2 * kk * LBO_128, LBO_128, SBO),
-                     smem_desc(wb + 2 * kk * lbo_b, lbo_b, SBO), L == 3 ? id_o : id_h, kk > 0 ? 1u : 0u);
+          for (int kk = 0; kk < NH / KB; kk++)
+            mma_f16kind(tmem, smem_desc(a_addr + 2 * kk * LBO_128, LBO_128, SBO),
+                        smem_desc(wb + 2 * kk * lbo_b, lbo_b, SBO), idesc, 1);
         }
         mma_commit(bar_a);
       }
-      const bool waited = bar_wait(bar_a, parity);
+      const bool waited = gt < 32 ? bar_wait(bar_a, parity) : true;
       if (!group_all(waited, g)) {  // the group leaves together
         if (gt == 0) atomicOr(err, 1);
         ok = false;
@@ -293,16 +324,15 @@ static __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const in
       parity ^= 1;
       fence_after();
       if (L < 3) {
-        epilogue_hidden(tmem, bias + NH * L, A, q, hq, t & 31);
+        epilogue_hidden(tmem, A, q, hq, t & 31);
       } else if (gt < TILE) {
         float v[8];
         tmem_ld8(tmem + ((uint32_t)(32 * q) << 16), v);
         const int row = tile * TILE + gt;
         if (row < n) {
           float4 *yo = reinterpret_cast<float4 *>(Y + (size_t)row * NOUT);
-          const float *b4 = bias + 3 * NH;
-          yo[0] = make_float4(v[0] + b4[0], v[1] + b4[1], v[2] + b4[2], v[3] + b4[3]);
-          yo[1] = make_float4(v[4] + b4[4], v[5] + b4[5], v[6] + b4[6], v[7] + b4[7]);
+          yo[0] = make_float4(v[0], v[1], v[2], v[3]);
+          yo[1] = make_float4(v[4], v[5], v[6], v[7]);
         }
       }
     }
@@ -321,39 +351,49 @@ static __global__ void __launch_bounds__(THREADS, 1) k_mlp_infer(int n, const in
   }
 }
 
-static __global__ void k_f32_to_bf16(long long n, const float *__restrict__ x, __nv_bfloat16 *__restrict__ y) {
+static __global__ void k_f32_to_f16(long long n, const float *__restrict__ x, __half *__restrict__ y) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) y[i] = __float2bfloat16_rn(x[i]);
+  if (i < n) y[i] = __float2half_rn(x[i]);
 }
 
 // Parameters (W1[NH x NIN], b1, W2[NH x NH], b2, W3, b3, W4[NOUT x NH], b4)
-// -> shared-memory image of the BF16 weights (W4 padded to NOUTP rows with
-// zeros) and the FP32 biases (b4 padded likewise).  W2, W3 and W4 are stored
-// halved: the epilogue hands them twice the GELU.
-static __global__ void k_mlp_pack(const float *__restrict__ p, unsigned char *__restrict__ img, float *__restrict__ bias) {
+// -> shared-memory image: the FP16 weights (W4 padded to NOUTP rows with
+// zeros), the bias operands (each bias as the FP16 pair hi = fp16(b),
+// lo = fp16(b - hi), b4 padded with zeros) and the ONES operand.  W2, W3 and
+// W4 are stored halved: the epilogue hands them twice the GELU.
+static __global__ void k_mlp_pack(const float *__restrict__ p, unsigned char *__restrict__ img) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const float *W1 = p, *b1 = W1 + NH * NIN, *W2 = b1 + NH, *b2 = W2 + NH * NH, *W3 = b2 + NH, *b3 = W3 + NH * NH,
               *W4 = b3 + NH, *b4 = W4 + NOUT * NH;
   if (i < NH * NIN) {
     const int r = i / NIN, k = i % NIN;
-    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W1 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(W1[i]);
+    *reinterpret_cast<__half *>(img + OFF_W1 + kmajor_off(r, k, NH)) = __float2half_rn(W1[i]);
   }
   if (i < NH * NH) {
     const int r = i / NH, k = i % NH;
-    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W2 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(0.5f * W2[i]);
-    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W3 + kmajor_off(r, k, NH)) = __float2bfloat16_rn(0.5f * W3[i]);
+    *reinterpret_cast<__half *>(img + OFF_W2 + kmajor_off(r, k, NH)) = __float2half_rn(0.5f * W2[i]);
+    *reinterpret_cast<__half *>(img + OFF_W3 + kmajor_off(r, k, NH)) = __float2half_rn(0.5f * W3[i]);
   }
   if (i < NOUTP * NH) {
     const int r = i / NH, k = i % NH;
-    *reinterpret_cast<__nv_bfloat16 *>(img + OFF_W4 + kmajor_off(r, k, NOUTP)) =
-        __float2bfloat16_rn(r < NOUT ? 0.5f * W4[r * NH + k] : 0.0f);
+    *reinterpret_cast<__half *>(img + OFF_W4 + kmajor_off(r, k, NOUTP)) =
+        __float2half_rn(r < NOUT ? 0.5f * W4[r * NH + k] : 0.0f);
   }
-  if (i < NH) {
-    bias[i] = b1[i];
-    bias[NH + i] = b2[i];
-    bias[2 * NH + i] = b3[i];
+  auto bias_entry = [](float b, int k) {
+    const __half hi = __float2half_rn(b);
+    return k == 0 ? hi : k == 1 ? __float2half_rn(b - __half2float(hi)) : __float2half_rn(0.0f);
+  };
+  if (i < NH * KB) {
+    const int r = i / KB, k = i % KB;
+    *reinterpret_cast<__half *>(img + OFF_B1 + kmajor_off(r, k, NH)) = bias_entry(b1[r], k);
+    *reinterpret_cast<__half *>(img + OFF_B2 + kmajor_off(r, k, NH)) = bias_entry(b2[r], k);
+    *reinterpret_cast<__half *>(img + OFF_B3 + kmajor_off(r, k, NH)) = bias_entry(b3[r], k);
+    *reinterpret_cast<__half *>(img + OFF_ONES + kmajor_off(r, k, TILE)) = __float2half_rn(k < 2 ? 1.0f : 0.0f);
   }
-  if (i < NOUTP) bias[3 * NH + i] = i < NOUT ? b4[i] : 0.0f;
+  if (i < NOUTP * KB) {
+    const int r = i / KB, k = i % KB;
+    *reinterpret_cast<__half *>(img + OFF_B4 + kmajor_off(r, k, NOUTP)) = bias_entry(r < NOUT ? b4[r] : 0.0f, k);
+  }
 }
 
 }  // namespace mlp

@@ -163,9 +163,8 @@ struct fvm_ctx {
   // one captured step per mode (shared / individual), replayed by fvm_run
   cudaGraphExec_t graph[2];
   Sched hS;  // host copy of the device scheduler, refreshed after synchronisation
-  // learned flux network: BF16 weight image and FP32 biases
+  // learned flux network: image of the FP16 weights and bias operands
   unsigned char *mlp_img = nullptr;
-  float *mlp_bias = nullptr;
   int *mlp_err = nullptr;
   float *mlp_param = nullptr;  // FP32 master parameters
   // learned-flux mode: 0 exact, 1 network on gated faces, 2 exact + harvest
@@ -345,7 +344,6 @@ void fvm_destroy(fvm_ctx *c) {
   drop_graphs(c);
   free_all(c);
   if (c->mlp_img) cudaFree(c->mlp_img);
-  if (c->mlp_bias) cudaFree(c->mlp_bias);
   if (c->mlp_err) cudaFree(c->mlp_err);
   if (c->mlp_param) cudaFree(c->mlp_param);
   for (int k = 0; k < 2 * KT_COUNT; k++) cudaEventDestroy(c->kev[k]);
@@ -743,7 +741,7 @@ static int enq_limiter(fvm_ctx *c) {
   return 0;
 }
 
-static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfloat16 *X, float *Y);
+static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __half *X, float *Y);
 
 static int enq_update(fvm_ctx *c) {
   Dev &d = c->d;
@@ -1566,7 +1564,7 @@ int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const doub
 
 // The network on n rows (or on *n_dev rows, at most nmax, counted on the
 // device): persistent CTAs, one per SM, four 128-row tiles in flight in each.
-static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfloat16 *X, float *Y) {
+static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __half *X, float *Y) {
   if (nmax <= 0) return 0;
   static bool attr_set[kMaxDevices] = {};  // per device, like the attribute itself
   if (c->device < 0 || c->device >= kMaxDevices) { c->err = "device index out of range"; return FVM_EINVAL; }
@@ -1579,12 +1577,12 @@ static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __nv_bfl
   const int nchains = (nmax + mlp::TILE * mlp::GROUPS - 1) / (mlp::TILE * mlp::GROUPS);
   const int grid = nchains < nsm ? nchains : nsm;
   mlp::k_mlp_infer<<<grid, mlp::THREADS, mlp::SMEM_BYTES, c->st>>>(nmax, n_dev, X, Y, (const uint4 *)c->mlp_img,
-                                                          c->mlp_bias, c->mlp_err);
+                                                          c->mlp_err);
   LAUNCH_CHECK();
   return 0;
 }
 
-static int mlp_launch(fvm_ctx *c, int n, const __nv_bfloat16 *X, float *Y) {
+static int mlp_launch(fvm_ctx *c, int n, const __half *X, float *Y) {
   return mlp_launch_dev(c, n, nullptr, X, Y);
 }
 
@@ -1595,13 +1593,12 @@ int fvm_mlp_set_weights(fvm_ctx *c, const float *params) {
   CK(cudaSetDevice(c->device));
   if (!c->mlp_img) {
     CK(cudaMalloc(&c->mlp_img, mlp::IMG_BYTES));
-    CK(cudaMalloc(&c->mlp_bias, mlp::NBIAS * sizeof(float)));
     CK(cudaMalloc(&c->mlp_err, sizeof(int)));
     CK(cudaMalloc(&c->mlp_param, mlp::NPARAM * sizeof(float)));
     CK(cudaMemsetAsync(c->mlp_err, 0, sizeof(int), c->st));
   }
   CK(cudaMemcpyAsync(c->mlp_param, params, mlp::NPARAM * sizeof(float), cudaMemcpyHostToDevice, c->st));
-  mlp::k_mlp_pack<<<(mlp::NH * mlp::NH + 255) / 256, 256, 0, c->st>>>(c->mlp_param, c->mlp_img, c->mlp_bias);
+  mlp::k_mlp_pack<<<(mlp::NH * mlp::NH + 255) / 256, 256, 0, c->st>>>(c->mlp_param, c->mlp_img);
   LAUNCH_CHECK();
   CK(cudaStreamSynchronize(c->st));
   return 0;
@@ -1774,7 +1771,7 @@ int fvm_mlp_train(fvm_ctx *c, long long n, const float *X, const float *T, const
     c->launches += 2;
   }
   CK(cudaGetLastError());
-  mlp::k_mlp_pack<<<(mlp::NH * mlp::NH + 255) / 256, 256, 0, c->st>>>(c->mlp_param, c->mlp_img, c->mlp_bias);
+  mlp::k_mlp_pack<<<(mlp::NH * mlp::NH + 255) / 256, 256, 0, c->st>>>(c->mlp_param, c->mlp_img);
   LAUNCH_CHECK();
   if (loss_out && steps > 0)
     CK(cudaMemcpyAsync(loss_out, hist, (size_t)steps * sizeof(float), cudaMemcpyDeviceToHost, c->st));
@@ -1796,16 +1793,16 @@ int fvm_mlp_eval_counted(fvm_ctx *c, int nmax, int n, const float *X, float *Y) 
   CK(cudaSetDevice(c->device));
   const size_t nx = (size_t)nmax * mlp::NIN, ny = (size_t)nmax * mlp::NOUT;
   float *dx = nullptr, *dy = nullptr;
-  __nv_bfloat16 *db = nullptr;
+  __half *db = nullptr;
   int *dn = nullptr;
   CK(cudaMallocAsync(&dx, nx * sizeof(float), c->st));
-  CK(cudaMallocAsync(&db, nx * sizeof(__nv_bfloat16), c->st));
+  CK(cudaMallocAsync(&db, nx * sizeof(__half), c->st));
   CK(cudaMallocAsync(&dy, ny * sizeof(float), c->st));
   CK(cudaMallocAsync(&dn, sizeof(int), c->st));
   CK(cudaMemcpyAsync(dx, X, nx * sizeof(float), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(dy, Y, ny * sizeof(float), cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(dn, &n, sizeof(int), cudaMemcpyHostToDevice, c->st));
-  mlp::k_f32_to_bf16<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>((long long)nx, dx, db);
+  mlp::k_f32_to_f16<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>((long long)nx, dx, db);
   LAUNCH_CHECK();
   int rc = mlp_launch_dev(c, nmax, dn, db, dy);
   if (rc) return rc;
@@ -1828,12 +1825,12 @@ int fvm_mlp_eval(fvm_ctx *c, int n, const float *X, float *Y) {
   CK(cudaSetDevice(c->device));
   const size_t nx = (size_t)n * mlp::NIN, ny = (size_t)n * mlp::NOUT;
   float *dx = nullptr, *dy = nullptr;
-  __nv_bfloat16 *db = nullptr;
+  __half *db = nullptr;
   CK(cudaMallocAsync(&dx, nx * sizeof(float), c->st));
-  CK(cudaMallocAsync(&db, nx * sizeof(__nv_bfloat16), c->st));
+  CK(cudaMallocAsync(&db, nx * sizeof(__half), c->st));
   CK(cudaMallocAsync(&dy, ny * sizeof(float), c->st));
   CK(cudaMemcpyAsync(dx, X, nx * sizeof(float), cudaMemcpyHostToDevice, c->st));
-  mlp::k_f32_to_bf16<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>((long long)nx, dx, db);
+  mlp::k_f32_to_f16<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>((long long)nx, dx, db);
   LAUNCH_CHECK();
   int rc = mlp_launch(c, n, db, dy);
   if (rc) return rc;
@@ -1868,7 +1865,7 @@ int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, fl
   const size_t nf = (size_t)(c->nf > 0 ? c->nf : 1);
   int rc = 0;
   if (!d.lX) {
-    rc |= dalloc_bytes(c, &d.lX, nf * 16 * sizeof(__nv_bfloat16));
+    rc |= dalloc_bytes(c, &d.lX, nf * 16 * sizeof(__half));
     rc |= dalloc_bytes(c, &d.lY, nf * 8 * sizeof(float));
     rc |= dalloc_bytes(c, &d.lface, nf * sizeof(int));
     rc |= dalloc_bytes(c, &d.lcount, sizeof(int));
@@ -1882,7 +1879,7 @@ int fvm_set_flux_mode(fvm_ctx *c, int mode, float drho, float dp, float mach, fl
   }
   if (rc) return FVM_ENOMEM;
   LearnBuf &lb = c->lb;
-  lb.X = (__nv_bfloat16 *)d.lX;
+  lb.X = (__half *)d.lX;
   lb.Y = (float *)d.lY;
   lb.gface = (int *)d.lface;
   lb.count = (int *)d.lcount;

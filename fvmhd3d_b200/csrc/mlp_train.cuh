@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(128) k_gemm_tc(int M, int N, int K, const floa
       const uint32_t a = mlp::smem_u32(sa[st]), b = mlp::smem_u32(sb[st]);
 #pragma unroll
       for (int kk = 0; kk < TK / 16; kk++)
-        mlp::mma_bf16(tmem, mlp::smem_desc(a + 2 * kk * LBO_A, LBO_A, SBO), mlp::smem_desc(b + 2 * kk * LBO_B, LBO_B, SBO),
+        mlp::mma_f16kind(tmem, mlp::smem_desc(a + 2 * kk * LBO_A, LBO_A, SBO), mlp::smem_desc(b + 2 * kk * LBO_B, LBO_B, SBO),
                       idesc, (ch > c_begin || kk > 0) ? 1u : 0u);
       mlp::mma_commit(mlp::smem_u32(bars + st));
     }

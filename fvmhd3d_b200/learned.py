@@ -1,7 +1,7 @@
 """Learned face flux: harvesting, training and evaluation on the GPU.
 
-The network (16 -> 128 -> 128 -> 128 -> 8, GELU, BF16 weights, FP32
-accumulation) predicts, on smooth faces, the dissipative part of the HLLD
+The network (16 -> 128 -> 128 -> 128 -> 8, GELU; FP16 operands for
+inference, BF16 for training, FP32 accumulation) predicts, on smooth faces, the dissipative part of the HLLD
 flux in the face frame (the HLLD flux minus the mean of the two sides'
 physical fluxes) divided by the size m of the face's scaled jump; the flux
 pass multiplies the output by m in FP32, so the network's error is relative

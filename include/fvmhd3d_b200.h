@@ -198,13 +198,14 @@ int fvm_compute_flux_static(fvm_ctx *c, int nface, const double *wij, const doub
 
 /* Network 16 -> 128 -> 128 -> 128 -> 8 with GELU hidden layers; parameters in
  * this order, row-major, FP32: W1[128x16], b1[128], W2[128x128], b2[128],
- * W3[128x128], b3[128], W4[8x128], b4[8].  Weights are rounded to BF16 for the
- * tensor cores; biases stay FP32. */
+ * W3[128x128], b3[128], W4[8x128], b4[8].  Inference rounds the weights,
+ * the inputs and the hidden activations to FP16 for the tensor cores (the
+ * training products round their operands to BF16); biases stay FP32. */
 #define FVM_MLP_NPARAM 36232
 int fvm_mlp_set_weights(fvm_ctx *c, const float *params);
 
 /* Known-answer entry: Y[n x 8] = network(X[n x 16]) on the tensor cores, host
- * buffers in and out (X rounded to BF16). */
+ * buffers in and out (X rounded to FP16). */
 int fvm_mlp_eval(fvm_ctx *c, int n, const float *X, float *Y);
 
 /* The same network with the row count read on the device, as the flux

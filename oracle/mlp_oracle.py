@@ -3,9 +3,14 @@
 The network (16 -> 128 -> 128 -> 128 -> 8, GELU hidden layers) has no
 counterpart in the reference; this module is the oracle the tensor-core
 inference and training kernels are checked against.  It reproduces their
-rounding points: inputs, weights and hidden activations rounded to BF16
-(round to nearest even), products and sums in float64 (the kernels accumulate
-in FP32), biases unrounded.
+rounding points, with products and sums in float64 (the kernels accumulate in
+FP32) and biases unrounded:
+
+- ``forward`` / ``loss_and_grad`` (the training kernels): inputs, weights and
+  hidden activations rounded to BF16 (round to nearest even);
+- ``infer`` (the tensor-core inference kernel): inputs and weights rounded to
+  FP16, each hidden pre-activation rounded to FP16 before its GELU and twice
+  the GELU's value rounded to FP16 (the next layer's weights halved).
 
 Parameter vector order: W1[128x16], b1[128], W2[128x128], b2[128],
 W3[128x128], b3[128], W4[8x128], b4[8] (row-major).
@@ -26,6 +31,12 @@ def bf16(x):
     u = x.view(np.uint32).astype(np.uint64)
     u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
     return u.astype(np.uint32).view(np.float32)
+
+
+def f16(x):
+    """Round to the nearest FP16 value (ties to even) by way of FP32, as the
+    kernel rounds its FP32 values; returns float32."""
+    return np.asarray(x, np.float32).astype(np.float16).astype(np.float32)
 
 
 def unpack(p):
@@ -66,6 +77,20 @@ def forward(p, X, keep=False):
         ins.append(a)
     y = a @ Ws[3].T + b4
     return (y, ins, pre, Ws) if keep else y
+
+
+def infer(p, X):
+    """Outputs (n x 8) of the inference kernel's rounded network, in the
+    kernel's own form: each hidden layer stores twice its GELU and the next
+    layer's weights are halved before rounding (W2, W3, W4)."""
+    W1, b1, W2, b2, W3, b3, W4, b4 = unpack(p)
+    a = f16(X).astype(np.float64)
+    z = a @ f16(W1).astype(np.float64).T + b1
+    for W, b in ((W2, b2), (W3, b3), (W4, b4)):
+        x = f16(z).astype(np.float64)
+        a = f16(2.0 * gelu(x)).astype(np.float64)
+        z = a @ f16(0.5 * W).astype(np.float64).T + b
+    return z
 
 
 def loss_and_grad(p, X, Y, wt=None):

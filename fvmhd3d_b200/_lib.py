@@ -75,6 +75,8 @@ SIGNATURES = {
     "fvm_set_tuning": (c_int, [c_void_p, c_void_p]),
     "fvm_set_fused": (c_int, [c_void_p, c_int]),
     "fvm_fused_step_count": (c_ll, [c_void_p]),
+    "fvm_set_list_building": (c_int, [c_void_p, c_int]),
+    "fvm_incremental_step_count": (c_ll, [c_void_p]),
     "fvm_compute_flux": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_compute_flux_static": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_last_step_ms": (c_float, [c_void_p]),

@@ -34,6 +34,9 @@ struct Sched {
   double sink;                // written only by a calibration kernel, never in practice
   int ninv;                   // cells in the involved-cell list of a partial step
   unsigned long long fused_steps;  // steps run by the persistent rung kernel
+  int inc[2];  // incremental list building: [0] links of the active cells, [1] 1 when
+               // this step's lists were built that way
+  unsigned long long inc_steps;  // steps whose lists were built incrementally
 };
 
 struct Dev {
@@ -46,6 +49,9 @@ struct Dev {
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
   int *flist, *fbcount; // ordered active-face list and its block offsets (partial steps)
   int *clist, *cbcount; // ordered list of the step's active and neighbour cells, block offsets (partial steps)
+  int *ilist;           // the step's active cells, unordered (incremental list building, INC_CAP)
+  unsigned *ibits;      // one bit per cell, zero between steps (incremental list building)
+  int *icount;          // per block of k_inc_count: its involved cells (INC_BLOCKS)
   unsigned char *bnb;   // per cell: 1 when a neighbour is a boundary cell (set with the boundary codes)
   int2 *lfj;            // per link: face id, neighbour (~j when the cell is s2)
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
@@ -116,6 +122,11 @@ constexpr int CPW = 64;
 
 namespace {
 
+// Links of the active cells plus the cells themselves up to which a partial
+// step's lists can be built incrementally (k_inc_*), and the room of the
+// active-cell list that path starts from.
+constexpr int INC_CAP = 8192;
+
 enum : unsigned char { A_ACTIVE = 1, A_LNGB = 2, A_HASNGB = 4 };
 enum : unsigned char { F_SWAP = 1, F_SKIPJ = 2, F_OFF = 4 };
 
@@ -126,23 +137,45 @@ __device__ __forceinline__ bool face_active(const unsigned char *act, const int 
 __device__ __forceinline__ void ld3(const double *p, double *o) { o[0] = p[0]; o[1] = p[1]; o[2] = p[2]; }
 
 // ---- begin_step: active flags (Scheduler::pull_active_list) ---------------
+// Active flags of the step's cells (MPI/Scheduler.h:108-154 picks the rungs)
+// and their count.  With ilist, the active cells are also listed (in block
+// order, at most INC_CAP of them) and the links of all of them counted in
+// *ilinks, for the incremental list building of a partial step.
 __global__ void k_active(int n, const int *FVM_RESTRICT rung, const Sched *FVM_RESTRICT S,
-                         unsigned char *FVM_RESTRICT act, int *FVM_RESTRICT nactive) {
+                         unsigned char *FVM_RESTRICT act, int *FVM_RESTRICT nactive, const int *FVM_RESTRICT off,
+                         int *FVM_RESTRICT ilist, int *FVM_RESTRICT ilinks) {
   const unsigned long long flags = S->flags;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   bool a = false;
+  int links = 0;
   if (i < n) {
     const int r = rung[i];
     a = r >= 0 && r < RUNGMAX && ((flags >> (RUNGMAX - 1 - r)) & 1ULL);
     act[i] = a ? A_ACTIVE : 0;
+    if (a && ilist) links = off[i + 1] - off[i];
   }
-  __shared__ int bsum;
-  if (threadIdx.x == 0) bsum = 0;
+  __shared__ int wcnt[32], wlinks[32], base;
+  const unsigned ballot = __ballot_sync(0xffffffffu, a);
+  for (int o = 16; o > 0; o >>= 1) links += __shfl_xor_sync(0xffffffffu, links, o);
+  if (lane == 0) { wcnt[wid] = __popc(ballot); wlinks[wid] = links; }
   __syncthreads();
-  const unsigned cnt = __popc(__ballot_sync(0xffffffffu, a));
-  if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&bsum, (int)cnt);
+  if (threadIdx.x == 0) {
+    int tot = 0, tl = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+      const int cw = wcnt[w];
+      wcnt[w] = tot;  // exclusive prefix: the warp's first slot in the block
+      tot += cw;
+      tl += wlinks[w];
+    }
+    base = tot ? atomicAdd(nactive, tot) : 0;
+    if (ilist && tl) atomicAdd(ilinks, tl);
+  }
   __syncthreads();
-  if (threadIdx.x == 0 && bsum) atomicAdd(nactive, bsum);
+  if (a && ilist) {
+    const int slot = base + wcnt[wid] + __popc(ballot & ((1u << lane) - 1u));
+    if (slot < INC_CAP) ilist[slot] = i;
+  }
 }
 
 // per-step face flags: active face (a face of an active non-boundary cell,
@@ -186,6 +219,151 @@ __global__ void k_faceflags(int nf, const int2 *FVM_RESTRICT s12, unsigned char 
   __syncthreads();
   if (threadIdx.x == 0 && bsum) atomicAdd(nface_active, bsum);
   if (bcount && threadIdx.x == 0) bcount[blockIdx.x] = bsum;  // per-block counts of the face compaction
+}
+
+// ---- incremental list building ---------------------------------------------
+// A partial step with few active cells builds the flags and lists of
+// k_faceflags and the compactions from the active cells' links, without a
+// pass over every face and cell.  The involved cells are the active cells and
+// their neighbours; the faces whose flags and codes the step reads are the
+// links of those cells, and k_inc_faces rewrites exactly those (a face outside
+// them keeps what an earlier step left; k_faceflags treats it as it treats
+// every face, and an incremental step that reaches it rewrites it first).
+// The involved-cell list comes out in ascending order, as k_place_cells
+// leaves it (the adjust_timesteps sites are taken from it in that order);
+// the active-face list holds the same faces as k_place_faces leaves, in the
+// order they were found: every face pass computes each face on its own.
+
+// The neighbour marks of k_faceflags (an inactive neighbour of an active cell
+// is a local neighbour, the active cell has one), and the involved cells as
+// bits of ibits.  One warp per active cell, a lane per link.
+__global__ void k_inc_mark(const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, unsigned char *act,
+                           const Sched *FVM_RESTRICT S, const int *FVM_RESTRICT ilist, unsigned *FVM_RESTRICT ibits) {
+  const int na = S->iscal[1], lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int u = w0; u < na; u += nw) {
+    const int c = ilist[u], q1 = off[c + 1];
+    bool ngb = false;
+    for (int q = off[c] + lane; q < q1; q += 32) {
+      const int jy = lfj[q].y, j = jy >= 0 ? jy : ~jy;
+      if (!(act[j] & A_ACTIVE)) {  // the active bit never changes in this kernel
+        act[j] = A_LNGB;
+        ngb = true;
+        atomicOr(&ibits[j >> 5], 1u << (j & 31));
+      }
+    }
+    if (__any_sync(0xffffffffu, ngb) && lane == 0) act[c] = A_ACTIVE | A_HASNGB;
+    if (lane == 0) atomicOr(&ibits[c >> 5], 1u << (c & 31));
+  }
+}
+
+// The involved cells in ascending order from ibits (clist, count ninv),
+// clearing the bits read, in two launches of INC_BLOCKS blocks: block b
+// takes the words [b W, (b + 1) W), W a multiple of its thread count, and
+// each thread a run of consecutive words.  k_inc_count counts each block's
+// bits; k_inc_cells places them after the counts of the blocks before it.
+constexpr int INC_BLOCKS = 64;
+__device__ __forceinline__ void inc_words(int n, int &w0, int &w1) {
+  const int nw = (n + 31) >> 5;
+  const int W = ((nw + INC_BLOCKS - 1) / INC_BLOCKS + blockDim.x - 1) / blockDim.x * blockDim.x;
+  const int per = W / blockDim.x;
+  w0 = blockIdx.x * W + threadIdx.x * per;
+  w1 = min(nw, w0 + per);
+}
+__device__ __forceinline__ int block_sum(int v, int *wsum) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if (lane == 0) wsum[wid] = v;
+  __syncthreads();
+  int t = 0;
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += wsum[w];
+  return t;
+}
+__global__ void __launch_bounds__(256) k_inc_count(int n, const unsigned *FVM_RESTRICT ibits,
+                                                   int *FVM_RESTRICT bcnt) {
+  __shared__ int wsum[8];
+  int w0, w1;
+  inc_words(n, w0, w1);
+  int c = 0;
+  for (int w = w0; w < w1; w++) c += __popc(ibits[w]);
+  const int t = block_sum(c, wsum);
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = t;
+}
+__global__ void __launch_bounds__(256) k_inc_cells(int n, Sched *FVM_RESTRICT S, unsigned *FVM_RESTRICT ibits,
+                                                   const int *FVM_RESTRICT bcnt, int *FVM_RESTRICT clist) {
+  __shared__ int wsum[8], base;
+  if (threadIdx.x < 32) {  // the counts of the blocks before this one, and of all
+    int before = 0, all = 0;
+    for (int b = threadIdx.x; b < INC_BLOCKS; b += 32) {
+      const int v = bcnt[b];
+      all += v;
+      before += b < (int)blockIdx.x ? v : 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      before += __shfl_xor_sync(0xffffffffu, before, o);
+      all += __shfl_xor_sync(0xffffffffu, all, o);
+    }
+    if (threadIdx.x == 0) {
+      base = before;
+      if (blockIdx.x == 0) S->ninv = all;
+    }
+  }
+  int w0, w1;
+  inc_words(n, w0, w1);
+  int c = 0;
+  for (int w = w0; w < w1; w++) c += __popc(ibits[w]);
+  // exclusive scan of c over the block's threads
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int x = c;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) wsum[wid] = x;
+  __syncthreads();
+  int pos = base + x - c;
+  for (int w = 0; w < wid; w++) pos += wsum[w];
+  for (int w = w0; w < w1; w++) {
+    unsigned v = ibits[w];
+    if (!v) continue;
+    ibits[w] = 0u;
+    while (v) {
+      clist[pos++] = 32 * w + __ffs(v) - 1;
+      v &= v - 1u;
+    }
+  }
+}
+
+// Flags and codes of every face of the involved cells as k_faceflags sets
+// them (an inactive face is coded F_OFF), and the active faces, each listed
+// once: by its s1 cell when that cell is active and not a boundary cell, else
+// by its s2 cell.  One warp per involved cell, a lane per link.
+__global__ void k_inc_faces(const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const int2 *FVM_RESTRICT s12,
+                            const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+                            unsigned char *FVM_RESTRICT fflag, unsigned char *FVM_RESTRICT fcode,
+                            unsigned char *FVM_RESTRICT fcode2, Sched *FVM_RESTRICT S, const int *FVM_RESTRICT clist,
+                            int *FVM_RESTRICT flist) {
+  const int nc = S->ninv, lane = threadIdx.x & 31;
+  const int w0 = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int u = w0; u < nc; u += nw) {
+    const int c = clist[u], q1 = off[c + 1];
+    const bool cact = act[c] & A_ACTIVE;
+    for (int q = off[c] + lane; q < q1; q += 32) {
+      const int f = lfj[q].x;
+      const int2 e = s12[f];
+      const bool a1 = act[e.x] & A_ACTIVE, a2 = act[e.y] & A_ACTIVE;
+      const bool b1 = bnd[e.x] != NO_BOUNDARY, b2 = bnd[e.y] != NO_BOUNDARY;
+      const bool own1 = a1 && !b1, a = own1 || (a2 && !b2);
+      fflag[f] = (unsigned char)((a ? FF_ACTIVE : 0) | (b1 ? FF_BND1 : 0) | (b2 ? FF_BND2 : 0));
+      if (!a) {
+        fcode[f] = F_OFF;
+        fcode2[f] = F_OFF;
+      } else if (cact && c == (own1 ? e.x : e.y)) {
+        flist[atomicAdd(&S->iscal[3], 1)] = f;
+      }
+    }
+  }
 }
 
 // Face offsets used by every face loop, computed once per generator layout:
@@ -1959,6 +2137,8 @@ __global__ void k_sched_begin(Params P, Sched *S) {
   S->iscal[0] = 0;
   S->iscal[1] = 0;
   S->iscal[3] = 0;
+  S->inc[0] = 0;
+  S->inc[1] = 0;
 }
 
 __global__ void k_sched_end(Sched *S, int n) {

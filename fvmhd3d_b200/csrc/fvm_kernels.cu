@@ -182,6 +182,9 @@ struct fvm_ctx {
   // persistent rung kernel (fvm_fused.cu): captured partial steps whose
   // involved cells number at most fused_max run as one launch (0: never)
   int fused_max = 0;
+  // partial steps whose active cells and their links number at most inc_max
+  // build their lists incrementally (0: always the pass over every face)
+  int inc_max = INC_CAP;
   int fused_bpsm = 0;          // its resident blocks per SM (queried outside capture)
   cudaStream_t aux = nullptr;  // captures the branches of the fused/stage choice
   unsigned *gbar = nullptr;    // its grid barrier
@@ -391,6 +394,10 @@ static int alloc_mesh(fvm_ctx *c, long long ncell, long long nface, long long nl
   rc |= dalloc(c, &d.fcode, nface); rc |= dalloc(c, &d.fcode2, nface);
   rc |= dalloc(c, &d.flist, nface); rc |= dalloc(c, &d.fbcount, (nface + CB - 1) / CB + 1);
   rc |= dalloc(c, &d.clist, ncell); rc |= dalloc(c, &d.cbcount, (ncell + CB - 1) / CB + 1);
+  rc |= dalloc(c, &d.ilist, INC_CAP);
+  const long long ibits_words = (ncell + 31) / 32;
+  rc |= dalloc(c, &d.ibits, ibits_words);
+  rc |= dalloc(c, &d.icount, INC_BLOCKS);
   rc |= dalloc(c, &d.bnb, ncell);
   rc |= dalloc_bytes(c, &d.tau, 10 * c->rb * (size_t)ncell);
   rc |= dalloc_bytes(c, &d.fcon, 14 * c->rb * (size_t)nface);
@@ -400,6 +407,10 @@ static int alloc_mesh(fvm_ctx *c, long long ncell, long long nface, long long nl
   if (c->keep_step_dU) rc |= dalloc(c, &d.stepdU, 14 * (size_t)ncell);
   rc |= dalloc(c, &d.S, 1); rc |= dalloc(c, &d.counters, 4);
   if (rc) { free_all(c); return FVM_ENOMEM; }
+  if (cudaMemset(d.ibits, 0, sizeof(unsigned) * ibits_words) != cudaSuccess) {  // zero between steps
+    free_all(c);
+    return FVM_ENOMEM;
+  }
   c->cap_n = ncell;
   c->cap_f = nface;
   c->cap_l = nl;
@@ -669,14 +680,9 @@ int fvm_set_state(fvm_ctx *c, const double *vel, const double *tlast, const doub
 
 // ---- step launches (no host synchronisation) ------------------------------
 
-static int enq_begin(fvm_ctx *c) {
-  const int n = c->n;
+// The flags and lists of a partial step by a pass over every face and cell.
+static int enq_lists_meshwide(fvm_ctx *c) {
   Dev &d = c->d;
-  kt_begin(c, KT_FLAGS);
-  k_sched_begin<<<1, 1, 0, c->st>>>(c->P, d.S);
-  LAUNCH_CHECK();
-  k_active<<<nblk(n, 256), 256, 0, c->st>>>(n, d.rung, d.S, d.act, &d.S->iscal[1]);
-  LAUNCH_CHECK();
   // partial steps: blocks of CB faces, whose counts start the face compaction
   k_faceflags<<<nblk(c->nf, CB), CB, 0, c->st>>>(c->nf, d.s12, d.act, d.bnd, d.fflag, &d.S->iscal[3], d.fcode,
                                                  d.fcode2, c->use_flist ? d.fbcount : nullptr);
@@ -695,6 +701,114 @@ static int enq_begin(fvm_ctx *c) {
     k_place_cells<<<nbc, CB, 0, c->st>>>(c->n, d.act, d.cbcount, d.clist);
     LAUNCH_CHECK();
   }
+  return 0;
+}
+
+// The same flags and lists built from the active cells' links (k_inc_*).
+static int enq_lists_incremental(fvm_ctx *c) {
+  Dev &d = c->d;
+  // a warp per cell: 8 cells per 256-thread block, up to 4 blocks per SM
+  const int grid = std::max(1, std::min(4 * c->sms, INC_CAP / 8));
+  k_inc_mark<<<grid, 256, 0, c->st>>>(d.off, d.lfj, d.act, d.S, d.ilist, d.ibits);
+  LAUNCH_CHECK();
+  k_inc_count<<<INC_BLOCKS, 256, 0, c->st>>>(c->n, d.ibits, d.icount);
+  LAUNCH_CHECK();
+  k_inc_cells<<<INC_BLOCKS, 256, 0, c->st>>>(c->n, d.S, d.ibits, d.icount, d.clist);
+  LAUNCH_CHECK();
+  k_inc_faces<<<grid, 256, 0, c->st>>>(d.off, d.lfj, d.s12, d.act, d.bnd, d.fflag, d.fcode, d.fcode2, d.S, d.clist,
+                                       d.flist);
+  LAUNCH_CHECK();
+  return 0;
+}
+
+// Sets the branch of a captured partial step's list building: incremental
+// when the active cells and their links number at most inc_max.
+__global__ void k_inc_choose(Sched *S, int inc_max, cudaGraphConditionalHandle h) {
+  const int small = S->iscal[1] + S->inc[0] <= inc_max;
+  S->inc[1] = small;
+  S->inc_steps += small;
+  cudaGraphSetConditional(h, small ? 1u : 0u);
+}
+__global__ void k_inc_set(Sched *S) {
+  S->inc[1] = 1;
+  S->inc_steps += 1;
+}
+
+// Captured partial step: an if/else graph node whose branches build the
+// lists incrementally or by the pass over every face (same lists, same bits).
+static int enq_lists_choice(fvm_ctx *c) {
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  k_inc_choose<<<1, 1, 0, c->st>>>(c->d.S, c->inc_max, h);
+  LAUNCH_CHECK();
+  CK(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 2;
+  cudaGraphNode_t cn;
+  CK(cudaGraphAddNode(&cn, g, deps, nd, &cp));
+  cudaGraph_t body_inc = cp.conditional.phGraph_out[0], body_mesh = cp.conditional.phGraph_out[1];
+  // each branch is captured with the auxiliary stream standing in for the
+  // context's
+  int rc = 0;
+  for (int b = 0; b < 2 && !rc; b++) {
+    std::swap(c->st, c->aux);
+    const cudaError_t be = cudaStreamBeginCaptureToGraph(c->st, b == 0 ? body_inc : body_mesh, nullptr, nullptr, 0,
+                                                         cudaStreamCaptureModeRelaxed);
+    cudaError_t ee = cudaSuccess;
+    cudaGraph_t done = nullptr;
+    if (be == cudaSuccess) {
+      rc = b == 0 ? enq_lists_incremental(c) : enq_lists_meshwide(c);
+      ee = cudaStreamEndCapture(c->st, &done);
+    }
+    std::swap(c->st, c->aux);
+    CK(be);
+    if (rc) return rc;
+    CK(ee);
+  }
+  CK(cudaStreamUpdateCaptureDependencies(c->st, &cn, 1, cudaStreamSetCaptureDependencies));
+  return 0;
+}
+
+static int enq_begin(fvm_ctx *c) {
+  const int n = c->n;
+  Dev &d = c->d;
+  kt_begin(c, KT_FLAGS);
+  k_sched_begin<<<1, 1, 0, c->st>>>(c->P, d.S);
+  LAUNCH_CHECK();
+  const bool inc = c->use_flist && c->inc_max > 0;
+  k_active<<<nblk(n, 256), 256, 0, c->st>>>(n, d.rung, d.S, d.act, &d.S->iscal[1], d.off, inc ? d.ilist : nullptr,
+                                            &d.S->inc[0]);
+  LAUNCH_CHECK();
+  int rc = 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  CK(cudaStreamIsCapturing(c->st, &cs));
+  if (inc && cs == cudaStreamCaptureStatusActive && !c->prof) {
+    rc = enq_lists_choice(c);
+  } else if (inc && cs == cudaStreamCaptureStatusNone) {
+    // an eager step makes the same choice on the host
+    int cnt[2] = {0, 0};
+    CK(cudaMemcpyAsync(&cnt[0], &d.S->iscal[1], sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(&cnt[1], &d.S->inc[0], sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (cnt[0] + cnt[1] <= c->inc_max) {
+      k_inc_set<<<1, 1, 0, c->st>>>(d.S);
+      LAUNCH_CHECK();
+      rc = enq_lists_incremental(c);
+    } else {
+      rc = enq_lists_meshwide(c);
+    }
+  } else {
+    rc = enq_lists_meshwide(c);
+  }
+  if (rc) return rc;
   kt_end(c, KT_FLAGS);
   return 0;
 }
@@ -1999,6 +2113,20 @@ int state_copy(fvm_ctx *c, StateCopy &sc, bool save) {
 extern "C" {
 
 long long fvm_fused_step_count(const fvm_ctx *c) { return c ? (long long)c->hS.fused_steps : -1; }
+
+long long fvm_incremental_step_count(const fvm_ctx *c) { return c ? (long long)c->hS.inc_steps : -1; }
+
+int fvm_set_list_building(fvm_ctx *c, int max_entries) {
+  if (!c || max_entries < 0 || max_entries > INC_CAP) {
+    if (c) c->err = "fvm_set_list_building: max_entries must lie in [0, " + std::to_string(INC_CAP) + "]";
+    return FVM_EINVAL;
+  }
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  drop_graphs(c);  // captured partial steps hold the choice
+  c->inc_max = max_entries;
+  return 0;
+}
 
 int fvm_set_fused(fvm_ctx *c, int max_cells) {
   if (!c || max_cells < 0) return FVM_EINVAL;

@@ -283,6 +283,17 @@ class System:
         """Steps the persistent rung kernel has run (as of the last run/step)."""
         return int(self.L.fvm_fused_step_count(self.h))
 
+    def set_list_building(self, max_entries) -> None:
+        """Partial steps whose active cells plus their links number at most
+        max_entries (at most 8192) build their lists from those cells' links
+        instead of a pass over every face (0: never)."""
+        self._check(self.L.fvm_set_list_building(self.h, int(max_entries)), "fvm_set_list_building")
+
+    @property
+    def incremental_steps(self) -> int:
+        """Steps whose lists were built incrementally (as of the last run/step)."""
+        return int(self.L.fvm_incremental_step_count(self.h))
+
     def set_tuning(self, staged_limiter, face_block, cell_block, cell2_block) -> None:
         """Set the launch choices the autotuner picks (see autotune)."""
         ch = np.array([staged_limiter, face_block, cell_block, cell2_block], np.int32)

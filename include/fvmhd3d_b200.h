@@ -294,6 +294,23 @@ int fvm_set_fused(fvm_ctx *c, int max_cells);
  * (as of the last fvm_run or fvm_step). */
 long long fvm_fused_step_count(const fvm_ctx *c);
 
+/* List building of partial steps (individual timesteps).  A step whose
+ * active cells plus their links number at most max_entries builds its flags,
+ * ordered active-face list and involved-cell list from the active cells'
+ * links; larger steps take the pass over every face and cell.  Both select
+ * the same sites (MPI/iterate.cpp:58-113): the same involved cells in
+ * ascending order and the same active faces (listed in the order they are
+ * found; each face pass computes every face on its own, so the results are
+ * the same bits).  max_entries lies in [0, 8192]; 8192
+ * is the default, 0 turns the incremental form off.  The choice is made on
+ * the device each captured step (on the host for eager steps).  Has no
+ * counterpart in the reference. */
+int fvm_set_list_building(fvm_ctx *c, int max_entries);
+
+/* Steps whose lists were built incrementally since the state was installed
+ * (as of the last fvm_run or fvm_step). */
+long long fvm_incremental_step_count(const fvm_ctx *c);
+
 /* Sets the launch choices fvm_autotune picks (same 4 ints: staged limiter
  * 0/1, then block sizes 32, 64 or 128), e.g. to replay a tuned configuration
  * on another run of the same mesh. */

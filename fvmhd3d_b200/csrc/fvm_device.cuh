@@ -49,7 +49,7 @@ struct Dev {
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
   int *flist, *fbcount; // ordered active-face list and its block offsets (partial steps)
   int *clist, *cbcount; // ordered list of the step's active and neighbour cells, block offsets (partial steps)
-  int *ilist;           // the step's active cells, unordered (incremental list building, INC_CAP)
+  int *ilist;           // the step's active cells, unordered (incremental list building)
   unsigned *ibits;      // one bit per cell, zero between steps (incremental list building)
   int *icount;          // per block of k_inc_count: its involved cells (INC_BLOCKS)
   unsigned char *bnb;   // per cell: 1 when a neighbour is a boundary cell (set with the boundary codes)
@@ -122,10 +122,6 @@ constexpr int CPW = 64;
 
 namespace {
 
-// Links of the active cells plus the cells themselves up to which a partial
-// step's lists can be built incrementally (k_inc_*), and the room of the
-// active-cell list that path starts from.
-constexpr int INC_CAP = 8192;
 
 enum : unsigned char { A_ACTIVE = 1, A_LNGB = 2, A_HASNGB = 4 };
 enum : unsigned char { F_SWAP = 1, F_SKIPJ = 2, F_OFF = 4 };
@@ -139,8 +135,8 @@ __device__ __forceinline__ void ld3(const double *p, double *o) { o[0] = p[0]; o
 // ---- begin_step: active flags (Scheduler::pull_active_list) ---------------
 // Active flags of the step's cells (MPI/Scheduler.h:108-154 picks the rungs)
 // and their count.  With ilist, the active cells are also listed (in block
-// order, at most INC_CAP of them) and the links of all of them counted in
-// *ilinks, for the incremental list building of a partial step.
+// order) and the links of all of them counted in *ilinks, for the
+// incremental list building of a partial step.
 __global__ void k_active(int n, const int *FVM_RESTRICT rung, const Sched *FVM_RESTRICT S,
                          unsigned char *FVM_RESTRICT act, int *FVM_RESTRICT nactive, const int *FVM_RESTRICT off,
                          int *FVM_RESTRICT ilist, int *FVM_RESTRICT ilinks) {
@@ -174,7 +170,7 @@ __global__ void k_active(int n, const int *FVM_RESTRICT rung, const Sched *FVM_R
   __syncthreads();
   if (a && ilist) {
     const int slot = base + wcnt[wid] + __popc(ballot & ((1u << lane) - 1u));
-    if (slot < INC_CAP) ilist[slot] = i;
+    ilist[slot] = i;
   }
 }
 

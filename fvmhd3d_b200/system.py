@@ -285,8 +285,9 @@ class System:
 
     def set_list_building(self, max_entries) -> None:
         """Partial steps whose active cells plus their links number at most
-        max_entries (at most 8192) build their lists from those cells' links
-        instead of a pass over every face (0: never)."""
+        max_entries build their lists from those cells' links instead of a
+        pass over every face (-1: 1/256 of the mesh's cells plus links, at
+        least 8192, the default; 0: never)."""
         self._check(self.L.fvm_set_list_building(self.h, int(max_entries)), "fvm_set_list_building")
 
     @property

@@ -296,15 +296,15 @@ long long fvm_fused_step_count(const fvm_ctx *c);
 
 /* List building of partial steps (individual timesteps).  A step whose
  * active cells plus their links number at most max_entries builds its flags,
- * ordered active-face list and involved-cell list from the active cells'
- * links; larger steps take the pass over every face and cell.  Both select
- * the same sites (MPI/iterate.cpp:58-113): the same involved cells in
- * ascending order and the same active faces (listed in the order they are
- * found; each face pass computes every face on its own, so the results are
- * the same bits).  max_entries lies in [0, 8192]; 8192
- * is the default, 0 turns the incremental form off.  The choice is made on
- * the device each captured step (on the host for eager steps).  Has no
- * counterpart in the reference. */
+ * active-face list and involved-cell list from the active cells' links;
+ * larger steps take the pass over every face and cell.  Both select the same
+ * sites (MPI/iterate.cpp:58-113): the same involved cells in ascending order
+ * and the same active faces (listed in the order they are found; each face
+ * pass computes every face on its own, so the results are the same bits).
+ * max_entries: -1 (the default) for 1/256 of the mesh's cells plus links
+ * (at least 8192), 0 to turn the incremental form off, or a positive bound.  The
+ * choice is made on the device each captured step (on the host for eager
+ * steps).  Has no counterpart in the reference. */
 int fvm_set_list_building(fvm_ctx *c, int max_entries);
 
 /* Steps whose lists were built incrementally since the state was installed

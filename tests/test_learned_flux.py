@@ -65,8 +65,8 @@ def test_twice_gelu_with_halved_weights_is_the_same_network():
 # per output over the rows, relative to that output's largest magnitude.  The
 # kernel differs from the oracle by FP32 accumulation order and its GELU
 # epilogue in packed half precision (u and the result rounded to FP16, the
-# hardware tanh.approx.f16x2).
-INFER_RTOL = 6e-3
+# hardware tanh.approx.f16x2): measured at most 1.4e-3.
+INFER_RTOL = 3e-3
 
 
 # 148 SMs x 4 tile chains x 128 rows = 75,776 rows per wave: the larger

@@ -1014,20 +1014,70 @@ __device__ __forceinline__ void gather_contrib(int c, int q0, int q1, const int2
   }
 }
 
+// The same sums with G consecutive lanes per cell (G a power of two, gmask
+// the group's lanes, gl this lane's index in it): lane gl loads the records
+// of links q0 + gl, q0 + gl + G, ..., and every lane of the group adds all
+// the records in link order, each taken by shuffle from the lane that
+// loaded it, with the operations of gather_contrib: the sums are its bits,
+// and a cell's walk is q1 - q0 over G loads deep instead of q1 - q0.
+template <typename R, int G>
+__device__ __forceinline__ void gather_contrib_group(int q0, int q1, const int2 *FVM_RESTRICT lfj,
+                                                     const R *FVM_RESTRICT fcon,
+                                                     const unsigned char *FVM_RESTRICT fcode, bool skipj_allowed,
+                                                     int gl, unsigned gmask, double *s) {
+  constexpr bool kahan = sizeof(R) == 4;
+  double comp[14];
+#pragma unroll
+  for (int k = 0; k < 14; k++) { s[k] = 0.0; comp[k] = 0.0; }
+  for (int base = q0; base < q1; base += G) {
+    const int q = base + gl;
+    R vr[14];  // the record as stored; the side and use bits travel with it
+    int info = 0;
+    if (q < q1) {
+      const int2 fj = lfj[q];
+      const int f = fj.x;
+      load_n<R, 14>(fcon + 14 * (size_t)f, vr);
+      const unsigned char code = fcode[f];
+      const bool is_i = (fj.y >= 0) != ((code & F_SWAP) != 0);
+      const bool use = !(code & F_OFF) && !(!is_i && skipj_allowed && (code & F_SKIPJ));
+      info = (is_i ? 1 : 0) | (use ? 2 : 0);
+    } else {
+#pragma unroll
+      for (int k = 0; k < 14; k++) vr[k] = R(0);
+    }
+    const int m = min(G, q1 - base);
+    for (int j = 0; j < m; j++) {
+      const int ij = __shfl_sync(gmask, info, j, G);
+      const bool is_i = ij & 1, use = (ij & 2) != 0;
+      const double wu = is_i ? -1.0 : 1.0;
+#pragma unroll
+      for (int k = 0; k < 14; k++) {
+        const double v = double(__shfl_sync(gmask, vr[k], j, G));
+        if (kahan) {
+          const double term = ((k < NF) == is_i) ? -v : v;
+          const double y = term - comp[k];
+          const double t = s[k] + y;
+          comp[k] = use ? (t - s[k]) - y : comp[k];
+          s[k] = use ? t : s[k];
+        } else {
+          // fma(+-1, use ? v : 0, s) of gather_contrib: the product is exact
+          s[k] = s[k] + (k < NF ? wu : -wu) * (use ? v : 0.0);
+        }
+      }
+    }
+  }
+}
+
 // ---- compute_update cell pass (MPI/compute_update.cpp:274-498) -----------
+// The cell's update from its summed face contributions s (ac: its act
+// flags, active or local neighbour).
 template <typename R>
-__device__ __forceinline__ void corr_cell_body(int c, double t_global, const Params &P,
-    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
-    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+__device__ __forceinline__ void corr_cell_finish(int c, unsigned char ac, const double *s, double t_global,
+    const Params &P, const double *FVM_RESTRICT cvol, const int *FVM_RESTRICT bnd,
     const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast, double *FVM_RESTRICT volp,
     const R *FVM_RESTRICT Wrec, const R *FVM_RESTRICT tau,
-    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
     double *FVM_RESTRICT U, double *FVM_RESTRICT dU, double *FVM_RESTRICT stepdU,
     unsigned long long *FVM_RESTRICT counters, float *FVM_RESTRICT divb) {
-  const unsigned char ac = act[c];
-  if (!(ac & (A_ACTIVE | A_LNGB))) return;
-  double s[14];
-  gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, true, s);
   double *d0p = dU + 14 * (size_t)c;  // rows of 14 doubles: 2-wide loads and stores
   double d0[14];
   load_n<double, 14>(d0p, d0);
@@ -1112,6 +1162,42 @@ __device__ __forceinline__ void corr_cell_body(int c, double t_global, const Par
   double Un[NF];
   to_conservative(W1, V, Un);
   store_n<double, NF>(U + 10 * (size_t)c, Un);
+}
+
+template <typename R>
+__device__ __forceinline__ void corr_cell_body(int c, double t_global, const Params &P,
+    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
+    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+    const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast, double *FVM_RESTRICT volp,
+    const R *FVM_RESTRICT Wrec, const R *FVM_RESTRICT tau,
+    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
+    double *FVM_RESTRICT U, double *FVM_RESTRICT dU, double *FVM_RESTRICT stepdU,
+    unsigned long long *FVM_RESTRICT counters, float *FVM_RESTRICT divb) {
+  const unsigned char ac = act[c];
+  if (!(ac & (A_ACTIVE | A_LNGB))) return;
+  double s[14];
+  gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, true, s);
+  corr_cell_finish<R>(c, ac, s, t_global, P, cvol, bnd, pos, tlast, volp, Wrec, tau, U, dU, stepdU, counters, divb);
+}
+
+// The same with G lanes per cell (gather_contrib_group; the group's first
+// lane finishes the cell).
+template <typename R, int G>
+__device__ __forceinline__ void corr_cell_group(int c, int gl, unsigned gmask, double t_global, const Params &P,
+    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
+    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+    const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast, double *FVM_RESTRICT volp,
+    const R *FVM_RESTRICT Wrec, const R *FVM_RESTRICT tau,
+    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
+    double *FVM_RESTRICT U, double *FVM_RESTRICT dU, double *FVM_RESTRICT stepdU,
+    unsigned long long *FVM_RESTRICT counters, float *FVM_RESTRICT divb) {
+  const unsigned char ac = act[c];
+  if (!(ac & (A_ACTIVE | A_LNGB))) return;
+  double s[14];
+  gather_contrib_group<R, G>(off[c], off[c + 1], lfj, fcon, fcode, true, gl, gmask, s);
+  if (gl == 0)
+    corr_cell_finish<R>(c, ac, s, t_global, P, cvol, bnd, pos, tlast, volp, Wrec, tau, U, dU, stepdU, counters,
+                        divb);
 }
 
 // One thread per cell; in partial steps a fixed grid strides over the
@@ -1856,16 +1942,10 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Par
 // Writes the predicted time derivative t into the cell's Wrec and the
 // cell's final rung/tend.  Arithmetic in double for both bulk types.
 template <typename R>
-__device__ __forceinline__ void pred_cell_body(int c, double t_global, int min_rung, const Params &P,
-    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
-    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
-    const double *FVM_RESTRICT pos, const double *FVM_RESTRICT U,
-    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
-    int *FVM_RESTRICT rung, double *FVM_RESTRICT tend, R *FVM_RESTRICT Wrec) {
-  if (!(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
+__device__ __forceinline__ void pred_cell_finish(int c, const double *dot, double t_global, int min_rung,
+    const Params &P, const double *FVM_RESTRICT cvol, const double *FVM_RESTRICT pos,
+    const double *FVM_RESTRICT U, int *FVM_RESTRICT rung, double *FVM_RESTRICT tend, R *FVM_RESTRICT Wrec) {
   const double V = cvol[c];
-  double dot[14];
-  gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, false, dot);
   double u0[NF], W0[NF];
   load_n<double, NF>(U + 10 * (size_t)c, u0);
   to_primitive(u0, V, W0);
@@ -1907,6 +1987,34 @@ __device__ __forceinline__ void pred_cell_body(int c, double t_global, int min_r
   rf = rf < rb ? rb : rf;
   rung[c] = rf;
   tend[c] = t_global + get_dt(P, rf);
+}
+
+template <typename R>
+__device__ __forceinline__ void pred_cell_body(int c, double t_global, int min_rung, const Params &P,
+    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
+    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+    const double *FVM_RESTRICT pos, const double *FVM_RESTRICT U,
+    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
+    int *FVM_RESTRICT rung, double *FVM_RESTRICT tend, R *FVM_RESTRICT Wrec) {
+  if (!(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
+  double dot[14];
+  gather_contrib<R>(c, off[c], off[c + 1], lfj, fcon, fcode, false, dot);
+  pred_cell_finish<R>(c, dot, t_global, min_rung, P, cvol, pos, U, rung, tend, Wrec);
+}
+
+// The same with G lanes per cell (gather_contrib_group; the group's first
+// lane finishes the cell).
+template <typename R, int G>
+__device__ __forceinline__ void pred_cell_group(int c, int gl, unsigned gmask, double t_global, int min_rung,
+    const Params &P, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
+    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+    const double *FVM_RESTRICT pos, const double *FVM_RESTRICT U,
+    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
+    int *FVM_RESTRICT rung, double *FVM_RESTRICT tend, R *FVM_RESTRICT Wrec) {
+  if (!(act[c] & A_ACTIVE) || bnd[c] != NO_BOUNDARY) return;
+  double dot[14];
+  gather_contrib_group<R, G>(off[c], off[c + 1], lfj, fcon, fcode, false, gl, gmask, dot);
+  if (gl == 0) pred_cell_finish<R>(c, dot, t_global, min_rung, P, cvol, pos, U, rung, tend, Wrec);
 }
 
 // One thread per cell; in partial steps a fixed grid strides over clist.

@@ -18,6 +18,11 @@
 
 namespace {
 
+// Lanes per cell in the cell passes of compute_update and compute_update0:
+// a small step has few cells, and each cell's walk over its ~16 faces is a
+// chain of dependent loads; split over 8 lanes it is two loads deep.
+constexpr int kCellGroup = 8;
+
 // Polls of a grid barrier wait before it gives up (about 100 ns each): far
 // above the longest stage of a step this kernel runs (the sequential
 // adjust_timesteps sweep over at most its involved cells).
@@ -109,6 +114,10 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   // 200-cell step against 0.15 ms with the whole grid).
   const unsigned nwork = gridDim.x;
   const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = (int)nwork * blockDim.x;
+  // lane groups of the cell passes that split a cell's faces (same sums, in
+  // the same order, as one thread per cell)
+  const int gl = threadIdx.x & (kCellGroup - 1);
+  const unsigned gmask = ((1u << kCellGroup) - 1u) << ((threadIdx.x & 31) & ~(kCellGroup - 1));
   unsigned gen = load_acquire(&a.gbar[1]);
 #define FVM_GRID_SYNC() \
   if (!grid_barrier(a.gbar, gen, a.gerr, nwork)) return
@@ -138,9 +147,14 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   corr_flux_dev<R, LM_EXACT>(nf, P, S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, d.tlast, (const R *)d.Wrec,
                              (const R *)d.fst, (R *)d.fcon, d.fcode, a.lb, d.flist, 1, gt, gn);
   FVM_GRID_SYNC();
-  corr_cell_dev<R>(n, P, S, d.off, d.lfj, d.s12, d.cvol, d.act, d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
-                   (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU, d.stepdU, d.counters, d.perm, d.divb,
-                   d.clist, gt, gn);
+  {  // the cells: kCellGroup lanes per cell, the walk over its faces split among them
+    const double t_global = S->t_global;
+    const int ninv = S->ninv;
+    for (int t = gt / kCellGroup; t < ninv; t += gn / kCellGroup)
+      corr_cell_group<R, kCellGroup>(d.clist[t], gl, gmask, t_global, P, d.off, d.lfj, d.cvol, d.act, d.bnd, d.pos,
+                                     d.tlast, d.volp, (const R *)d.Wrec, (const R *)d.tau, (const R *)d.fcon,
+                                     d.fcode, d.U, d.dU, d.stepdU, d.counters, d.divb);
+  }
   FVM_GRID_SYNC();
   pvel_dev(n, P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel, d.clist, &S->ninv, gt, gn);
   FVM_GRID_SYNC();
@@ -193,8 +207,14 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   pred_flux_dev<R, LM_EXACT>(nf, P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, (const R *)d.Wst, (R *)d.fcon2,
                              d.fcode2, S, d.rung, a.lb, d.flist, 1, gt, gn);
   FVM_GRID_SYNC();
-  pred_cell_dev<R>(n, P, S, d.off, d.lfj, d.s12, d.cvol, d.act, d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2,
-                   d.rung, d.tend, (R *)d.Wrec, d.perm, d.clist, gt, gn);
+  {
+    const double t_global = S->t_global;
+    const int min_rung = S->min_rung, ninv = S->ninv;
+    for (int t = gt / kCellGroup; t < ninv; t += gn / kCellGroup)
+      pred_cell_group<R, kCellGroup>(d.clist[t], gl, gmask, t_global, min_rung, P, d.off, d.lfj, d.cvol, d.act,
+                                     d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung, d.tend,
+                                     (R *)d.Wrec);
+  }
   FVM_GRID_SYNC();
   recon_dev<R, CellTune<R>::KH_REC, CellTune<R>::MINB_REC>(n, P, S, d.off, d.lfj, d.cvol, d.act, d.bnd,
                                                            (const R *)d.Wst, d.rung, (R *)d.Wrec, d.perm,

@@ -1293,9 +1293,15 @@ __global__ void k_pvel(int n, Params P, const unsigned char *FVM_RESTRICT act, c
 // ---- compute_timestep(i) (MPI/compute_timestep.cpp:6-51) ------------------
 // The face minimum min_f h / x_f is taken as h / max_f x_f: h > 0 and a
 // rounded quotient never increases with its divisor, so both give the same
-// double, with one division instead of one per face.
+// double, with one division instead of one per face.  With G > 1 lanes per
+// cell (gl this lane's index in its group, gmask the group's lanes) every
+// lane computes the cell's own terms, the faces are split among the lanes
+// and their maximum is reduced by shuffles: a maximum does not depend on the
+// order, so every lane gets the double one lane would.
+template <int G = 1>
 __device__ double cell_timestep(const Params &P, int i, bool with_faces, const int *off, const int2 *lfj,
-                                const int *bnd, const double *U, const double *volp, const double *vel) {
+                                const int *bnd, const double *U, const double *volp, const double *vel, int gl = 0,
+                                unsigned gmask = 0xffffffffu) {
   double W[NF];
   to_primitive(U + 10 * (size_t)i, volp[i], W);
   const double *pv = vel + 3 * (size_t)i;
@@ -1314,8 +1320,8 @@ __device__ double cell_timestep(const Params &P, int i, bool with_faces, const i
   if (with_faces) {
     const double fac = b ? 0.0 : 1.0;
     double xmax = 0.0;
-    const int q1 = off[i + 1];
-    for (int q = off[i]; q < q1; q++) {
+    const int q0 = off[i], q1 = off[i + 1];
+    for (int q = q0 + gl; q < q1; q += G) {
       const int2 fj = lfj[q];
       const int j = fj.y >= 0 ? fj.y : ~fj.y;
       const double *vj = vel + 3 * (size_t)j;
@@ -1326,7 +1332,8 @@ __device__ double cell_timestep(const Params &P, int i, bool with_faces, const i
       const double dwa = sqrt(dw[0] * dw[0] + dw[1] * dw[1] + dw[2] * dw[2]);
       xmax = smax(xmax, smax(fac * (csi + rv), 1.0 / FVM_HUGE + dwa));
     }
-    if (q1 > off[i]) dti = smin(dti, h / xmax);
+    for (int o = G / 2; o > 0; o >>= 1) xmax = smax(xmax, __shfl_xor_sync(gmask, xmax, o, G));
+    if (q1 > q0) dti = smin(dti, h / xmax);
   }
   return dti * P.courant;
 }
@@ -1374,6 +1381,38 @@ __device__ __forceinline__ void timestep_dev(int n, Params P, const int *FVM_RES
   for (int o = 16; o > 0; o >>= 1) vmin = smin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
   if ((threadIdx.x & 31) == 0 && vmin < FVM_HUGE) atomic_min_pos(dmin, vmin);
 }
+// The same with G lanes per cell over the involved-cell list (the group's
+// first lane writes the cell's dt and takes part in the minimum).
+template <int G>
+__device__ __forceinline__ void timestep_group(Params P, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
+                           const unsigned char *FVM_RESTRICT act,
+                           const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT U,
+                           const double *FVM_RESTRICT volp, const double *FVM_RESTRICT vel,
+                           const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast,
+                           const double *FVM_RESTRICT tend, double *FVM_RESTRICT dtl,
+                           double *FVM_RESTRICT dmin, const int *FVM_RESTRICT clist, int ninv, int gl,
+                           unsigned gmask, int g0, int gn) {
+  double vmin = FVM_HUGE;
+  for (int t_ = g0; t_ < ninv; t_ += gn) {
+    const int i = clist[t_];
+    const unsigned char a = act[i];
+    if (!(a & (A_ACTIVE | A_LNGB))) {
+      if (gl == 0) dtl[i] = FVM_HUGE;
+    } else if (!(a & A_ACTIVE)) {
+      if (gl == 0) dtl[i] = (tend[i] - tlast[i]) * (bnd[i] != NO_BOUNDARY ? -1.0 : 1.0);
+    } else {
+      const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
+                              cell_timestep<G>(P, i, true, off, lfj, bnd, U, volp, vel, gl, gmask));
+      if (gl == 0) {
+        vmin = smin(vmin, dti);
+        dtl[i] = bnd[i] != NO_BOUNDARY ? -1.0 * dti : dti;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) vmin = smin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+  if ((threadIdx.x & 31) == 0 && vmin < FVM_HUGE) atomic_min_pos(dmin, vmin);
+}
+
 __global__ void k_timestep(int n, Params P, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
                            const unsigned char *FVM_RESTRICT act,
                            const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT U,
@@ -1447,6 +1486,49 @@ __device__ __forceinline__ void adjust_mark_dev(int n, const int *FVM_RESTRICT o
   __syncthreads();
   if (threadIdx.x == 0 && bsum) atomicAdd(ndirty, bsum);
 }
+// The same with G lanes per site over the involved-cell list: the faces
+// split among the lanes (the marks do not depend on the order), the site's
+// own marks and count by the group's first lane.  Called by every thread of
+// the block.
+template <int G>
+__device__ __forceinline__ void adjust_mark_group(const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
+                              const unsigned char *FVM_RESTRICT act,
+                              const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT dtl,
+                              unsigned char *FVM_RESTRICT hash, int *FVM_RESTRICT ndirty,
+                              unsigned char *FVM_RESTRICT site, unsigned char *FVM_RESTRICT work,
+                              const int *FVM_RESTRICT clist, int ninv, int gl, unsigned gmask, int g0, int gn) {
+  int ndirty_t = 0;
+  for (int t_ = g0; t_ < ninv; t_ += gn) {
+    const int i = clist[t_];
+    if (!(act[i] & A_ACTIVE) || bnd[i] != NO_BOUNDARY) continue;
+    bool dirty = false;
+    const double di = dtl[i];
+    for (int q = off[i] + gl; q < off[i + 1]; q += G) {
+      const int2 fj = lfj[q];
+      const int j = fj.y >= 0 ? fj.y : ~fj.y;
+      const double dj = dtl[j];
+      if (dj < 0.0) continue;
+      hash[j] = 1;
+      if (2.0 * dj < di || 2.0 * di < dj) {
+        dirty = true;
+        work[j] = 1;
+      }
+    }
+    dirty = __any_sync(gmask, dirty);
+    if (gl == 0) {
+      site[i] = 1;
+      if (dirty) { work[i] = 1; ndirty_t++; }
+    }
+  }
+  __shared__ int bsum;
+  if (threadIdx.x == 0) bsum = 0;
+  __syncthreads();
+  for (int o = 16; o > 0; o >>= 1) ndirty_t += __shfl_xor_sync(0xffffffffu, ndirty_t, o);
+  if ((threadIdx.x & 31) == 0 && ndirty_t) atomicAdd(&bsum, ndirty_t);
+  __syncthreads();
+  if (threadIdx.x == 0 && bsum) atomicAdd(ndirty, bsum);
+}
+
 __global__ void k_adjust_mark(int n, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
                               const unsigned char *FVM_RESTRICT act,
                               const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT dtl,

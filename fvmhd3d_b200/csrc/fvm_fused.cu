@@ -18,9 +18,10 @@
 
 namespace {
 
-// Lanes per cell in the cell passes of compute_update and compute_update0:
-// a small step has few cells, and each cell's walk over its ~16 faces is a
-// chain of dependent loads; split over 8 lanes it is two loads deep.
+// Lanes per cell in the cell passes of compute_update and compute_update0,
+// the timestep and the adjust_timesteps marks: a small step has few cells,
+// and each cell's walk over its ~16 faces is a chain of dependent loads;
+// split over 8 lanes it is two loads deep.
 constexpr int kCellGroup = 8;
 
 // Polls of a grid barrier wait before it gives up (about 100 ns each): far
@@ -160,13 +161,13 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   FVM_GRID_SYNC();
   // compute_timesteps(false): CFL timestep and its minimum, halving,
   // adjust_timesteps (marks, parallel replays, sequential fallback), rungs
-  timestep_dev(n, P, d.off, d.lfj, d.act, d.bnd, d.U, d.volp, d.vel, d.pos, d.tlast, d.tend, d.dtl, &S->dtmin,
-               d.clist, &S->ninv, gt, gn);
+  timestep_group<kCellGroup>(P, d.off, d.lfj, d.act, d.bnd, d.U, d.volp, d.vel, d.pos, d.tlast, d.tend, d.dtl,
+                             &S->dtmin, d.clist, S->ninv, gl, gmask, gt / kCellGroup, gn / kCellGroup);
   FVM_GRID_SYNC();
   halve_dev(n, d.act, &S->dtmin, d.dtl, d.clist, &S->ninv, gt, gn);
   FVM_GRID_SYNC();
-  adjust_mark_dev(n, d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash, &S->iscal[4], d.act0, d.awork, d.clist, &S->ninv,
-                  gt, gn);
+  adjust_mark_group<kCellGroup>(d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash, &S->iscal[4], d.act0, d.awork, d.clist,
+                                S->ninv, gl, gmask, gt / kCellGroup, gn / kCellGroup);
   {  // active non-boundary sites (the count the separate-kernel step takes from its compaction)
     const int ninv = S->ninv;
     int cnt = 0;

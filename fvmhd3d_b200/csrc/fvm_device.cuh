@@ -769,8 +769,15 @@ __global__ void __launch_bounds__(128, MINB) k_limiter_st(int n, Params P, const
   if (only_all && S->iscal[1] != n) return;
   const double t_global = S->t_global;
   const bool reuse = FVM_REUSE_MINMAX && S->mnmx_ok && S->iscal[1] == n;
-  limiter_st_block<R, KH>(blockIdx.x, n, reuse, t_global, soff, lsm, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
-                          Wrec, tau, fst, perm, mnmx, mz, lld);
+  // one cell block per block, or (a grid smaller than the cell blocks, as
+  // partial steps launch it, where it usually has nothing to do) a loop over
+  // them; a block's threads meet at the block's barriers in every pass
+  const int ncb = (n + CST - 1) / CST;
+  for (int cb = blockIdx.x; cb < ncb; cb += gridDim.x) {
+    if (cb != (int)blockIdx.x) __syncthreads();  // the previous pass is done with the staging
+    limiter_st_block<R, KH>(cb, n, reuse, t_global, soff, lsm, off, lnk, lfj, s12, geo, dr1, fflag, act, tlast,
+                            Wrec, tau, fst, perm, mnmx, mz, lld);
+  }
 }
 template <typename R, int KH, int MINB>
 __device__ __forceinline__ void limiter_dev(int n, Params P, const Sched *FVM_RESTRICT S,

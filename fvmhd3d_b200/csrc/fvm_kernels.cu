@@ -847,8 +847,13 @@ static int enq_limiter(fvm_ctx *c) {
                                 limiter_stage_bytes<R, CellTune<R>::KH_LIM>()));
         attr[c->device] = true;
       }
+      // a partial step launches it on a grid of resident blocks (it returns
+      // at once unless every cell is active); a global step on one block per
+      // cell block
+      const long long ncb = nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>());
+      const long long grid = c->use_flist ? std::min<long long>(ncb, (long long)CellTune<R>::MINB_LIM * c->sms) : ncb;
       k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
-          <<<nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>()), 128,
+          <<<(unsigned)grid, 128,
              limiter_stage_bytes<R, CellTune<R>::KH_LIM>(), c->st>>>(
           c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
           (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, c->use_flist, (const R *)d.lld);

@@ -62,11 +62,18 @@ def test_twice_gelu_with_halved_weights_is_the_same_network():
 
 
 # Tensor-core inference against the oracle's rounded network: largest error
-# per output over the rows, relative to that output's largest magnitude.  The
-# kernel differs from the oracle by FP32 accumulation order and its GELU
-# epilogue in packed half precision (u and the result rounded to FP16, the
-# hardware tanh.approx.f16x2): measured at most 1.4e-3.
+# per output over the rows, relative to that output's largest magnitude over
+# 4096 rows of the same distribution (a few rows alone would make the scale
+# the size of whatever values they happen to have).  The kernel differs from
+# the oracle by FP32 accumulation order and its GELU epilogue in packed half
+# precision (u and the result rounded to FP16, the hardware
+# tanh.approx.f16x2): measured at most 1.4e-3.
 INFER_RTOL = 3e-3
+
+
+def output_scale(p):
+    X = np.random.default_rng(12345).normal(size=(4096, M.NIN))
+    return np.abs(M.infer(p, X)).max(axis=0)
 
 
 # 148 SMs x 4 tile chains x 128 rows = 75,776 rows per wave: the larger
@@ -83,8 +90,7 @@ def test_tensor_core_inference_matches_oracle(n):
     X = rng.normal(size=(n, M.NIN)).astype(np.float32)
     got = s.mlp_eval(X)
     ref = M.infer(p, X)
-    scale = np.abs(ref).max(axis=0)
-    err = np.abs(got - ref).max(axis=0) / scale
+    err = np.abs(got - ref).max(axis=0) / output_scale(p)
     assert np.isfinite(got).all()
     assert err.max() <= INFER_RTOL, err
 
@@ -105,7 +111,7 @@ def test_tensor_core_inference_with_a_device_row_count():
     got = s.mlp_eval_counted(X, n, Y0)
     assert (got[n:] == 7.0).all()
     ref = M.infer(p, X[:n])
-    err = np.abs(got[:n] - ref).max(axis=0) / np.abs(ref).max(axis=0)
+    err = np.abs(got[:n] - ref).max(axis=0) / output_scale(p)
     assert err.max() <= INFER_RTOL, err
 
 

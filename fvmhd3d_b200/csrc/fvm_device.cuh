@@ -641,6 +641,124 @@ __device__ __forceinline__ void limiter_thread(int i, int k0, bool reuse, double
   }
 }
 
+// limiter_thread with G lanes (a group of consecutive lanes, gl this lane's
+// index, gmask the group's lanes) for one cell and primitive pair, in a step
+// where not every cell is active (pass 1 always runs): the faces are split
+// among the lanes in passes 1 and 3; the neighbour minimum and maximum of
+// pass 1 do not depend on the order (only their magnitudes are used) and are
+// reduced by shuffles; pass 2's ratio minimum compares cross-multiplied
+// products, whose rounding makes it depend on the order, so every lane folds
+// the faces in face order, each face's extrapolated difference taken by
+// shuffle from the lane that computed it.  The same bits as limiter_thread.
+template <typename R, int KH, int G>
+__device__ __forceinline__ void limiter_group(int i, int k0, int gl, unsigned gmask, double t_global,
+    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const unsigned char *FVM_RESTRICT fflag,
+    const unsigned char *FVM_RESTRICT act, const double *FVM_RESTRICT tlast,
+    const R *FVM_RESTRICT Wrec, R *FVM_RESTRICT tau, R *FVM_RESTRICT fst, const R *FVM_RESTRICT lld) {
+  if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
+  const double ti = tlast[i];
+  const R *ri = Wrec + 50 * (size_t)i + k0;
+  R mn[KH], mx[KH], ln[KH], lq[KH], wi[KH];
+#pragma unroll
+  for (int k = 0; k < KH; k++) { mn[k] = R(0); mx[k] = R(0); ln[k] = R(2); lq[k] = R(1); wi[k] = ri[k]; }
+  const int q0 = off[i], q1 = off[i + 1];
+  bool zero = false;
+  for (int q = q0 + gl; q < q1; q += G) {
+    const int2 fj = lfj[q];
+    const int f = fj.x, j = fj.y >= 0 ? fj.y : ~fj.y;
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE)) continue;
+    if (ff & (FF_BND1 | FF_BND2)) { zero = true; continue; }
+    R rj[KH];
+    load_n<R, KH>(Wrec + 50 * (size_t)j + k0, rj);
+#pragma unroll
+    for (int k = 0; k < KH; k++) {
+      const R diff = rj[k] - wi[k];
+      mn[k] = smin(mn[k], diff);
+      mx[k] = smax(mx[k], diff);
+    }
+  }
+  for (int o = G / 2; o > 0; o >>= 1) {
+#pragma unroll
+    for (int k = 0; k < KH; k++) {
+      mn[k] = smin(mn[k], __shfl_xor_sync(gmask, mn[k], o, G));
+      mx[k] = smax(mx[k], __shfl_xor_sync(gmask, mx[k], o, G));
+    }
+  }
+  zero = __any_sync(gmask, zero);
+  R *to = tau + 10 * (size_t)i + k0;
+  R gx[KH], gy[KH], gz[KH], gt[KH];
+  if (zero) {
+#pragma unroll
+    for (int k = 0; k < KH; k++) { if (gl == 0) to[k] = R(0); gx[k] = gy[k] = gz[k] = gt[k] = R(0); }
+  } else {
+    R thr[KH];
+#pragma unroll
+    for (int k = 0; k < KH; k++) {
+      gx[k] = ri[10 + k]; gy[k] = ri[20 + k]; gz[k] = ri[30 + k]; gt[k] = ri[40 + k];
+      thr[k] = limiter_thr(mn[k], mx[k]);
+    }
+    for (int base = q0; base < q1; base += G) {
+      const int q = base + gl;
+      R dW[KH];
+      int fa = 0;
+#pragma unroll
+      for (int k = 0; k < KH; k++) dW[k] = R(0);
+      if (q < q1) {
+        const int2 fj = lfj[q];
+        const int f = fj.x;
+        if (fflag[f] & FF_ACTIVE) {
+          fa = 1;
+          const bool own = fj.y >= 0;
+          const double tj = tlast[own ? fj.y : ~fj.y];
+          const double dtI = t_global - (own ? ti : tj), dtJ = t_global - (own ? tj : ti);
+          const double dth = 0.5 * smin(dtI, dtJ);
+          const R *l3 = lld + 3 * (size_t)q;
+          const R dr[3] = {l3[0], l3[1], l3[2]};
+          const R dtt = R(own ? dtI - dth : dtJ - dth);
+#pragma unroll
+          for (int k = 0; k < KH; k++) {
+            const R dWx = gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2];
+            dW[k] = dWx + gt[k] * dtt;
+          }
+        }
+      }
+      const int m = min(G, q1 - base);
+      for (int jj = 0; jj < m; jj++) {
+        const int faj = __shfl_sync(gmask, fa, jj, G);
+#pragma unroll
+        for (int k = 0; k < KH; k++) {
+          const R d = __shfl_sync(gmask, dW[k], jj, G);
+          if (faj) limiter_ratio(ln[k], lq[k], d, mn[k], mx[k], thr[k]);
+        }
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KH; k++) {
+      const R tk = limiter_finish(ln[k], lq[k]);
+      if (gl == 0) to[k] = tk;
+      gx[k] *= tk; gy[k] *= tk; gz[k] *= tk; gt[k] *= tk;
+    }
+  }
+  for (int q = q0 + gl; q < q1; q += G) {
+    const int2 fj = lfj[q];
+    const int f = fj.x;
+    const unsigned char ff = fflag[f];
+    if (!(ff & FF_ACTIVE) || (ff & (FF_BND1 | FF_BND2))) continue;
+    const bool own = fj.y >= 0;
+    const double tj = tlast[own ? fj.y : ~fj.y];
+    const double dtI = t_global - (own ? ti : tj), dtJ = t_global - (own ? tj : ti);
+    const double dt = smin(dtI, dtJ);
+    const R *l3 = lld + 3 * (size_t)q;
+    const R dr[3] = {l3[0], l3[1], l3[2]};
+    const R dtt = R(own ? dtI - 0.5 * dt : dtJ - 0.5 * dt);
+    R o[KH];
+#pragma unroll
+    for (int k = 0; k < KH; k++) o[k] = wi[k] + ((gx[k] * dr[0] + gy[k] * dr[1] + gz[k] * dr[2]) + gt[k] * dtt);
+    store_n<R, KH>(fst + 20 * (size_t)f + (own ? 0 : 10) + k0, o);
+  }
+}
+
 // Staged limiter: a block's CST cells (TPC threads each) first compute the
 // per-face records of passes 2 and 3 (the side's offset dr, the two time
 // offsets, the face and its flags) for all their faces together, into shared

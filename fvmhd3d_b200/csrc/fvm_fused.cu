@@ -23,6 +23,9 @@ namespace {
 // and each cell's walk over its ~16 faces is a chain of dependent loads;
 // split over 8 lanes it is two loads deep.
 constexpr int kCellGroup = 8;
+// Lanes per cell and primitive pair in the slope limiter (five pairs per
+// cell, so a cell takes 20 lanes).
+constexpr int kLimGroup = 4;
 
 // Polls of a grid barrier wait before it gives up (about 100 ns each): far
 // above the longest stage of a step this kernel runs (the sequential
@@ -140,9 +143,17 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   if (gt < 4) S->iscal[4 + gt] = 0;
   if (gt < 8) d.aflag[gt] = 0;
   // slope limiter over the involved cells
-  limiter_dev<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>(
-      n, P, S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec, (R *)d.tau,
-      (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, d.clist, 0, (const R *)d.lld, gt, gn);
+  {  // kLimGroup lanes per cell and primitive pair (a step with few cells,
+     // never every cell active: the limiter's first pass always runs)
+    constexpr int KH = CellTune<R>::KH_LIM, TPC = 10 / KH;
+    const double t_global = S->t_global;
+    const int units = TPC * S->ninv, gl4 = threadIdx.x & (kLimGroup - 1);
+    const unsigned gmask4 = ((1u << kLimGroup) - 1u) << ((threadIdx.x & 31) & ~(kLimGroup - 1));
+    for (int t = gt / kLimGroup; t < units; t += gn / kLimGroup)
+      limiter_group<R, KH, kLimGroup>(d.clist[t / TPC], (t % TPC) * KH, gl4, gmask4, t_global, d.off, d.lfj,
+                                      d.fflag, d.act, d.tlast, (const R *)d.Wrec, (R *)d.tau, (R *)d.fst,
+                                      (const R *)d.lld);
+  }
   FVM_GRID_SYNC();
   // compute_update: face fluxes over the active faces, then the cells
   corr_flux_dev<R, LM_EXACT>(nf, P, S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, d.tlast, (const R *)d.Wrec,

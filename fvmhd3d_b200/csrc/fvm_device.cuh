@@ -2030,22 +2030,25 @@ __global__ void k_rungs(int n, Params P, const Sched *FVM_RESTRICT S, int shared
 
 // distribute_fluid_update_data: primitives of the updated state
 template <typename R>
+__device__ __forceinline__ void wst_body(int i, const unsigned char *FVM_RESTRICT act,
+                                         const double *FVM_RESTRICT U, const double *FVM_RESTRICT volp,
+                                         R *FVM_RESTRICT Wst) {
+  if (!(act[i] & (A_ACTIVE | A_LNGB))) return;
+  double u[NF], W[NF];
+  load_n<double, NF>(U + 10 * (size_t)i, u);
+  to_primitive(u, volp[i], W);
+  R w[NF];
+#pragma unroll
+  for (int k = 0; k < NF; k++) w[k] = R(W[k]);
+  store_n<R, NF>(Wst + 10 * (size_t)i, w);
+}
+template <typename R>
 __device__ __forceinline__ void wst_dev(int n, const unsigned char *FVM_RESTRICT act, const double *FVM_RESTRICT U,
                       const double *FVM_RESTRICT volp, R *FVM_RESTRICT Wst, const int *FVM_RESTRICT clist,
                       const int *FVM_RESTRICT ninv, int gt0_, int gnt_) {
   const int cnt = clist ? *ninv : n;  // every cell, or in partial steps the involved-cell list
   const bool lst = clist && cnt != n;
-  for (int t = gt0_; t < cnt; t += gnt_) {
-    const int i = lst ? clist[t] : t;
-    if (!(act[i] & (A_ACTIVE | A_LNGB))) continue;
-    double u[NF], W[NF];
-    load_n<double, NF>(U + 10 * (size_t)i, u);
-    to_primitive(u, volp[i], W);
-    R w[NF];
-#pragma unroll
-    for (int k = 0; k < NF; k++) w[k] = R(W[k]);
-    store_n<R, NF>(Wst + 10 * (size_t)i, w);
-  }
+  for (int t = gt0_; t < cnt; t += gnt_) wst_body<R>(lst ? clist[t] : t, act, U, volp, Wst);
 }
 template <typename R>
 __global__ void k_wst(int n, const unsigned char *FVM_RESTRICT act, const double *FVM_RESTRICT U,

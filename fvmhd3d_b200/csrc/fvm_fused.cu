@@ -162,13 +162,16 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   {  // the cells: kCellGroup lanes per cell, the walk over its faces split among them
     const double t_global = S->t_global;
     const int ninv = S->ninv;
-    for (int t = gt / kCellGroup; t < ninv; t += gn / kCellGroup)
-      corr_cell_group<R, kCellGroup>(d.clist[t], gl, gmask, t_global, P, d.off, d.lfj, d.cvol, d.act, d.bnd, d.pos,
-                                     d.tlast, d.volp, (const R *)d.Wrec, (const R *)d.tau, (const R *)d.fcon,
-                                     d.fcode, d.U, d.dU, d.stepdU, d.counters, d.divb);
+    for (int t = gt / kCellGroup; t < ninv; t += gn / kCellGroup) {
+      const int c = d.clist[t];
+      corr_cell_group<R, kCellGroup>(c, gl, gmask, t_global, P, d.off, d.lfj, d.cvol, d.act, d.bnd, d.pos, d.tlast,
+                                     d.volp, (const R *)d.Wrec, (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U,
+                                     d.dU, d.stepdU, d.counters, d.divb);
+      // compute_pvel of the same cell (its own updated state; no stage
+      // before the timestep reads a velocity)
+      if (gl == 0) pvel_body(c, P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel);
+    }
   }
-  FVM_GRID_SYNC();
-  pvel_dev(n, P, d.act, d.bnd, d.U, d.volp, d.cvol, d.ccen, d.pos, d.vel, d.clist, &S->ninv, gt, gn);
   FVM_GRID_SYNC();
   // compute_timesteps(false): CFL timestep and its minimum, halving,
   // adjust_timesteps (marks, parallel replays, sequential fallback), rungs
@@ -190,31 +193,52 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
   adjust_init_dev(n, d.off, d.lfj, d.act, &S->iscal[4], d.dtl, d.dt0, d.rdv, d.wrv, d.aflag, d.clist, &S->ninv, gt,
                   gn);
   FVM_GRID_SYNC();
+  bool settled = false;
   for (int k = 0; k < ADJ_ITERS; k++) {
     adjust_replay_dev(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv, d.wrv, d.dtl, d.aflag, d.awork, 0, gt,
                       gn, d.clist, S->ninv);
     FVM_GRID_SYNC();
     // stop once replay k changed nothing (settled) or every replay has run
-    const bool settled = vload(&d.aflag[k % 3]) == 0;
-    if (settled || k + 1 >= ADJ_ITERS) {
-      if (settled && gt == 0) d.aflag[5] = 1;
-      break;
+    settled = vload(&d.aflag[k % 3]) == 0;
+    if (settled || k + 1 >= ADJ_ITERS) break;
+  }
+  // adjust_restore_dev's decision, taken by every block from the same flags:
+  // the sequential sweep runs from the initial timesteps when the replays did
+  // not settle; otherwise the replays' timesteps stand and no barrier is
+  // needed before the rungs
+  {
+    const bool fallback = !settled && vload(&d.aflag[(ADJ_ITERS - 1) % 3]) != 0;
+    if (gt == 0) {
+      if (settled) d.aflag[5] = 1;
+      S->iscal[6] = vload(&d.aflag[3]);
+      S->iscal[7] = fallback ? 1 : 0;
+      if (fallback) d.aflag[4] = 1;
+    }
+    if (fallback) {
+      const int ninv = S->ninv;
+      for (int t = gt; t < ninv; t += gn) {
+        const int u = d.clist[t];
+        if (d.act[u] & (A_ACTIVE | A_LNGB)) d.dtl[u] = d.dt0[u];
+      }
+      FVM_GRID_SYNC();
+      if (blockIdx.x == 0) {  // not settled: the sequential sweep
+        compact_sites(d.clist, S->ninv, d.act0, d.alist);
+        __syncthreads();
+        if (threadIdx.x == 0) adjust_seq_dev(d.off, d.lnk, d.s12, d.alist, &S->iscal[5], &d.aflag[4], d.dtl);
+      }
+      FVM_GRID_SYNC();
     }
   }
-  FVM_GRID_SYNC();
-  adjust_restore_dev(n, d.act, d.dt0, d.dtl, d.aflag, &S->iscal[6], d.clist, &S->ninv, gt, gn);
-  FVM_GRID_SYNC();
-  if (vload(&d.aflag[4]) && blockIdx.x == 0) {  // not settled: the sequential sweep
-    compact_sites(d.clist, S->ninv, d.act0, d.alist);
-    __syncthreads();
-    if (threadIdx.x == 0) adjust_seq_dev(d.off, d.lnk, d.s12, d.alist, &S->iscal[5], &d.aflag[4], d.dtl);
+  {  // rungs (and correct()) and distribute_fluid_update_data: both per cell, own data only
+    const double t_global = S->t_global;
+    const int min_rung = S->min_rung, ninv = S->ninv;
+    for (int t = gt; t < ninv; t += gn) {
+      const int i = d.clist[t];
+      rungs_body<R>(i, t_global, min_rung, P, 0, d.act, d.hash, d.dtl, &S->dtmin, d.rung, d.tlast, d.tend,
+                    (R *)d.Wrec, S->iscal, d.vel, d.opos, d.ovel);
+      wst_body<R>(i, d.act, d.U, d.volp, (R *)d.Wst);
+    }
   }
-  FVM_GRID_SYNC();
-  rungs_dev<R>(n, P, S, 0, d.act, d.hash, d.dtl, &S->dtmin, d.rung, d.tlast, d.tend, (R *)d.Wrec, S->iscal, d.vel,
-               d.opos, d.ovel, d.clist, gt, gn);
-  FVM_GRID_SYNC();
-  // distribute_fluid_update_data, compute_update0, compute_reconstruction
-  wst_dev<R>(n, d.act, d.U, d.volp, (R *)d.Wst, d.clist, &S->ninv, gt, gn);
   FVM_GRID_SYNC();
   pred_flux_dev<R, LM_EXACT>(nf, P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, (const R *)d.Wst, (R *)d.fcon2,
                              d.fcode2, S, d.rung, a.lb, d.flist, 1, gt, gn);

@@ -189,6 +189,10 @@ struct fvm_ctx {
   int inc_max = -1;
   int fused_bpsm = 0;          // its resident blocks per SM (queried outside capture)
   cudaStream_t aux = nullptr;  // captures the branches of the fused/stage choice
+  // fvm_step_host: the copy stream and the events that order its copies
+  // against the stage kernels (created on first use)
+  cudaStream_t cpy = nullptr;
+  cudaEvent_t hev[5] = {};
   unsigned *gbar = nullptr;    // its grid barrier
   int *gerr = nullptr;         // its error bits
   std::string err;
@@ -357,6 +361,9 @@ void fvm_destroy(fvm_ctx *c) {
   cudaEventDestroy(c->ev0);
   cudaEventDestroy(c->ev1);
   if (c->aux) cudaStreamDestroy(c->aux);
+  if (c->cpy) cudaStreamDestroy(c->cpy);
+  for (cudaEvent_t e : c->hev)
+    if (e) cudaEventDestroy(e);
   cudaStreamDestroy(c->st);
   delete c;
 }
@@ -876,7 +883,7 @@ static int enq_limiter(fvm_ctx *c) {
 
 static int mlp_launch_dev(fvm_ctx *c, int nmax, const int *n_dev, const __half *X, float *Y);
 
-static int enq_update(fvm_ctx *c) {
+static int enq_corr_flux(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_CORR_FLUX);
   const LearnBuf &lb = c->lb;
@@ -899,6 +906,11 @@ static int enq_update(fvm_ctx *c) {
 #undef CORR_FLUX
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_FLUX);
+  return 0;
+}
+
+static int enq_corr_cell(fvm_ctx *c) {
+  Dev &d = c->d;
   kt_begin(c, KT_CORR_CELL);
   BULK(k_corr_cell<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
                                                           d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
@@ -908,6 +920,12 @@ static int enq_update(fvm_ctx *c) {
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_CELL);
   return 0;
+}
+
+// compute_update: the face fluxes, then the cells.
+static int enq_update(fvm_ctx *c) {
+  const int rc = enq_corr_flux(c);
+  return rc ? rc : enq_corr_cell(c);
 }
 
 static int enq_pvel(fvm_ctx *c) {
@@ -1282,6 +1300,103 @@ int fvm_step(fvm_ctx *c, int shared) {
   if ((rc = read_sched(c))) return rc;
   if ((rc = check_fused_errors(c))) return rc;
   kt_collect(c);
+  cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
+  c->max_rung = c->hS.iscal[0];
+  if ((rc = check_sched_errors(c))) return rc;
+  return c->hS.iscal[1];
+}
+
+// fvm_set_state + fvm_step + fvm_get_state in one call, the host arrays read
+// and then overwritten in place, with the copies of U and dU on a second
+// stream overlapping the stage kernels: in before the compute_update cell
+// pass needs them, out as soon as that pass has finished them (the later
+// stages do not write U or dU), then the velocities after compute_pvel and
+// tlast after the rungs; rung, tend and the reconstruction after the step.
+// Always the stage kernels.
+int fvm_step_host(fvm_ctx *c, int shared, unsigned long long tsys_ticks, double *vel, double *tlast, double *tend,
+                  int *rung, double *U, double *dU, double *wrec) {
+  if (!c || !c->have_mesh) return FVM_ENOMESH;
+  if (c->in_step) { c->err = "fvm_step_host: inside a step"; return FVM_EINVAL; }
+  if (!vel || !tlast || !tend || !rung || !U || !dU || !wrec) {
+    c->err = "fvm_step_host: every state array is required";
+    return FVM_EINVAL;
+  }
+  for (int i = 0; i < c->n; i++)  // as fvm_set_state: nothing is uploaded when a rung is out of range
+    if (rung[i] < 0 || rung[i] >= RUNGMAX - 1) { c->err = "fvm_step_host: rung out of range"; return FVM_ERANGE; }
+  CK(cudaSetDevice(c->device));
+  if (!c->cpy) {
+    CK(cudaStreamCreateWithFlags(&c->cpy, cudaStreamNonBlocking));
+    for (cudaEvent_t &e : c->hev) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  }
+  Dev &d = c->d;
+  const size_t n = c->n;
+  cudaStream_t st = c->st, cs = c->cpy;
+  const size_t wbytes = 50 * n * sizeof(double);
+  double *wtmp = nullptr;  // the FP32 bulk path converts the reconstruction on the device
+  // the inputs the first stages read, on the compute stream
+  CK(cudaEventRecord(c->ev0, st));
+  CK(cudaMemcpyAsync(d.rung, rung, n * sizeof(int), cudaMemcpyHostToDevice, st));
+  if (!c->fp32) {
+    CK(cudaMemcpyAsync(d.Wrec, wrec, wbytes, cudaMemcpyHostToDevice, st));
+  } else {
+    CK(cudaMallocAsync(&wtmp, wbytes, st));
+    CK(cudaMemcpyAsync(wtmp, wrec, wbytes, cudaMemcpyHostToDevice, st));
+    k_convert<double, float><<<nblk(50LL * n, 256), 256, 0, st>>>(50LL * n, wtmp, (float *)d.Wrec);
+    LAUNCH_CHECK();
+  }
+  CK(cudaMemcpyAsync(d.tlast, tlast, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d.vel, vel, 3 * n * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d.tend, tend, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(d.volp, d.cvol, n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+  k_sched_set<<<1, 1, 0, st>>>(c->P, d.S, tsys_ticks, 0);
+  LAUNCH_CHECK();
+  int rc = enqueue_maxrung(c);
+  if (rc) return rc;
+  // U and dU on the copy stream once the early inputs are in (the two would
+  // only share the link), while the step's first stages run
+  CK(cudaEventRecord(c->hev[0], st));
+  CK(cudaStreamWaitEvent(cs, c->hev[0], 0));
+  CK(cudaMemcpyAsync(d.U, U, 10 * n * sizeof(double), cudaMemcpyHostToDevice, cs));
+  CK(cudaMemcpyAsync(d.dU, dU, 14 * n * sizeof(double), cudaMemcpyHostToDevice, cs));
+  CK(cudaEventRecord(c->hev[1], cs));
+  c->use_flist = shared ? 0 : 1;
+  if ((rc = enq_begin(c))) return rc;
+  if ((rc = enq_limiter(c))) return rc;
+  // the learned flux's positivity gate reads the cells' U in the flux pass
+  if (c->learn_mode == 1) CK(cudaStreamWaitEvent(st, c->hev[1], 0));
+  if ((rc = enq_corr_flux(c))) return rc;
+  CK(cudaStreamWaitEvent(st, c->hev[1], 0));
+  if ((rc = enq_corr_cell(c))) return rc;
+  CK(cudaEventRecord(c->hev[2], st));
+  CK(cudaStreamWaitEvent(cs, c->hev[2], 0));
+  CK(cudaMemcpyAsync(U, d.U, 10 * n * sizeof(double), cudaMemcpyDeviceToHost, cs));
+  CK(cudaMemcpyAsync(dU, d.dU, 14 * n * sizeof(double), cudaMemcpyDeviceToHost, cs));
+  if ((rc = enq_pvel(c))) return rc;
+  CK(cudaEventRecord(c->hev[3], st));
+  CK(cudaStreamWaitEvent(cs, c->hev[3], 0));
+  CK(cudaMemcpyAsync(vel, d.vel, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, cs));
+  if ((rc = enq_timesteps(c, shared))) return rc;
+  CK(cudaEventRecord(c->hev[4], st));
+  CK(cudaStreamWaitEvent(cs, c->hev[4], 0));
+  CK(cudaMemcpyAsync(tlast, d.tlast, n * sizeof(double), cudaMemcpyDeviceToHost, cs));
+  if ((rc = enq_collect(c))) return rc;
+  if ((rc = enq_update0(c))) return rc;
+  if ((rc = enq_recon(c))) return rc;
+  if ((rc = enq_end(c, shared))) return rc;
+  CK(cudaMemcpyAsync(rung, d.rung, n * sizeof(int), cudaMemcpyDeviceToHost, st));
+  CK(cudaMemcpyAsync(tend, d.tend, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (!c->fp32) {
+    CK(cudaMemcpyAsync(wrec, d.Wrec, wbytes, cudaMemcpyDeviceToHost, st));
+  } else {
+    k_convert<float, double><<<nblk(50LL * n, 256), 256, 0, st>>>(50LL * n, (const float *)d.Wrec, wtmp);
+    LAUNCH_CHECK();
+    CK(cudaMemcpyAsync(wrec, wtmp, wbytes, cudaMemcpyDeviceToHost, st));
+    CK(cudaFreeAsync(wtmp, st));
+  }
+  CK(cudaEventRecord(c->ev1, st));
+  CK(cudaStreamSynchronize(cs));
+  c->have_state = true;
+  if ((rc = read_sched(c))) return rc;
   cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
   c->max_rung = c->hS.iscal[0];
   if ((rc = check_sched_errors(c))) return rc;

@@ -330,6 +330,27 @@ class System:
         self._check(self.L.fvm_set_state(self.h, *[_p(a) for a in conv], ctypes.c_ulonglong(tsys_ticks)),
                     "fvm_set_state")
 
+    STATE_ARRAYS = (("vel", np.float64, 3), ("tlast", np.float64, 1), ("tend", np.float64, 1),
+                    ("rung", np.int32, 1), ("U", np.float64, 10), ("dU", np.float64, 14),
+                    ("wrec", np.float64, 50))
+
+    def step_host(self, state, shared=True, tsys_ticks=None) -> int:
+        """One step on host-owned state (fvm_step_host): `state` maps vel,
+        tlast, tend, rung, U, dU and wrec to C-contiguous arrays of the
+        right type (pinned for the copies to overlap), read and then
+        overwritten with the stepped state.  tsys_ticks defaults to the
+        context's clock.  Returns the active cell count."""
+        n = self.mesh.ncell
+        for k, t, w in self.STATE_ARRAYS:
+            a = state[k]
+            if a.dtype != t or not a.flags["C_CONTIGUOUS"] or a.size != n * w:
+                raise ValueError(f"step_host: {k} must be a C-contiguous {np.dtype(t).name} array of {n * w}")
+        ticks = self.tsys_ticks if tsys_ticks is None else int(tsys_ticks)
+        r = self.L.fvm_step_host(self.h, 1 if shared else 0, ctypes.c_ulonglong(ticks),
+                                 *[_p(state[k]) for k, _, _ in self.STATE_ARRAYS])
+        self._check(r, "fvm_step_host")
+        return r
+
     def active_faces(self) -> np.ndarray:
         n = ctypes.c_int(0)
         self._check(self.L.fvm_get_active_faces(self.h, None, ctypes.byref(n)), "fvm_get_active_faces")

@@ -148,6 +148,20 @@ int fvm_end_step(fvm_ctx *c, int shared);
  * end_step.  Returns the number of active cells. */
 int fvm_step(fvm_ctx *c, int shared);
 
+/* fvm_set_state + fvm_step + fvm_get_state in one call: the step reads the
+ * host state (vel[3n], tlast[n], tend[n], rung[n], U[10n], dU[14n],
+ * wrec[50n], the system clock tsys_ticks as fvm_set_state takes it) and
+ * writes the stepped state back into the same arrays.  The copies of U and
+ * dU run on a second stream, overlapped with the stage kernels (in while the
+ * face fluxes are computed, out while the later stages run), and the host
+ * waits once, at the end.  The host arrays should be pinned.  A rung outside
+ * [0, 31) on input returns FVM_ERANGE before anything is uploaded.  Always the stage
+ * kernels; no counterpart in the reference (a drop-in that keeps the
+ * reference's host arrays calls it once per fluid step).  Returns the active
+ * cell count. */
+int fvm_step_host(fvm_ctx *c, int shared, unsigned long long tsys_ticks, double *vel, double *tlast, double *tend,
+                  int *rung, double *U, double *dU, double *wrec);
+
 /* nsteps full steps replayed from one captured CUDA graph (the scheduler
  * runs on the device, so there is no host round trip between steps).
  * Returns the summed number of active cells; faces_out (may be NULL)

@@ -89,3 +89,28 @@ def test_list_building_setting_rejects_bad_values():
     s.set_list_building(-1)
     s.run(2, shared=True)  # global steps build no lists
     assert s.incremental_steps == 0
+
+
+def test_incremental_lists_with_the_learned_flux():
+    """Learned-flux mode on individual timesteps (deferring pass, network,
+    finishing pass over the active-face list): the faces' slots follow the
+    list's order, but each face's network row and flux are its own, so the
+    incremental lists give the bits of the pass over every face."""
+    import fvmhd3d_b200 as F
+    from fvmhd3d_b200 import learned as L
+    model = L.load_model()
+    m, W = contrast_blast(12, 5)
+    a = gpu_system(m, W, precision=F.FVM_PREC_FP32)
+    b = gpu_system(m, W, precision=F.FVM_PREC_FP32)
+    for s in (a, b):
+        L.apply(s, model)
+        s.set_flux_mode(1, judge=4, **L.GATE)
+    a.set_list_building(0)
+    for _ in range(10):
+        assert a.step(shared=False) == b.step(shared=False)
+    assert b.incremental_steps >= 2
+    same_bits(a, b)
+    sa, sb = a.learn_stats(), b.learn_stats()
+    assert sa["deferred"] > 0
+    for k in ("deferred", "fallback", "judged", "positivity_fallback"):  # counts (the error sums are atomics)
+        assert sa[k] == sb[k], k

@@ -51,7 +51,7 @@ struct Dev {
   int *clist, *cbcount; // ordered list of the step's active and neighbour cells, block offsets (partial steps)
   int *ilist;           // the step's active cells, unordered (incremental list building)
   unsigned *ibits;      // one bit per cell, zero between steps (incremental list building)
-  int *icount;          // per block of k_inc_count: its involved cells (INC_BLOCKS)
+  int *icount;          // per block of k_inc_count / k_site_count: its count (SITE_BLOCKS)
   unsigned char *bnb;   // per cell: 1 when a neighbour is a boundary cell (set with the boundary codes)
   int2 *lfj;            // per link: face id, neighbour (~j when the cell is s2)
   int *lsort, *lpart;   // per link: links of the cell by ascending neighbour; the same face's other link
@@ -1909,8 +1909,99 @@ __global__ void k_adjust_replay(int n, int kparam, const int *FVM_RESTRICT off, 
                                 const int *FVM_RESTRICT lsort, const int *FVM_RESTRICT lpart,
                                 const unsigned char *FVM_RESTRICT act, const double *FVM_RESTRICT dt0,
                                 double *FVM_RESTRICT rdv, double *FVM_RESTRICT wrv, double *FVM_RESTRICT dtl,
-                                int *FVM_RESTRICT aflag, unsigned char *FVM_RESTRICT work, int kdev) {
-  adjust_replay_dev(n, kparam, off, lfj, lsort, lpart, act, dt0, rdv, wrv, dtl, aflag, work, kdev, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+                                int *FVM_RESTRICT aflag, unsigned char *FVM_RESTRICT work, int kdev,
+                                const int *FVM_RESTRICT ulist, const int *FVM_RESTRICT ucount) {
+  adjust_replay_dev(n, kparam, off, lfj, lsort, lpart, act, dt0, rdv, wrv, dtl, aflag, work, kdev,
+                    blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x, ulist, ulist ? *ucount : 0);
+}
+
+// A partial step's adjust_timesteps work arrays, cleared for its involved
+// cells only: every mark, work list and replay write of the step lands on
+// one of them, and every reader walks them only (the replays through their
+// list, the site compaction below).
+__global__ void k_adjust_clear(int n, const int *FVM_RESTRICT clist, const int *FVM_RESTRICT ninv,
+                               unsigned char *FVM_RESTRICT hash, unsigned char *FVM_RESTRICT act0,
+                               unsigned char *FVM_RESTRICT work) {
+  const int cnt = *ninv;
+  const bool lst = cnt != n;  // every cell involved: the list is the identity
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < cnt; t += gridDim.x * blockDim.x) {
+    const int i = lst ? clist[t] : t;
+    hash[i] = 0;
+    act0[i] = 0;
+    work[i] = 0;
+    work[(size_t)n + i] = 0;
+  }
+}
+
+// The active non-boundary sites (act0) in ascending order from the ascending
+// involved-cell list, in two launches of SITE_BLOCKS blocks over contiguous
+// chunks of it: k_site_count counts each chunk's sites, k_site_place writes
+// them after the counts of the chunks before (alist, count in *nsites).
+// Enough blocks that a chunk of a step with every cell involved is a few
+// rounds of the block.
+constexpr int SITE_BLOCKS = 512;
+__device__ __forceinline__ void site_chunk(int cnt, int &t0, int &t1) {
+  const int C = (cnt + SITE_BLOCKS - 1) / SITE_BLOCKS;
+  t0 = blockIdx.x * C;
+  t1 = min(cnt, t0 + C);
+}
+__global__ void __launch_bounds__(256) k_site_count(int n, const int *FVM_RESTRICT clist,
+                                                    const int *FVM_RESTRICT ninv,
+                                                    const unsigned char *FVM_RESTRICT act0, int *FVM_RESTRICT bcnt) {
+  __shared__ int wsum[8];
+  const int cnt = *ninv;
+  const bool lst = cnt != n;
+  int t0, t1;
+  site_chunk(cnt, t0, t1);
+  int c = 0;
+  for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) c += act0[lst ? clist[t] : t] != 0;
+  const int tot = block_sum(c, wsum);
+  if (threadIdx.x == 0) bcnt[blockIdx.x] = tot;
+}
+__global__ void __launch_bounds__(256) k_site_place(int n, const int *FVM_RESTRICT clist,
+                                                    const int *FVM_RESTRICT ninv,
+                                                    const unsigned char *FVM_RESTRICT act0,
+                                                    const int *FVM_RESTRICT bcnt, int *FVM_RESTRICT alist,
+                                                    int *FVM_RESTRICT nsites) {
+  __shared__ int wsum[8], base;
+  if (threadIdx.x < 32) {
+    int before = 0, all = 0;
+    for (int b = threadIdx.x; b < SITE_BLOCKS; b += 32) {
+      const int v = bcnt[b];
+      all += v;
+      before += b < (int)blockIdx.x ? v : 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      before += __shfl_xor_sync(0xffffffffu, before, o);
+      all += __shfl_xor_sync(0xffffffffu, all, o);
+    }
+    if (threadIdx.x == 0) {
+      base = before;
+      if (blockIdx.x == 0) *nsites = all;
+    }
+  }
+  __syncthreads();
+  const int cnt = *ninv;
+  const bool lst = cnt != n;
+  int t0, t1;
+  site_chunk(cnt, t0, t1);
+  // the chunk in rounds of blockDim entries, each placed by a block scan
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int r0 = t0; r0 < t1; r0 += blockDim.x) {
+    const int t = r0 + threadIdx.x;
+    const int i = t < t1 ? (lst ? clist[t] : t) : -1;
+    const bool f = i >= 0 && act0[i] != 0;
+    const unsigned bal = __ballot_sync(0xffffffffu, f);
+    if (lane == 0) wsum[wid] = __popc(bal);
+    __syncthreads();
+    int o = base;
+    for (int w = 0; w < wid; w++) o += wsum[w];
+    if (f) alist[o + __popc(bal & ((1u << lane) - 1u))] = i;
+    __syncthreads();
+    if (threadIdx.x == 0)
+      for (int w = 0; w < (int)(blockDim.x >> 5); w++) base += wsum[w];
+    __syncthreads();
+  }
 }
 
 // In a captured step the replays run as the body of a conditional WHILE

@@ -406,7 +406,7 @@ static int alloc_mesh(fvm_ctx *c, long long ncell, long long nface, long long nl
   rc |= dalloc(c, &d.ilist, ncell);
   const long long ibits_words = (ncell + 31) / 32;
   rc |= dalloc(c, &d.ibits, ibits_words);
-  rc |= dalloc(c, &d.icount, INC_BLOCKS);
+  rc |= dalloc(c, &d.icount, std::max(INC_BLOCKS, SITE_BLOCKS));
   rc |= dalloc(c, &d.bnb, ncell);
   rc |= dalloc_bytes(c, &d.tau, 10 * c->rb * (size_t)ncell);
   rc |= dalloc_bytes(c, &d.fcon, 14 * c->rb * (size_t)nface);
@@ -416,7 +416,11 @@ static int alloc_mesh(fvm_ctx *c, long long ncell, long long nface, long long nl
   if (c->keep_step_dU) rc |= dalloc(c, &d.stepdU, 14 * (size_t)ncell);
   rc |= dalloc(c, &d.S, 1); rc |= dalloc(c, &d.counters, 4);
   if (rc) { free_all(c); return FVM_ENOMEM; }
-  if (cudaMemset(d.ibits, 0, sizeof(unsigned) * ibits_words) != cudaSuccess) {  // zero between steps
+  // zero between steps (ibits), and cleared per step only where a step
+  // works (the adjust_timesteps work arrays of partial steps)
+  if (cudaMemset(d.ibits, 0, sizeof(unsigned) * ibits_words) != cudaSuccess ||
+      cudaMemset(d.hash, 0, ncell) != cudaSuccess || cudaMemset(d.act0, 0, ncell) != cudaSuccess ||
+      cudaMemset(d.awork, 0, 2 * ncell) != cudaSuccess) {
     free_all(c);
     return FVM_ENOMEM;
   }
@@ -949,20 +953,32 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
   if (!shared) {
     k_halve<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.act, &d.S->dtmin, d.dtl, cl, &d.S->ninv);
     LAUNCH_CHECK();
-    CK(cudaMemsetAsync(d.hash, 0, n, c->st));
     CK(cudaMemsetAsync(&d.S->iscal[4], 0, 4 * sizeof(int), c->st));
-    CK(cudaMemsetAsync(d.awork, 0, 2 * (size_t)n, c->st));
-    CK(cudaMemsetAsync(d.act0, 0, n, c->st));
+    if (cl) {  // the work arrays and the site list over the involved cells only
+      k_adjust_clear<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, cl, &d.S->ninv, d.hash, d.act0, d.awork);
+      LAUNCH_CHECK();
+    } else {
+      CK(cudaMemsetAsync(d.hash, 0, n, c->st));
+      CK(cudaMemsetAsync(d.awork, 0, 2 * (size_t)n, c->st));
+      CK(cudaMemsetAsync(d.act0, 0, n, c->st));
+    }
     k_adjust_mark<<<sgrid(c, n, 128), 128, 0, c->st>>>(n, d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash,
                                                       &d.S->iscal[4], d.act0, d.awork, cl, &d.S->ninv);
     LAUNCH_CHECK();
-    const int nb = (int)((n + CB - 1) / CB);
-    k_count_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount);
-    LAUNCH_CHECK();
-    k_scan_counts<<<1, CB, 0, c->st>>>(nb, d.bcount, &d.S->iscal[5]);
-    LAUNCH_CHECK();
-    k_place_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount, d.alist);
-    LAUNCH_CHECK();
+    if (cl) {
+      k_site_count<<<SITE_BLOCKS, 256, 0, c->st>>>(n, cl, &d.S->ninv, d.act0, d.icount);
+      LAUNCH_CHECK();
+      k_site_place<<<SITE_BLOCKS, 256, 0, c->st>>>(n, cl, &d.S->ninv, d.act0, d.icount, d.alist, &d.S->iscal[5]);
+      LAUNCH_CHECK();
+    } else {
+      const int nb = (int)((n + CB - 1) / CB);
+      k_count_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount);
+      LAUNCH_CHECK();
+      k_scan_counts<<<1, CB, 0, c->st>>>(nb, d.bcount, &d.S->iscal[5]);
+      LAUNCH_CHECK();
+      k_place_flags<<<nb, CB, 0, c->st>>>(n, d.act0, d.bcount, d.alist);
+      LAUNCH_CHECK();
+    }
 #if FVM_ADJUST_REPLAY
     CK(cudaMemsetAsync(d.aflag, 0, 8 * sizeof(int), c->st));
     k_adjust_init<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.act, &d.S->iscal[4], d.dtl, d.dt0,
@@ -989,8 +1005,9 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
       CK(cudaGraphAddNode(&cn, g, deps, nd, &cp));
       cudaGraph_t body = cp.conditional.phGraph_out[0];
       int k0 = 0, kdev = 1;
+      const int *ulist = cl, *ucount = cl ? &d.S->ninv : nullptr;  // the replays walk the involved cells
       void *ra[] = {(void *)&n, &k0, &d.off, &d.lfj, &d.lsort, &d.lpart, &d.act, &d.dt0, &d.rdv, &d.wrv, &d.dtl,
-                    &d.aflag, &d.awork, &kdev};
+                    &d.aflag, &d.awork, &kdev, &ulist, &ucount};
       cudaKernelNodeParams kp = {};
       kp.func = (void *)k_adjust_replay;
       kp.gridDim = dim3(rgrid);
@@ -1010,7 +1027,7 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
     } else {
       for (int k = 0; k < ADJ_ITERS; k++) {
         k_adjust_replay<<<rgrid, 128, 0, c->st>>>(n, k, d.off, d.lfj, d.lsort, d.lpart, d.act, d.dt0, d.rdv, d.wrv,
-                                                  d.dtl, d.aflag, d.awork, 0);
+                                                  d.dtl, d.aflag, d.awork, 0, cl, cl ? &d.S->ninv : nullptr);
         LAUNCH_CHECK();
       }
     }

@@ -1820,6 +1820,9 @@ constexpr int ADJ_ITERS = 24;
 
 __device__ __forceinline__ int lfj_nb(int2 fj) { return fj.y >= 0 ? fj.y : ~fj.y; }
 
+// G consecutive lanes per cell (the link entries are independent of one
+// another), gt0_ and gnt_ in lanes.
+template <int G = 1>
 __device__ __forceinline__ void adjust_init_dev(int n, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
                               const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT ndirty,
                               const double *FVM_RESTRICT dtl, double *FVM_RESTRICT dt0, double *FVM_RESTRICT rdv,
@@ -1829,12 +1832,13 @@ __device__ __forceinline__ void adjust_init_dev(int n, const int *FVM_RESTRICT o
   if (gt0_ == 0) aflag[2] = 1;  // replay 0 runs
   const int cnt_ = clist ? *ninv : n;
   const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
-  for (int t_ = gt0_; t_ < cnt_; t_ += gnt_) {
+  const int gl = gt0_ % G;
+  for (int t_ = gt0_ / G; t_ < cnt_; t_ += gnt_ / G) {
     const int u = lst ? clist[t_] : t_;
     if (!(act[u] & (A_ACTIVE | A_LNGB))) continue;
     const double du = dtl[u];
-    dt0[u] = du;
-    for (int q = off[u]; q < off[u + 1]; q++) {
+    if (gl == 0) dt0[u] = du;
+    for (int q = off[u] + gl; q < off[u + 1]; q += G) {
       const int v = lfj_nb(lfj[q]);
       rdv[q] = (act[v] & (A_ACTIVE | A_LNGB)) ? dtl[v] : du;
       wrv[q] = du;
@@ -1846,7 +1850,8 @@ __global__ void k_adjust_init(int n, const int *FVM_RESTRICT off, const int2 *FV
                               const double *FVM_RESTRICT dtl, double *FVM_RESTRICT dt0, double *FVM_RESTRICT rdv,
                               double *FVM_RESTRICT wrv, int *FVM_RESTRICT aflag, const int *FVM_RESTRICT clist,
                               const int *FVM_RESTRICT ninv) {
-  adjust_init_dev(n, off, lfj, act, ndirty, dtl, dt0, rdv, wrv, aflag, clist, ninv, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+  adjust_init_dev<8>(n, off, lfj, act, ndirty, dtl, dt0, rdv, wrv, aflag, clist, ninv,
+                     blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
 }
 
 __device__ __forceinline__ void adjust_replay_dev(int n, int kparam, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,

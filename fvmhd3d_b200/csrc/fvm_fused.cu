@@ -190,8 +190,8 @@ __global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_rung_step(FusedStep a
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(&S->iscal[5], cnt);
   }
   FVM_GRID_SYNC();
-  adjust_init_dev(n, d.off, d.lfj, d.act, &S->iscal[4], d.dtl, d.dt0, d.rdv, d.wrv, d.aflag, d.clist, &S->ninv, gt,
-                  gn);
+  adjust_init_dev<kCellGroup>(n, d.off, d.lfj, d.act, &S->iscal[4], d.dtl, d.dt0, d.rdv, d.wrv, d.aflag, d.clist,
+                              &S->ninv, gt, gn);
   FVM_GRID_SYNC();
   bool settled = false;
   for (int k = 0; k < ADJ_ITERS; k++) {

@@ -1475,39 +1475,11 @@ __device__ __forceinline__ void atomic_min_pos(double *addr, double v) {
   atomicMin((unsigned long long *)addr, (unsigned long long)__double_as_longlong(v));
 }
 
-// compute_timesteps(false) first loops (MPI/compute_timestep.cpp:78-96); the
-// global minimum is reduced per warp before one atomic per warp
-__device__ __forceinline__ void timestep_dev(int n, Params P, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
-                           const unsigned char *FVM_RESTRICT act,
-                           const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT U,
-                           const double *FVM_RESTRICT volp, const double *FVM_RESTRICT vel,
-                           const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast,
-                           const double *FVM_RESTRICT tend, double *FVM_RESTRICT dtl,
-                           double *FVM_RESTRICT dmin, const int *FVM_RESTRICT clist, const int *FVM_RESTRICT ninv, int gt0_, int gnt_) {
-  // every cell, or in partial steps the involved-cell list (the dt of any
-  // other cell is never read)
-  double vmin = FVM_HUGE;
-  const int cnt_ = clist ? *ninv : n;
-  const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
-  for (int t_ = gt0_; t_ < cnt_; t_ += gnt_) {
-    const int i = lst ? clist[t_] : t_;
-    const unsigned char a = act[i];
-    if (!(a & (A_ACTIVE | A_LNGB))) {
-      dtl[i] = FVM_HUGE;
-    } else if (!(a & A_ACTIVE)) {
-      dtl[i] = (tend[i] - tlast[i]) * (bnd[i] != NO_BOUNDARY ? -1.0 : 1.0);
-    } else {
-      const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
-                              cell_timestep(P, i, true, off, lfj, bnd, U, volp, vel));
-      vmin = smin(vmin, dti);
-      dtl[i] = bnd[i] != NO_BOUNDARY ? -1.0 * dti : dti;
-    }
-  }
-  for (int o = 16; o > 0; o >>= 1) vmin = smin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
-  if ((threadIdx.x & 31) == 0 && vmin < FVM_HUGE) atomic_min_pos(dmin, vmin);
-}
-// The same with G lanes per cell over the involved-cell list (the group's
-// first lane writes the cell's dt and takes part in the minimum).
+// compute_timesteps(false) first loops (MPI/compute_timestep.cpp:78-96) with
+// G lanes per cell (cell_timestep's faces split among them), over the
+// involved-cell list or every cell; the group's first lane writes the cell's
+// dt and takes part in the global minimum, reduced per warp before one
+// atomic per warp.
 template <int G>
 __device__ __forceinline__ void timestep_group(Params P, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
                            const unsigned char *FVM_RESTRICT act,
@@ -1516,10 +1488,13 @@ __device__ __forceinline__ void timestep_group(Params P, const int *FVM_RESTRICT
                            const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast,
                            const double *FVM_RESTRICT tend, double *FVM_RESTRICT dtl,
                            double *FVM_RESTRICT dmin, const int *FVM_RESTRICT clist, int ninv, int gl,
-                           unsigned gmask, int g0, int gn) {
+                           unsigned gmask, int g0, int gn, int n = 0) {
+  // clist and its count ninv, or (clist null) every one of the n cells
   double vmin = FVM_HUGE;
-  for (int t_ = g0; t_ < ninv; t_ += gn) {
-    const int i = clist[t_];
+  const int cnt = clist ? ninv : n;
+  const bool lst = clist && cnt != n;  // every cell involved: the list is the identity
+  for (int t_ = g0; t_ < cnt; t_ += gn) {
+    const int i = lst ? clist[t_] : t_;
     const unsigned char a = act[i];
     if (!(a & (A_ACTIVE | A_LNGB))) {
       if (gl == 0) dtl[i] = FVM_HUGE;
@@ -1545,7 +1520,12 @@ __global__ void k_timestep(int n, Params P, const int *FVM_RESTRICT off, const i
                            const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast,
                            const double *FVM_RESTRICT tend, double *FVM_RESTRICT dtl,
                            double *FVM_RESTRICT dmin, const int *FVM_RESTRICT clist, const int *FVM_RESTRICT ninv) {
-  timestep_dev(n, P, off, lfj, act, bnd, U, volp, vel, pos, tlast, tend, dtl, dmin, clist, ninv, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+  // one thread per cell: every lane of a group would repeat the cell's own
+  // terms (a cube root among them), and on a full step that costs more than
+  // the shorter face walk gains (0.26 -> 0.69 ms on the 128^3 blast)
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+  timestep_group<1>(P, off, lfj, act, bnd, U, volp, vel, pos, tlast, tend, dtl, dmin, clist, clist ? *ninv : 0, 0,
+                    0xffffffffu, gt, gn, n);
 }
 
 // dt >= 8 dt_min halving (MPI/compute_timestep.cpp:103-104)
@@ -1574,57 +1554,23 @@ __global__ void k_halve(int n, const unsigned char *FVM_RESTRICT act, const doub
 //  3. otherwise k_adjust_seq sweeps the ascending list of active
 //     non-boundary sites (compacted in parallel) in one thread, exactly as
 //     the reference does.
-__device__ __forceinline__ void adjust_mark_dev(int n, const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
-                              const unsigned char *FVM_RESTRICT act,
-                              const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT dtl,
-                              unsigned char *FVM_RESTRICT hash, int *FVM_RESTRICT ndirty,
-                              unsigned char *FVM_RESTRICT site, unsigned char *FVM_RESTRICT work,
-                              const int *FVM_RESTRICT clist, const int *FVM_RESTRICT ninv, int gt0_, int gnt_) {
-  // site[] starts cleared; only the active non-boundary sites are marked
-  int ndirty_t = 0;
-  const int cnt_ = clist ? *ninv : n;
-  const bool lst = clist && cnt_ != n;  // every cell involved: the list is the identity
-  for (int t_ = gt0_; t_ < cnt_; t_ += gnt_) {
-    const int i = lst ? clist[t_] : t_;
-    if (!(act[i] & A_ACTIVE) || bnd[i] != NO_BOUNDARY) continue;
-    bool dirty = false;
-    site[i] = 1;
-    const double di = dtl[i];
-    for (int q = off[i]; q < off[i + 1]; q++) {
-      const int2 fj = lfj[q];
-      const int j = fj.y >= 0 ? fj.y : ~fj.y;
-      const double dj = dtl[j];
-      if (dj < 0.0) continue;
-      hash[j] = 1;
-      if (2.0 * dj < di || 2.0 * di < dj) {
-        dirty = true;
-        work[j] = 1;  // both ends of a pair outside a factor 2 start the replay's work list
-      }
-    }
-    if (dirty) { work[i] = 1; ndirty_t++; }
-  }
-  __shared__ int bsum;
-  if (threadIdx.x == 0) bsum = 0;
-  __syncthreads();
-  for (int o = 16; o > 0; o >>= 1) ndirty_t += __shfl_xor_sync(0xffffffffu, ndirty_t, o);
-  if ((threadIdx.x & 31) == 0 && ndirty_t) atomicAdd(&bsum, ndirty_t);
-  __syncthreads();
-  if (threadIdx.x == 0 && bsum) atomicAdd(ndirty, bsum);
-}
-// The same with G lanes per site over the involved-cell list: the faces
-// split among the lanes (the marks do not depend on the order), the site's
-// own marks and count by the group's first lane.  Called by every thread of
-// the block.
+// The marks with G lanes per site, over the involved-cell list or every
+// cell: the faces split among the lanes (the marks do not depend on the
+// order), the site's own marks and count by the group's first lane.  Called
+// by every thread of the block.
 template <int G>
 __device__ __forceinline__ void adjust_mark_group(const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj,
                               const unsigned char *FVM_RESTRICT act,
                               const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT dtl,
                               unsigned char *FVM_RESTRICT hash, int *FVM_RESTRICT ndirty,
                               unsigned char *FVM_RESTRICT site, unsigned char *FVM_RESTRICT work,
-                              const int *FVM_RESTRICT clist, int ninv, int gl, unsigned gmask, int g0, int gn) {
+                              const int *FVM_RESTRICT clist, int ninv, int gl, unsigned gmask, int g0, int gn,
+                              int n = 0) {
   int ndirty_t = 0;
-  for (int t_ = g0; t_ < ninv; t_ += gn) {
-    const int i = clist[t_];
+  const int cnt = clist ? ninv : n;
+  const bool lst = clist && cnt != n;  // every cell involved: the list is the identity
+  for (int t_ = g0; t_ < cnt; t_ += gn) {
+    const int i = lst ? clist[t_] : t_;
     if (!(act[i] & A_ACTIVE) || bnd[i] != NO_BOUNDARY) continue;
     bool dirty = false;
     const double di = dtl[i];
@@ -1660,7 +1606,12 @@ __global__ void k_adjust_mark(int n, const int *FVM_RESTRICT off, const int2 *FV
                               unsigned char *FVM_RESTRICT hash, int *FVM_RESTRICT ndirty,
                               unsigned char *FVM_RESTRICT site, unsigned char *FVM_RESTRICT work,
                               const int *FVM_RESTRICT clist, const int *FVM_RESTRICT ninv) {
-  adjust_mark_dev(n, off, lfj, act, bnd, dtl, hash, ndirty, site, work, clist, ninv, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+  // eight lanes per site (adjust_mark_group)
+  constexpr int G = 8;
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+  const unsigned gmask = ((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1));
+  adjust_mark_group<G>(off, lfj, act, bnd, dtl, hash, ndirty, site, work, clist, clist ? *ninv : 0,
+                       gt & (G - 1), gmask, gt / G, gn / G, n);
 }
 
 // Order-preserving compaction of flagged cells: per-block counts, one-block

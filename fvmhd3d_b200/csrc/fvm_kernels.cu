@@ -962,7 +962,7 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
       CK(cudaMemsetAsync(d.awork, 0, 2 * (size_t)n, c->st));
       CK(cudaMemsetAsync(d.act0, 0, n, c->st));
     }
-    k_adjust_mark<<<sgrid(c, n, 128), 128, 0, c->st>>>(n, d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash,
+    k_adjust_mark<<<sgrid(c, 8LL * n, 128), 128, 0, c->st>>>(n, d.off, d.lfj, d.act, d.bnd, d.dtl, d.hash,
                                                       &d.S->iscal[4], d.act0, d.awork, cl, &d.S->ninv);
     LAUNCH_CHECK();
     if (cl) {

@@ -44,6 +44,7 @@ struct Dev {
   int2 *s12;
   double4 *geo, *cen, *dr1, *dr2;
   double *cvol, *ccen;
+  double *hcell;  // (cvol / (4 pi / 3))^(1/3), Params::hcell
   int *off, *lnk;
   int *perm;  // thread slot -> cell (face-count order inside windows of CPW cells)
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
@@ -1272,7 +1273,7 @@ __device__ __forceinline__ void corr_cell_finish(int c, unsigned char ac, const 
     Uc[WBY] -= dPsi[1];
     Uc[WBZ] -= dPsi[2];
     Uc[MPSI] -= dcs2 * divB;
-    const double l_min = pow(V / (4.0 * M_PI / 3.0), 1.0 / 3.0);
+    const double l_min = P.hcell[c];
     Uc[MPSI] *= exp(-0.5 * ch_sig / l_min * dt);
     to_primitive(Uc, V, W1);
   }
@@ -1440,7 +1441,7 @@ __device__ double cell_timestep(const Params &P, int i, bool with_faces, const i
     const double d[3] = {W[VELX] - pv[0] * s, W[VELY] - pv[1] * s, W[VELZ] - pv[2] * s};
     vrel = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
   }
-  const double h = pow(volp[i] / (4.0 * M_PI / 3.0), 1.0 / 3.0);
+  const double h = P.hcell[i];  // volp is the cell's volume
   double dti = h / (csi + vrel + 1.0 / FVM_HUGE);
   if (with_faces) {
     const double fac = b ? 0.0 : 1.0;
@@ -2225,7 +2226,7 @@ __device__ __forceinline__ void pred_cell_finish(int c, const double *dot, doubl
     Uc[WBY] -= dot[11] * dt;
     Uc[WBZ] -= dot[12] * dt;
     Uc[MPSI] -= dcs2 * divB * dt;
-    const double l_min = pow(V / (4.0 * M_PI / 3.0), 1.0 / 3.0);
+    const double l_min = P.hcell[c];
     Uc[MPSI] *= exp(-0.5 * ch_sig / l_min * dt);
   }
   double W1[NF];
@@ -2535,6 +2536,12 @@ __device__ __forceinline__ void maxrung_dev(int n, const int *FVM_RESTRICT rung,
 }
 __global__ void k_maxrung(int n, const int *FVM_RESTRICT rung, int *FVM_RESTRICT out) {
   maxrung_dev(n, rung, out, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+
+// (V / (4 pi / 3))^(1/3) per cell, for Params::hcell.
+__global__ void k_cell_radius(int n, const double *FVM_RESTRICT cvol, double *FVM_RESTRICT hcell) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) hcell[i] = pow(cvol[i] / (4.0 * M_PI / 3.0), 1.0 / 3.0);
 }
 
 // ---- init: compute_pvel + compute_timesteps(true) -------------------------

@@ -381,6 +381,7 @@ static int alloc_mesh(fvm_ctx *c, long long ncell, long long nface, long long nl
   rc |= dalloc(c, &d.dr1, nface); rc |= dalloc(c, &d.dr2, nface); rc |= dalloc(c, &d.fflag, nface);
   rc |= dalloc_bytes(c, &d.fst, 20 * c->rb * (size_t)nface);
   rc |= dalloc(c, &d.cvol, ncell); rc |= dalloc(c, &d.ccen, 3 * (size_t)ncell);
+  rc |= dalloc(c, &d.hcell, ncell);
   rc |= dalloc(c, &d.off, ncell + 1); rc |= dalloc(c, &d.lnk, nl); rc |= dalloc(c, &d.perm, ncell);
   rc |= dalloc(c, &d.lfj, nl);
   rc |= dalloc(c, &d.lsort, nl); rc |= dalloc(c, &d.lpart, nl);
@@ -427,6 +428,7 @@ static int alloc_mesh(fvm_ctx *c, long long ncell, long long nface, long long nl
   c->cap_n = ncell;
   c->cap_f = nface;
   c->cap_l = nl;
+  c->P.hcell = d.hcell;
   return 0;
 }
 
@@ -521,6 +523,8 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   CK(cudaMemcpyAsync(doff, off, b_o, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(dids, ids, b_i, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(d.cvol, cell_volume, sizeof(double) * ncell, cudaMemcpyHostToDevice, c->st));
+  k_cell_radius<<<nblk(ncell, 256), 256, 0, c->st>>>(ncell, d.cvol, d.hcell);
+  LAUNCH_CHECK();
   CK(cudaMemcpyAsync(d.ccen, cell_centroid, sizeof(double) * 3 * ncell, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemsetAsync(derr, 0x7f, sizeof(herr), c->st));
   CK(cudaMemsetAsync(flink, 0xff, b_fl, c->st));

@@ -26,6 +26,10 @@ struct Params {
   int eos;              // 0 ideal gas, 1 isothermal disk
   double iso_GM, iso_cfac;
   int static_mesh;      // 1: compute_pvel1 hook with vel = 0 (static generators)
+  // per cell: (V / (4 pi / 3))^(1/3), the length of the CFL timestep and of
+  // the Dedner damping, computed once per mesh (a cell's volume changes only
+  // with its mesh)
+  const double *hcell;
 };
 
 template <typename T> __host__ __device__ __forceinline__ T sqr(T x) { return x * x; }

@@ -436,23 +436,40 @@ def config5_leg(F, torch, local, steps=24):
     return out
 
 
-def remesh_leg(F, S, m, e2e):
+def remesh_leg(F, S, m, e2e, bnd=None):
     """The mesh installation the reference repeats every step
     (MPI/iterate.cpp:150 rebuilds the mesh; the fluid path then starts from
-    the new face and cell lists): fvm_set_mesh from host arrays, with the
-    per-link tables it builds on the device, timed by the host clock around
-    the call (it synchronises).  With the host's own mesh build excluded, as
-    for the reference, the end-to-end rate of a step that also reinstalls
-    the mesh is faces / (e2e step time + this time)."""
+    the new face and cell lists and generator positions): fvm_set_mesh and
+    fvm_set_positions from pinned host arrays (a host that remeshes every
+    step keeps them pinned, as it keeps its state for fvm_step_host), with
+    the checks and per-link tables they build on the device, timed by the
+    host clock around the calls (they synchronise).  With the host's own
+    mesh build excluded, as for the reference, the end-to-end rate of a step
+    that also reinstalls the mesh is faces / (e2e step time + this time)."""
     import torch
+
+    def pinned(a, dt):
+        a = np.ascontiguousarray(a, dt)
+        t = torch.empty(a.shape, dtype=torch.from_numpy(a[:0]).dtype, pin_memory=True)
+        t.numpy()[...] = a
+        return t.numpy()
+
+    arrs = [pinned(m.s1, np.int32), pinned(m.s2, np.int32), pinned(m.n, np.float64), pinned(m.centroid, np.float64),
+            pinned(m.volume, np.float64), pinned(m.cell_centroid, np.float64), pinned(m.cell_face_off, np.int64),
+            pinned(m.cell_face_ids, np.int32)]
+    pos = pinned(m.pos, np.float64)
+    b = None if bnd is None else pinned(bnd, np.int32)
+    p = F.system._p
     torch.cuda.synchronize()
     ts = []
     for _ in range(3):
         t0 = time.perf_counter()
-        S.set_mesh(m)
+        S._check(S.L.fvm_set_mesh(S.h, m.ncell, m.nface, *[p(a) for a in arrs]), "fvm_set_mesh")
+        S._check(S.L.fvm_set_positions(S.h, p(pos), p(b)), "fvm_set_positions")
         ts.append(time.perf_counter() - t0)
     out = {"set_mesh_ms": round(1e3 * min(ts), 2), "ncell": m.ncell, "nface": m.nface,
-           "path": "fvm_set_mesh from host arrays (upload, validation, link tables), host clock"}
+           "path": "fvm_set_mesh + fvm_set_positions from pinned host arrays (upload, validation, link and "
+                   "reconstruction tables), host clock"}
     if e2e:
         step_s = m.nface / e2e["value"]
         out["e2e_with_remesh"] = {"value": m.nface / (step_s + min(ts)), "unit": UNIT}
@@ -612,7 +629,7 @@ def run_gpu(args):
     if (not args.no_learned and shared and args.problem == "blast" and pb == 8 and os.path.exists(weights)):
         line["learned_fp32"] = learned_leg(F, m, W, 100, weights, stream_of=torch.cuda.ExternalStream)
     if not args.no_remesh:
-        line["e2e_remesh"] = remesh_leg(F, S, m, e2e)
+        line["e2e_remesh"] = remesh_leg(F, S, m, e2e, bnd)
     S.close()
     # the other configurations of the target, each on its own mesh (parity
     # cases of the headline are in tests/); rank 0 of a single-GPU run only

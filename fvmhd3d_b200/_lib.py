@@ -51,6 +51,7 @@ SIGNATURES = {
     "fvm_end_step": (c_int, [c_void_p, c_int]),
     "fvm_step": (c_int, [c_void_p, c_int]),
     "fvm_step_host": (c_int, [c_void_p, c_int, c_ull] + [c_void_p] * 7),
+    "fvm_set_positions": (c_int, [c_void_p, c_void_p, c_void_p]),
     "fvm_run": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "fvm_time": (c_double, [c_void_p]),
     "fvm_tsys_ticks": (c_ull, [c_void_p]),

@@ -155,6 +155,7 @@ struct fvm_ctx {
   int min_rung, max_rung;
   double t_global;
   bool have_mesh, have_state, in_step;
+  bool have_geom = false;  // generator positions and the tables built from them belong to the mesh
   bool fp32;    // bulk (reconstruction, limiter, flux) in single precision
   size_t rb;    // bytes of one bulk value
   unsigned long long cur_flags;
@@ -459,6 +460,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   drop_graphs(c);
   c->have_mesh = false;
   c->have_state = false;
+  c->have_geom = false;
   c->learn_mode = 0;
   c->lb = LearnBuf{};
   free_learn_buffers(c);
@@ -571,6 +573,37 @@ static int enqueue_maxrung(fvm_ctx *c) {
   return 0;
 }
 
+// Generator positions and boundary codes of the installed mesh, and what is
+// built from them: the boundary-neighbour flags, the face offsets and the
+// per-link tables of the limiter and the reconstruction.
+static int enq_positions(fvm_ctx *c, const double *pos, const int *bnd) {
+  const int n = c->n;
+  Dev &d = c->d;
+  CK(cudaMemcpyAsync(d.pos, pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, c->st));
+  if (bnd) CK(cudaMemcpyAsync(d.bnd, bnd, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
+  else CK(cudaMemsetAsync(d.bnd, 0, sizeof(int) * n, c->st));
+  k_bnd_neighbours<<<nblk(n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.bnd, d.bnb);
+  LAUNCH_CHECK();
+  k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
+  LAUNCH_CHECK();
+  BULK(k_link_recon<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.off, d.lfj, d.geo, d.dr1, d.dr2, (R *)d.lrw,
+                                                        (R *)d.lrd, (R *)d.lld));
+  LAUNCH_CHECK();
+  c->have_geom = true;
+  return 0;
+}
+
+int fvm_set_positions(fvm_ctx *c, const double *pos, const int *bnd) {
+  if (!c || !pos) { if (c) c->err = "fvm_set_positions: bad argument"; return FVM_EINVAL; }
+  if (!c->have_mesh) { c->err = "fvm_set_positions: no mesh"; return FVM_ENOMESH; }
+  if (c->in_step) { c->err = "fvm_set_positions: inside a step"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  const int rc = enq_positions(c, pos, bnd);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
 int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *bnd, int rung_offset) {
   if (!c || !W || !pos) { if (c) c->err = "fvm_init_problem: bad argument"; return FVM_EINVAL; }
   if (!c->have_mesh) { c->err = "fvm_init_problem: no mesh"; return FVM_ENOMESH; }
@@ -581,18 +614,10 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   CK(cudaMalloc(&dW, sizeof(double) * 10 * (size_t)n));
   cudaError_t e = cudaMemcpyAsync(dW, W, sizeof(double) * 10 * (size_t)n, cudaMemcpyHostToDevice, c->st);
   if (e != cudaSuccess) { cudaFree(dW); c->err = cudaGetErrorString(e); return FVM_ECUDA; }
-  CK(cudaMemcpyAsync(d.pos, pos, sizeof(double) * 3 * (size_t)n, cudaMemcpyHostToDevice, c->st));
-  if (bnd) CK(cudaMemcpyAsync(d.bnd, bnd, sizeof(int) * n, cudaMemcpyHostToDevice, c->st));
-  else CK(cudaMemsetAsync(d.bnd, 0, sizeof(int) * n, c->st));
-  k_bnd_neighbours<<<nblk(n, 256), 256, 0, c->st>>>(n, d.off, d.lfj, d.bnd, d.bnb);
-  LAUNCH_CHECK();
+  int rc = enq_positions(c, pos, bnd);
+  if (rc) { cudaFree(dW); return rc; }
   CK(cudaMemsetAsync(d.vel, 0, sizeof(double) * 3 * (size_t)n, c->st));
   CK(cudaMemsetAsync(d.tlast, 0, sizeof(double) * n, c->st));
-  k_face_geom<<<nblk(c->nf, 256), 256, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.cen, d.pos, d.dr1, d.dr2);
-  LAUNCH_CHECK();
-  BULK(k_link_recon<R><<<nblk(n, 256), 256, 0, c->st>>>(n, c->P, d.off, d.lfj, d.geo, d.dr1, d.dr2, (R *)d.lrw,
-                                                        (R *)d.lrd, (R *)d.lld));
-  LAUNCH_CHECK();
 
   BULK(k_init_state<R><<<nblk(n, 128), 128, 0, c->st>>>(n, dW, d.cvol, d.U, d.dU, (R *)d.Wrec, d.volp));
   LAUNCH_CHECK();
@@ -662,6 +687,7 @@ int fvm_get_state(fvm_ctx *c, double *pos, double *vel, double *tlast, double *t
 int fvm_set_state(fvm_ctx *c, const double *vel, const double *tlast, const double *tend, const int *rung,
                   const double *U, const double *dU, const double *wrec, unsigned long long tsys_ticks) {
   if (!c || !c->have_mesh) return FVM_ENOMESH;
+  if (!c->have_geom) { c->err = "fvm_set_state: no generator positions for this mesh (fvm_set_positions)"; return FVM_ENOMESH; }
   if (c->in_step) { c->err = "fvm_set_state: inside a step"; return FVM_EINVAL; }
   CK(cudaSetDevice(c->device));
   const size_t n = c->n;
@@ -1337,6 +1363,7 @@ int fvm_step(fvm_ctx *c, int shared) {
 int fvm_step_host(fvm_ctx *c, int shared, unsigned long long tsys_ticks, double *vel, double *tlast, double *tend,
                   int *rung, double *U, double *dU, double *wrec) {
   if (!c || !c->have_mesh) return FVM_ENOMESH;
+  if (!c->have_geom) { c->err = "fvm_step_host: no generator positions for this mesh (fvm_set_positions)"; return FVM_ENOMESH; }
   if (c->in_step) { c->err = "fvm_step_host: inside a step"; return FVM_EINVAL; }
   if (!vel || !tlast || !tend || !rung || !U || !dU || !wrec) {
     c->err = "fvm_step_host: every state array is required";

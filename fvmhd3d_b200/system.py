@@ -82,6 +82,14 @@ class System:
                 np.ascontiguousarray(m.cell_face_off, np.int64), np.ascontiguousarray(m.cell_face_ids, np.int32)]
         self._check(self.L.fvm_set_mesh(self.h, m.ncell, m.nface, *[_p(a) for a in arrs]), "fvm_set_mesh")
 
+    def set_positions(self, pos, bnd=None) -> None:
+        """Generator positions (and boundary codes) of the installed mesh and
+        the tables built from them, keeping the fluid state: after
+        set_mesh, before set_state / step_host."""
+        p = np.ascontiguousarray(pos, np.float64)
+        b = None if bnd is None else np.ascontiguousarray(bnd, np.int32)
+        self._check(self.L.fvm_set_positions(self.h, _p(p), _p(b)), "fvm_set_positions")
+
     def init_problem(self, W, bnd=None, rung_offset=0):
         W = np.ascontiguousarray(W, np.float64)
         pos = np.ascontiguousarray(self.mesh.pos, np.float64)

@@ -76,6 +76,16 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
                  const double *cell_centroid, const long long *cell_face_off,
                  const int *cell_face_ids);
 
+/* Generator positions pos[3n] and boundary codes bnd[n] (NULL: none) of the
+ * installed mesh, and the tables built from them (face offsets, per-link
+ * reconstruction and limiter weights, boundary-neighbour flags), without
+ * touching the fluid state or orig_pos / orig_vel.  A host that rebuilds its
+ * mesh every step (MPI/iterate.cpp:150) calls fvm_set_mesh, then this, then
+ * fvm_set_state (or fvm_step_host) with the state it keeps; fvm_init_problem
+ * does the same as part of setting up a problem.  fvm_set_state and
+ * fvm_step_host refuse a mesh without positions (FVM_ENOMESH). */
+int fvm_set_positions(fvm_ctx *c, const double *pos, const int *bnd);
+
 /* Initial state from primitives W, following the tail of the reference's
  * set_problem (MPI/problems/mri_disk3d.cpp:832-880): Wrec=(W,0,0,0,0),
  * U=cons(W), dU=0, compute_pvel, compute_timesteps(true), rung += rung_offset,

@@ -70,3 +70,40 @@ def test_step_host_rejects_a_rung_out_of_range_before_uploading():
         assert np.array_equal(before[k], after[k]), k
     with pytest.raises(ValueError):
         s.step_host({**h, "U": h["U"][:10]}, shared=True)
+
+
+def test_remesh_every_step_keeps_the_bits():
+    """The flow of a host that rebuilds its mesh every step: fvm_set_mesh,
+    fvm_set_positions, then the state it keeps (fvm_step_host).  Reinstalling
+    the same mesh each step gives the bits of steps on one installed mesh."""
+    m, z = load_golden("ref_disk4k_individual.npz")
+    kw = golden_params(z)
+    bnd = z.get("bnd")
+    a = gpu_system(m, z["W"], bnd=bnd, **kw)
+    b = gpu_system(m, z["W"], bnd=bnd, **kw)
+    hb = host_state(b)
+    for _ in range(5):
+        a.step(shared=False)
+        ticks = b.tsys_ticks
+        b.set_mesh(m)
+        b.set_positions(m.pos, bnd)
+        b.step_host(hb, shared=False, tsys_ticks=ticks)
+    sa = a.get_state()
+    for k, t, w in b.STATE_ARRAYS:
+        assert np.array_equal(np.asarray(sa[k], t).reshape(hb[k].shape), hb[k]), k
+    assert a.tsys_ticks == b.tsys_ticks
+
+
+def test_a_new_mesh_needs_its_positions_before_a_state():
+    import fvmhd3d_b200 as F
+    m, W = setup_case(8, "alfven", seed=2, noise=0.0)
+    s = gpu_system(m, W)
+    h = host_state(s)
+    s.set_mesh(m)
+    with pytest.raises(F.FvmError):
+        s.set_state(**h)
+    with pytest.raises(F.FvmError):
+        s.step_host(h, shared=True)
+    s.set_positions(m.pos)
+    s.set_state(**h)
+    s.step(shared=True)

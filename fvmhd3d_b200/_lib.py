@@ -13,6 +13,10 @@ c_int, c_double, c_void_p, c_ll, c_ull, c_float = (ctypes.c_int, ctypes.c_double
                                                    ctypes.c_longlong, ctypes.c_ulonglong, ctypes.c_float)
 
 
+# int (*)(void *user, double *dt_min): the reduction of fvm_set_reduce
+REDUCE_FN = ctypes.CFUNCTYPE(c_int, c_void_p, ctypes.POINTER(c_double))
+
+
 class FvmParams(ctypes.Structure):
     """Mirror of `struct fvm_params`."""
     _fields_ = [
@@ -79,6 +83,8 @@ SIGNATURES = {
     "fvm_fused_step_count": (c_ll, [c_void_p]),
     "fvm_set_list_building": (c_int, [c_void_p, c_int]),
     "fvm_incremental_step_count": (c_ll, [c_void_p]),
+    "fvm_set_reduce": (c_int, [c_void_p, REDUCE_FN, c_void_p]),
+    "fvm_set_halo": (c_int, [c_void_p, c_void_p]),
     "fvm_compute_flux": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_compute_flux_static": (c_int, [c_void_p, c_int] + [c_void_p] * 8),
     "fvm_last_step_ms": (c_float, [c_void_p]),

@@ -45,6 +45,7 @@ struct Dev {
   double4 *geo, *cen, *dr1, *dr2;
   double *cvol, *ccen;
   double *hcell;  // (cvol / (4 pi / 3))^(1/3), Params::hcell
+  unsigned char *halo;  // copies of other ranks' cells (Params::halo when set)
   int *off, *lnk;
   int *perm;  // thread slot -> cell (face-count order inside windows of CPW cells)
   int *alist, *bcount;  // ordered active-site list and block offsets (individual timesteps)
@@ -1505,7 +1506,7 @@ __device__ __forceinline__ void timestep_group(Params P, const int *FVM_RESTRICT
       const double dti = smin(extra_timestep(P, i, bnd, pos, vel),
                               cell_timestep<G>(P, i, true, off, lfj, bnd, U, volp, vel, gl, gmask));
       if (gl == 0) {
-        vmin = smin(vmin, dti);
+        if (!P.halo || !P.halo[i]) vmin = smin(vmin, dti);
         dtl[i] = bnd[i] != NO_BOUNDARY ? -1.0 * dti : dti;
       }
     }
@@ -2550,7 +2551,7 @@ __global__ void k_init_dt(int n, Params P, const int *FVM_RESTRICT bnd, const do
                           const double *FVM_RESTRICT pos, double *FVM_RESTRICT dmin) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double vmin = FVM_HUGE;
-  if (i < n)
+  if (i < n && !(P.halo && P.halo[i]))
     vmin = smin(extra_timestep(P, i, bnd, pos, vel),
                 cell_timestep(P, i, false, nullptr, nullptr, bnd, U, volp, vel));
   for (int o = 16; o > 0; o >>= 1) vmin = smin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));

@@ -189,6 +189,9 @@ struct fvm_ctx {
   // -1: automatic, see inc_limit)
   int inc_max = -1;
   int fused_bpsm = 0;          // its resident blocks per SM (queried outside capture)
+  // the reduction of the timestep minimum over ranks (fvm_set_reduce)
+  fvm_reduce_fn reduce = nullptr;
+  void *reduce_user = nullptr;
   cudaStream_t aux = nullptr;  // captures the branches of the fused/stage choice
   // fvm_step_host: the copy stream and the events that order its copies
   // against the stage kernels (created on first use)
@@ -382,7 +385,7 @@ static int alloc_mesh(fvm_ctx *c, long long ncell, long long nface, long long nl
   rc |= dalloc(c, &d.dr1, nface); rc |= dalloc(c, &d.dr2, nface); rc |= dalloc(c, &d.fflag, nface);
   rc |= dalloc_bytes(c, &d.fst, 20 * c->rb * (size_t)nface);
   rc |= dalloc(c, &d.cvol, ncell); rc |= dalloc(c, &d.ccen, 3 * (size_t)ncell);
-  rc |= dalloc(c, &d.hcell, ncell);
+  rc |= dalloc(c, &d.hcell, ncell); rc |= dalloc(c, &d.halo, ncell);
   rc |= dalloc(c, &d.off, ncell + 1); rc |= dalloc(c, &d.lnk, nl); rc |= dalloc(c, &d.perm, ncell);
   rc |= dalloc(c, &d.lfj, nl);
   rc |= dalloc(c, &d.lsort, nl); rc |= dalloc(c, &d.lpart, nl);
@@ -461,6 +464,7 @@ int fvm_set_mesh(fvm_ctx *c, int ncell, int nface, const int *s1, const int *s2,
   c->have_mesh = false;
   c->have_state = false;
   c->have_geom = false;
+  c->P.halo = nullptr;
   c->learn_mode = 0;
   c->lb = LearnBuf{};
   free_learn_buffers(c);
@@ -639,6 +643,10 @@ int fvm_init_problem(fvm_ctx *c, const double *W, const double *pos, const int *
   CK(cudaMemcpyAsync(&dtmin, &d.S->dtmin, sizeof(double), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
   cudaFree(dW);
+  if (c->reduce && c->reduce(c->reduce_user, &dtmin) != 0) {
+    c->err = "fvm_init_problem: the timestep reduction failed";
+    return FVM_EINVAL;
+  }
   c->min_rung = 0;
   const int rung = get_rung(c->P, dtmin, c->min_rung) + rung_offset;
   if (rung < 0 || rung >= RUNGMAX - 1) { c->err = "fvm_init_problem: initial rung out of range"; return FVM_ERANGE; }
@@ -980,6 +988,17 @@ static int enq_timesteps(fvm_ctx *c, int shared) {
   k_timestep<<<sgrid(c, n, 128), 128, 0, c->st>>>(n, c->P, d.off, d.lfj, d.act, d.bnd, d.U, d.volp, d.vel,
                                                   d.pos, d.tlast, d.tend, d.dtl, &d.S->dtmin, cl, &d.S->ninv);
   LAUNCH_CHECK();
+  if (c->reduce) {  // the minimum over ranks (MPI/compute_timestep.cpp:101)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(c->st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) { c->err = "the timestep reduction needs eager steps"; return FVM_EINVAL; }
+    double v = 0.0;
+    CK(cudaMemcpyAsync(&v, &d.S->dtmin, sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (c->reduce(c->reduce_user, &v) != 0) { c->err = "the timestep reduction failed"; return FVM_EINVAL; }
+    CK(cudaMemcpyAsync(&d.S->dtmin, &v, sizeof(double), cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
   if (!shared) {
     k_halve<<<sgrid(c, n, 256), 256, 0, c->st>>>(n, d.act, &d.S->dtmin, d.dtl, cl, &d.S->ninv);
     LAUNCH_CHECK();
@@ -1235,7 +1254,7 @@ static int enq_step(fvm_ctx *c, int shared) {
   if ((rc = enq_begin(c))) return rc;
   cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
   CK(cudaStreamIsCapturing(c->st, &cs));
-  const bool fusable = !shared && c->fused_max > 0 && c->fused_bpsm > 0 && c->learn_mode == 0;
+  const bool fusable = !shared && c->fused_max > 0 && c->fused_bpsm > 0 && c->learn_mode == 0 && !c->reduce;
   if (fusable && cs == cudaStreamCaptureStatusActive && !c->prof) {
     rc = enq_fused_or_stages(c);
   } else if (fusable && cs == cudaStreamCaptureStatusNone) {
@@ -1456,6 +1475,7 @@ int fvm_step_host(fvm_ctx *c, int shared, unsigned long long tsys_ticks, double 
 int fvm_run(fvm_ctx *c, int nsteps, int shared, long long *faces_out) {
   if (!c || !c->have_state) { if (c) c->err = "fvm_run: no state"; return FVM_ENOMESH; }
   if (c->in_step || nsteps < 0) { c->err = "fvm_run: bad call"; return FVM_EINVAL; }
+  if (c->reduce) { c->err = "fvm_run: a timestep reduction is installed (replayed steps cannot call the host)"; return FVM_EINVAL; }
   CK(cudaSetDevice(c->device));
   const int g = shared ? 1 : 0;
   if (!c->graph[g]) {
@@ -2307,6 +2327,31 @@ int fvm_set_list_building(fvm_ctx *c, int max_entries) {
   CK(cudaStreamSynchronize(c->st));
   drop_graphs(c);  // captured partial steps hold the choice
   c->inc_max = max_entries;
+  return 0;
+}
+
+int fvm_set_reduce(fvm_ctx *c, fvm_reduce_fn fn, void *user) {
+  if (!c) return FVM_EINVAL;
+  if (c->in_step) { c->err = "fvm_set_reduce: inside a step"; return FVM_EINVAL; }
+  c->reduce = fn;
+  c->reduce_user = fn ? user : nullptr;
+  return 0;
+}
+
+int fvm_set_halo(fvm_ctx *c, const unsigned char *halo) {
+  if (!c || !c->have_mesh) { if (c) c->err = "fvm_set_halo: no mesh"; return FVM_ENOMESH; }
+  if (c->in_step) { c->err = "fvm_set_halo: inside a step"; return FVM_EINVAL; }
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  drop_graphs(c);  // captured steps hold the parameters
+  if (!halo) {
+    c->P.halo = nullptr;
+    return 0;
+  }
+  std::vector<unsigned char> h(halo, halo + c->n);
+  for (auto &v : h) v = v ? 1 : 0;
+  CK(cudaMemcpy(c->d.halo, h.data(), c->n, cudaMemcpyHostToDevice));
+  c->P.halo = c->d.halo;
   return 0;
 }
 

@@ -30,6 +30,9 @@ struct Params {
   // the Dedner damping, computed once per mesh (a cell's volume changes only
   // with its mesh)
   const double *hcell;
+  // per cell, or null: the cell is a copy of another rank's cell, left out
+  // of the timestep minimum (fvm_set_halo)
+  const unsigned char *halo;
 };
 
 template <typename T> __host__ __device__ __forceinline__ T sqr(T x) { return x * x; }

@@ -291,6 +291,35 @@ class System:
         """Steps the persistent rung kernel has run (as of the last run/step)."""
         return int(self.L.fvm_fused_step_count(self.h))
 
+    def set_reduce(self, fn) -> None:
+        """The reduction of the timestep minimum over ranks (MPI_Allreduce MIN
+        of compute_timesteps, MPI/compute_timestep.cpp:101): fn(dt_min) ->
+        the minimum over ranks, called on this thread inside steps and
+        fvm_init_problem.  None removes it.  Steps with a reduction are eager
+        (run() refuses)."""
+        if fn is None:
+            self._reduce_cb = None
+            self._check(self.L.fvm_set_reduce(self.h, ctypes.cast(None, _lib.REDUCE_FN), None), "fvm_set_reduce")
+            return
+
+        def cb(_user, p):
+            try:
+                p[0] = float(fn(float(p[0])))
+                return 0
+            except Exception:  # reported by the library as a failed step
+                return 1
+
+        self._reduce_cb = _lib.REDUCE_FN(cb)  # kept alive while installed
+        self._check(self.L.fvm_set_reduce(self.h, self._reduce_cb, None), "fvm_set_reduce")
+
+    def set_halo(self, halo) -> None:
+        """Marks the installed mesh's copies of other ranks' cells (a bool
+        per cell; None: none); their timesteps stay out of the minimum."""
+        h = None if halo is None else np.ascontiguousarray(np.asarray(halo) != 0, np.uint8)
+        if h is not None and h.shape != (self.mesh.ncell,):
+            raise ValueError("set_halo: one flag per cell")
+        self._check(self.L.fvm_set_halo(self.h, _p(h)), "fvm_set_halo")
+
     def set_list_building(self, max_entries) -> None:
         """Partial steps whose active cells plus their links number at most
         max_entries build their lists from those cells' links instead of a

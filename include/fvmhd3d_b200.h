@@ -178,6 +178,33 @@ int fvm_step_host(fvm_ctx *c, int shared, unsigned long long tsys_ticks, double 
  * receives the summed number of active faces. */
 int fvm_run(fvm_ctx *c, int nsteps, int shared, long long *faces_out);
 
+/* ---- one domain of a partitioned mesh --------------------------------------
+ * A rank that owns part of the cells installs its owned cells plus the rings
+ * of neighbours around them as its mesh, and its host copies the neighbour
+ * rows from their owners between steps (the reference's
+ * distribute_particle_fluid_data / collect_results,
+ * MPI/distribute_work.cpp:367-724). */
+
+/* The reduction of the timestep minimum over ranks: MPI_Allreduce(MIN) of
+ * compute_timesteps (MPI/compute_timestep.cpp:101).  Given this rank's
+ * minimum in *dt_min, the function stores the minimum over ranks and returns
+ * 0 (non-zero fails the step with FVM_EINVAL). */
+typedef int (*fvm_reduce_fn)(void *user, double *dt_min);
+
+/* Installs (fn != NULL) or removes the reduction.  While it is installed,
+ * fvm_compute_timesteps, fvm_step and fvm_step_host wait for the rank's
+ * minimum, call fn on the calling thread and continue with its result, and
+ * fvm_init_problem calls it on the initial minimum; fvm_run, whose replayed
+ * steps cannot call the host, returns FVM_EINVAL, and the persistent rung
+ * kernel is not used. */
+int fvm_set_reduce(fvm_ctx *c, fvm_reduce_fn fn, void *user);
+
+/* Marks the installed mesh's copies of other ranks' cells (halo[i] != 0;
+ * NULL: every cell is this rank's).  Their timesteps are computed but left
+ * out of the minimum (a copy in the outer ring misses neighbours, so its
+ * value is not its owner's).  Cleared by fvm_set_mesh. */
+int fvm_set_halo(fvm_ctx *c, const unsigned char *halo);
+
 /* ---- inspection ----------------------------------------------------------- */
 
 double fvm_time(const fvm_ctx *c);                       /* system::t_global */

@@ -98,6 +98,25 @@ using namespace fvm;
 #ifndef FVM_CELL_LFJ
 #define FVM_CELL_LFJ 1  // cell kernels take (face, neighbour) from the link table instead of s12
 #endif
+// Resident blocks per SM that the compute_update and compute_update0 cell
+// passes ask for (FP64 / FP32 bulk).  Measured on the 128^3 blast: FP32
+// corrector cells 1.04 -> 0.78 ms and predictor cells 0.77 -> 0.74 ms at 5
+// (96 registers, a few bytes of spills); FP64 corrector cells 0.970 ->
+// 0.952 ms at 4 (121 registers), FP64 predictor cells best at 1 (123).
+#ifndef FVM_CORR_CELL_MINB_D
+#define FVM_CORR_CELL_MINB_D 4
+#endif
+#ifndef FVM_CORR_CELL_MINB_F
+#define FVM_CORR_CELL_MINB_F 5
+#endif
+#ifndef FVM_PRED_CELL_MINB_D
+#define FVM_PRED_CELL_MINB_D 1
+#endif
+#ifndef FVM_PRED_CELL_MINB_F
+#define FVM_PRED_CELL_MINB_F 5
+#endif
+#define FVM_CORR_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CORR_CELL_MINB_F : FVM_CORR_CELL_MINB_D)
+#define FVM_PRED_CELL_MINB(R) (sizeof(R) == 4 ? FVM_PRED_CELL_MINB_F : FVM_PRED_CELL_MINB_D)
 #ifndef FVM_CELL_UNROLL
 #define FVM_CELL_UNROLL 1  // unroll factor of the cell kernels' face loops (1 and 2 time the same within 1%)
 #endif
@@ -1347,7 +1366,7 @@ __device__ __forceinline__ void corr_cell_dev(int n, Params P, const Sched *FVM_
                       fcon, fcode, U, dU, stepdU, counters, divb);
 }
 template <typename R>
-__global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched *FVM_RESTRICT S,
+__global__ void __launch_bounds__(128, FVM_CORR_CELL_MINB(R)) k_corr_cell(int n, Params P, const Sched *FVM_RESTRICT S,
     const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const int2 *FVM_RESTRICT s12,
     const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
     const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast, double *FVM_RESTRICT volp,
@@ -2294,7 +2313,7 @@ __device__ __forceinline__ void pred_cell_dev(int n, Params P, const Sched *FVM_
                       fcode, rung, tend, Wrec);
 }
 template <typename R>
-__global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched *FVM_RESTRICT S,
+__global__ void __launch_bounds__(128, FVM_PRED_CELL_MINB(R)) k_pred_cell(int n, Params P, const Sched *FVM_RESTRICT S,
     const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const int2 *FVM_RESTRICT s12,
     const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
     const double *FVM_RESTRICT pos, const double *FVM_RESTRICT U,

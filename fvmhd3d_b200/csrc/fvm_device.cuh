@@ -87,14 +87,27 @@ struct Dev {
 using namespace fvm;
 
 // Minimum resident 128-thread blocks per SM for the face-flux kernels (caps
-// their registers: 3 -> 168 for FP64, 4 -> 128 for FP32, no spills).
+// their registers).  The learned-flux modes and the persistent rung kernel
+// take 3 (168 registers, FP64) or 4 (128, FP32).  The exact
+// face passes take 4 (128 registers and about 100 bytes of spills, FP64) or
+// 5 (96, FP32, none): the extra warps hide more of the face gathers than
+// the spills cost (128^3 blast: FP64 corrector flux 1.32 -> 1.24 ms,
+// predictor 1.19 -> 1.08; FP32 0.85 -> 0.75 and 0.80 -> 0.69).
 #ifndef FVM_FLUX_MINB_D
 #define FVM_FLUX_MINB_D 3
 #endif
 #ifndef FVM_FLUX_MINB_F
 #define FVM_FLUX_MINB_F 4
 #endif
+#ifndef FVM_EXACT_FLUX_MINB_D
+#define FVM_EXACT_FLUX_MINB_D 4
+#endif
+#ifndef FVM_EXACT_FLUX_MINB_F
+#define FVM_EXACT_FLUX_MINB_F 5
+#endif
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
+#define FVM_FLUX_MODE_MINB(R, MODE) \
+  ((MODE) == 0 ? (sizeof(R) == 4 ? FVM_EXACT_FLUX_MINB_F : FVM_EXACT_FLUX_MINB_D) : FVM_FLUX_MINB(R))
 #ifndef FVM_CELL_LFJ
 #define FVM_CELL_LFJ 1  // cell kernels take (face, neighbour) from the link table instead of s12
 #endif
@@ -491,7 +504,16 @@ template <> struct CellTune<double> {
   static constexpr int KH_LIM = 2, MINB_LIM = 6, KH_REC = 2, MINB_REC = FVM_RECON_MINB_D;
 };
 template <> struct CellTune<float> {
-  static constexpr int KH_LIM = 2, MINB_LIM = 8, KH_REC = 5, MINB_REC = 6;
+// FP32: 8 blocks for the reconstruction (64 registers, a few spills) and 10
+// for the limiter (46) beat 6 and 8 (128^3 blast: 1.085 -> 1.027 ms and
+// 0.915 -> 0.886 ms).
+#ifndef FVM_RECON_MINB_F
+#define FVM_RECON_MINB_F 8
+#endif
+#ifndef FVM_LIMITER_MINB_F
+#define FVM_LIMITER_MINB_F 10
+#endif
+  static constexpr int KH_LIM = 2, MINB_LIM = FVM_LIMITER_MINB_F, KH_REC = 5, MINB_REC = FVM_RECON_MINB_F;
 };
 
 // KH consecutive bulk values from p, as 2-wide loads when KH is even: the
@@ -1092,7 +1114,7 @@ __device__ __forceinline__ void corr_flux_dev(int nf, Params P, const Sched *FVM
   }
 }
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_corr_flux(int nf, Params P, const Sched *FVM_RESTRICT S,
+__global__ void __launch_bounds__(128, FVM_FLUX_MODE_MINB(R, MODE)) k_corr_flux(int nf, Params P, const Sched *FVM_RESTRICT S,
     const int2 *FVM_RESTRICT s12, const double4 *FVM_RESTRICT geo, const double4 *FVM_RESTRICT dr1,
     const unsigned char *FVM_RESTRICT fflag, const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT vel,
     const double *FVM_RESTRICT tlast, const R *FVM_RESTRICT Wrec, const R *FVM_RESTRICT fst,
@@ -2206,7 +2228,7 @@ __device__ __forceinline__ void pred_flux_dev(int nf, Params P,
   }
 }
 template <typename R, int MODE>
-__global__ void __launch_bounds__(128, FVM_FLUX_MINB(R)) k_pred_flux(int nf, Params P,
+__global__ void __launch_bounds__(128, FVM_FLUX_MODE_MINB(R, MODE)) k_pred_flux(int nf, Params P,
     const int2 *FVM_RESTRICT s12, const double4 *FVM_RESTRICT geo, const double4 *FVM_RESTRICT dr1,
     const unsigned char *FVM_RESTRICT fflag, const int *FVM_RESTRICT bnd,
     const double *FVM_RESTRICT vel, const R *FVM_RESTRICT Wst,

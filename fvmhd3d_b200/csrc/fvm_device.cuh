@@ -90,9 +90,10 @@ using namespace fvm;
 // their registers).  The learned-flux modes and the persistent rung kernel
 // take 3 (168 registers, FP64) or 4 (128, FP32).  The exact
 // face passes take 4 (128 registers and about 100 bytes of spills, FP64) or
-// 5 (96, FP32, none): the extra warps hide more of the face gathers than
-// the spills cost (128^3 blast: FP64 corrector flux 1.32 -> 1.24 ms,
-// predictor 1.19 -> 1.08; FP32 0.85 -> 0.75 and 0.80 -> 0.69).
+// 6 (80 registers, 16 bytes of spills, FP32): the extra warps hide more of
+// the face gathers than the spills cost (128^3 blast: FP64 corrector flux
+// 1.32 -> 1.24 ms, predictor 1.19 -> 1.08; FP32 0.85 -> 0.75 -> 0.69 and
+// 0.80 -> 0.69 -> 0.63 at 5 and 6).
 #ifndef FVM_FLUX_MINB_D
 #define FVM_FLUX_MINB_D 3
 #endif
@@ -103,7 +104,7 @@ using namespace fvm;
 #define FVM_EXACT_FLUX_MINB_D 4
 #endif
 #ifndef FVM_EXACT_FLUX_MINB_F
-#define FVM_EXACT_FLUX_MINB_F 5
+#define FVM_EXACT_FLUX_MINB_F 6
 #endif
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
 #define FVM_FLUX_MODE_MINB(R, MODE) \
@@ -501,7 +502,10 @@ template <> struct CellTune<double> {
 #ifndef FVM_RECON_MINB_D
 #define FVM_RECON_MINB_D 8
 #endif
-  static constexpr int KH_LIM = 2, MINB_LIM = 6, KH_REC = 2, MINB_REC = FVM_RECON_MINB_D;
+#ifndef FVM_LIMITER_MINB_D
+#define FVM_LIMITER_MINB_D 6
+#endif
+  static constexpr int KH_LIM = 2, MINB_LIM = FVM_LIMITER_MINB_D, KH_REC = 2, MINB_REC = FVM_RECON_MINB_D;
 };
 template <> struct CellTune<float> {
 // FP32: 8 blocks for the reconstruction (64 registers, a few spills) and 10

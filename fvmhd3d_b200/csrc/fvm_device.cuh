@@ -87,36 +87,42 @@ struct Dev {
 using namespace fvm;
 
 // Minimum resident 128-thread blocks per SM for the face-flux kernels (caps
-// their registers).  The learned-flux modes and the persistent rung kernel
-// take 3 (168 registers, FP64) or 4 (128, FP32).  The exact
-// face passes take 4 (128 registers and about 100 bytes of spills, FP64) or
-// 6 (80 registers, 16 bytes of spills, FP32): the extra warps hide more of
-// the face gathers than the spills cost (128^3 blast: FP64 corrector flux
-// 1.32 -> 1.24 ms, predictor 1.19 -> 1.08; FP32 0.85 -> 0.75 -> 0.69 and
-// 0.80 -> 0.69 -> 0.63 at 5 and 6).
+// their registers): 3 (168 registers, FP64) or 4 (128, FP32).
+//
+// Global steps (every cell active) launch their own instantiations of the
+// exact face passes, the compute_update / compute_update0 cell passes and
+// (FP32) the limiter and the reconstruction, with more resident blocks: the
+// extra warps hide more of the gathers than the spills cost.  Partial steps
+// keep the instantiations whose bits the persistent rung kernel reproduces:
+// the compiler may contract a multiply and an add differently when the
+// register budget changes, so a kernel compiled to another budget need not
+// give the same last bit.  Measured on the 128^3 blast: exact flux at 4
+// (FP64, 128 registers, about 100 bytes of spills) and 6 (FP32, 80
+// registers): corrector flux 1.32 -> 1.24 ms and 0.85 -> 0.69 ms, predictor
+// 1.19 -> 1.08 and 0.80 -> 0.63.
 #ifndef FVM_FLUX_MINB_D
 #define FVM_FLUX_MINB_D 3
 #endif
 #ifndef FVM_FLUX_MINB_F
 #define FVM_FLUX_MINB_F 4
 #endif
-#ifndef FVM_EXACT_FLUX_MINB_D
-#define FVM_EXACT_FLUX_MINB_D 4
+#ifndef FVM_GLOBAL_FLUX_MINB_D
+#define FVM_GLOBAL_FLUX_MINB_D 4
 #endif
-#ifndef FVM_EXACT_FLUX_MINB_F
-#define FVM_EXACT_FLUX_MINB_F 6
+#ifndef FVM_GLOBAL_FLUX_MINB_F
+#define FVM_GLOBAL_FLUX_MINB_F 6
 #endif
 #define FVM_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_FLUX_MINB_F : FVM_FLUX_MINB_D)
-#define FVM_FLUX_MODE_MINB(R, MODE) \
-  ((MODE) == 0 ? (sizeof(R) == 4 ? FVM_EXACT_FLUX_MINB_F : FVM_EXACT_FLUX_MINB_D) : FVM_FLUX_MINB(R))
+#define FVM_GLOBAL_FLUX_MINB(R) (sizeof(R) == 4 ? FVM_GLOBAL_FLUX_MINB_F : FVM_GLOBAL_FLUX_MINB_D)
 #ifndef FVM_CELL_LFJ
 #define FVM_CELL_LFJ 1  // cell kernels take (face, neighbour) from the link table instead of s12
 #endif
-// Resident blocks per SM that the compute_update and compute_update0 cell
-// passes ask for (FP64 / FP32 bulk).  Measured on the 128^3 blast: FP32
-// corrector cells 1.04 -> 0.78 ms and predictor cells 0.77 -> 0.74 ms at 5
-// (96 registers, a few bytes of spills); FP64 corrector cells 0.970 ->
-// 0.952 ms at 4 (121 registers), FP64 predictor cells best at 1 (123).
+// Resident blocks per SM that the global-step instantiations of the
+// compute_update and compute_update0 cell passes ask for (FP64 / FP32
+// bulk).  Measured on the 128^3 blast: FP32 corrector cells 1.04 -> 0.78 ms
+// and predictor cells 0.77 -> 0.74 ms at 5 (96 registers, a few bytes of
+// spills); FP64 corrector cells 0.970 -> 0.952 ms at 4 (121 registers),
+// FP64 predictor cells best at 1 (123).
 #ifndef FVM_CORR_CELL_MINB_D
 #define FVM_CORR_CELL_MINB_D 4
 #endif
@@ -506,18 +512,20 @@ template <> struct CellTune<double> {
 #define FVM_LIMITER_MINB_D 6
 #endif
   static constexpr int KH_LIM = 2, MINB_LIM = FVM_LIMITER_MINB_D, KH_REC = 2, MINB_REC = FVM_RECON_MINB_D;
+  static constexpr int MINB_LIM_G = MINB_LIM, MINB_REC_G = MINB_REC;  // global steps: the same
 };
 template <> struct CellTune<float> {
-// FP32: 8 blocks for the reconstruction (64 registers, a few spills) and 10
-// for the limiter (46) beat 6 and 8 (128^3 blast: 1.085 -> 1.027 ms and
-// 0.915 -> 0.886 ms).
+// global steps: 8 blocks for the reconstruction (64 registers, a few
+// spills) and 10 for the limiter (46) beat 6 and 8 (128^3 blast: 1.085 ->
+// 1.027 ms and 0.915 -> 0.886 ms)
 #ifndef FVM_RECON_MINB_F
 #define FVM_RECON_MINB_F 8
 #endif
 #ifndef FVM_LIMITER_MINB_F
 #define FVM_LIMITER_MINB_F 10
 #endif
-  static constexpr int KH_LIM = 2, MINB_LIM = FVM_LIMITER_MINB_F, KH_REC = 5, MINB_REC = FVM_RECON_MINB_F;
+  static constexpr int KH_LIM = 2, MINB_LIM = 8, KH_REC = 5, MINB_REC = 6;
+  static constexpr int MINB_LIM_G = FVM_LIMITER_MINB_F, MINB_REC_G = FVM_RECON_MINB_F;
 };
 
 // KH consecutive bulk values from p, as 2-wide loads when KH is even: the
@@ -1117,8 +1125,8 @@ __device__ __forceinline__ void corr_flux_dev(int nf, Params P, const Sched *FVM
     corr_face<R, MODE>(t, -1, t_global, P, S, s12, geo, dr1, fflag, bnd, vel, tlast, Wrec, fst, fcon, fcode, lb);
   }
 }
-template <typename R, int MODE>
-__global__ void __launch_bounds__(128, FVM_FLUX_MODE_MINB(R, MODE)) k_corr_flux(int nf, Params P, const Sched *FVM_RESTRICT S,
+template <typename R, int MODE, int MB = FVM_FLUX_MINB(R)>
+__global__ void __launch_bounds__(128, MB) k_corr_flux(int nf, Params P, const Sched *FVM_RESTRICT S,
     const int2 *FVM_RESTRICT s12, const double4 *FVM_RESTRICT geo, const double4 *FVM_RESTRICT dr1,
     const unsigned char *FVM_RESTRICT fflag, const int *FVM_RESTRICT bnd, const double *FVM_RESTRICT vel,
     const double *FVM_RESTRICT tlast, const R *FVM_RESTRICT Wrec, const R *FVM_RESTRICT fst,
@@ -1392,7 +1400,20 @@ __device__ __forceinline__ void corr_cell_dev(int n, Params P, const Sched *FVM_
                       fcon, fcode, U, dU, stepdU, counters, divb);
 }
 template <typename R>
-__global__ void __launch_bounds__(128, FVM_CORR_CELL_MINB(R)) k_corr_cell(int n, Params P, const Sched *FVM_RESTRICT S,
+__global__ void __launch_bounds__(128) k_corr_cell(int n, Params P, const Sched *FVM_RESTRICT S,
+    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const int2 *FVM_RESTRICT s12,
+    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+    const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast, double *FVM_RESTRICT volp,
+    const R *FVM_RESTRICT Wrec, const R *FVM_RESTRICT tau,
+    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
+    double *FVM_RESTRICT U, double *FVM_RESTRICT dU, double *FVM_RESTRICT stepdU,
+    unsigned long long *FVM_RESTRICT counters, const int *FVM_RESTRICT perm, float *FVM_RESTRICT divb,
+    const int *FVM_RESTRICT clist) {
+  corr_cell_dev<R>(n, P, S, off, lfj, s12, cvol, act, bnd, pos, tlast, volp, Wrec, tau, fcon, fcode, U, dU, stepdU, counters, perm, divb, clist, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+// The same for global steps, with more resident blocks.
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_CORR_CELL_MINB(R)) k_corr_cell_g(int n, Params P, const Sched *FVM_RESTRICT S,
     const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const int2 *FVM_RESTRICT s12,
     const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
     const double *FVM_RESTRICT pos, const double *FVM_RESTRICT tlast, double *FVM_RESTRICT volp,
@@ -2231,8 +2252,8 @@ __device__ __forceinline__ void pred_flux_dev(int nf, Params P,
     pred_face<R, MODE>(t, -1, P, s12, geo, dr1, fflag, bnd, vel, Wst, fcon, fcode, S, rung, lb);
   }
 }
-template <typename R, int MODE>
-__global__ void __launch_bounds__(128, FVM_FLUX_MODE_MINB(R, MODE)) k_pred_flux(int nf, Params P,
+template <typename R, int MODE, int MB = FVM_FLUX_MINB(R)>
+__global__ void __launch_bounds__(128, MB) k_pred_flux(int nf, Params P,
     const int2 *FVM_RESTRICT s12, const double4 *FVM_RESTRICT geo, const double4 *FVM_RESTRICT dr1,
     const unsigned char *FVM_RESTRICT fflag, const int *FVM_RESTRICT bnd,
     const double *FVM_RESTRICT vel, const R *FVM_RESTRICT Wst,
@@ -2339,7 +2360,18 @@ __device__ __forceinline__ void pred_cell_dev(int n, Params P, const Sched *FVM_
                       fcode, rung, tend, Wrec);
 }
 template <typename R>
-__global__ void __launch_bounds__(128, FVM_PRED_CELL_MINB(R)) k_pred_cell(int n, Params P, const Sched *FVM_RESTRICT S,
+__global__ void __launch_bounds__(128) k_pred_cell(int n, Params P, const Sched *FVM_RESTRICT S,
+    const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const int2 *FVM_RESTRICT s12,
+    const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
+    const double *FVM_RESTRICT pos, const double *FVM_RESTRICT U,
+    const R *FVM_RESTRICT fcon, const unsigned char *FVM_RESTRICT fcode,
+    int *FVM_RESTRICT rung, double *FVM_RESTRICT tend, R *FVM_RESTRICT Wrec, const int *FVM_RESTRICT perm,
+    const int *FVM_RESTRICT clist) {
+  pred_cell_dev<R>(n, P, S, off, lfj, s12, cvol, act, bnd, pos, U, fcon, fcode, rung, tend, Wrec, perm, clist, blockIdx.x * blockDim.x + threadIdx.x, gridDim.x * blockDim.x);
+}
+// The same for global steps, with more resident blocks.
+template <typename R>
+__global__ void __launch_bounds__(128, FVM_PRED_CELL_MINB(R)) k_pred_cell_g(int n, Params P, const Sched *FVM_RESTRICT S,
     const int *FVM_RESTRICT off, const int2 *FVM_RESTRICT lfj, const int2 *FVM_RESTRICT s12,
     const double *FVM_RESTRICT cvol, const unsigned char *FVM_RESTRICT act, const int *FVM_RESTRICT bnd,
     const double *FVM_RESTRICT pos, const double *FVM_RESTRICT U,

@@ -876,6 +876,31 @@ static int enq_begin(fvm_ctx *c) {
   return 0;
 }
 
+// The staged limiter, instantiation MINB (resident blocks per SM).  A partial
+// step launches it on a grid of resident blocks (it returns at once unless
+// every cell is active); a global step on one block per cell block.
+extern "C++" {
+template <typename R, int MINB>
+static int limiter_st_launch(fvm_ctx *c) {
+  Dev &d = c->d;
+  constexpr int KH = CellTune<R>::KH_LIM;
+  // the attribute is per device: set once for each device a context uses
+  static bool attr[kMaxDevices] = {};
+  if (c->device < 0 || c->device >= kMaxDevices) { c->err = "device index out of range"; return FVM_EINVAL; }
+  if (!attr[c->device]) {
+    CK(cudaFuncSetAttribute(k_limiter_st<R, KH, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            limiter_stage_bytes<R, KH>()));
+    attr[c->device] = true;
+  }
+  const long long ncb = nblk(c->n, limiter_cst<KH>());
+  const long long grid = c->use_flist ? std::min<long long>(ncb, (long long)MINB * c->sms) : ncb;
+  k_limiter_st<R, KH, MINB><<<(unsigned)grid, 128, limiter_stage_bytes<R, KH>(), c->st>>>(
+      c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
+      (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, c->use_flist, (const R *)d.lld);
+  return 0;
+}
+}  // extern "C++"
+
 static int enq_limiter(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_LIMITER);
@@ -887,36 +912,23 @@ static int enq_limiter(fvm_ctx *c) {
   const bool staged = c->tune.lim_staged != 0;
   if (staged) {
     BULK(({
-      // the attribute is per device: set once on each device a context uses
-      static bool attr[kMaxDevices] = {};
-      if (c->device < 0 || c->device >= kMaxDevices) { c->err = "device index out of range"; return FVM_EINVAL; }
-      if (!attr[c->device]) {
-        CK(cudaFuncSetAttribute(k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                limiter_stage_bytes<R, CellTune<R>::KH_LIM>()));
-        attr[c->device] = true;
-      }
-      // a partial step launches it on a grid of resident blocks (it returns
-      // at once unless every cell is active); a global step on one block per
-      // cell block
-      const long long ncb = nblk(c->n, limiter_cst<CellTune<R>::KH_LIM>());
-      const long long grid = c->use_flist ? std::min<long long>(ncb, (long long)CellTune<R>::MINB_LIM * c->sms) : ncb;
-      k_limiter_st<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
-          <<<(unsigned)grid, 128,
-             limiter_stage_bytes<R, CellTune<R>::KH_LIM>(), c->st>>>(
-          c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
-          (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, c->use_flist, (const R *)d.lld);
+      const int rc = c->use_flist ? limiter_st_launch<R, CellTune<R>::MINB_LIM>(c)
+                                  : limiter_st_launch<R, CellTune<R>::MINB_LIM_G>(c);
+      if (rc) return rc;
     }));
     LAUNCH_CHECK();
   }
   if (!staged || c->use_flist) {
     const int bs = c->tune.bs_cell2;
-    BULK(k_limiter<R, CellTune<R>::KH_LIM, CellTune<R>::MINB_LIM>
-         <<<sgrid(c, (long long)(10 / CellTune<R>::KH_LIM) * c->n, bs), bs, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo,
-                                                              d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec,
-                                                              (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx,
-                                                              d.mz, c->use_flist ? d.clist : nullptr,
-                                                              staged && c->use_flist, (const R *)d.lld));
+#define LIMITER_LIST(MB)                                                                                       \
+  BULK(k_limiter<R, CellTune<R>::KH_LIM, MB>                                                                  \
+       <<<sgrid(c, (long long)(10 / CellTune<R>::KH_LIM) * c->n, bs), bs, 0, c->st>>>(                         \
+           c->n, c->P, d.S, d.off, d.lnk, d.lfj, d.s12, d.geo, d.dr1, d.fflag, d.act, d.tlast, (const R *)d.Wrec, \
+           (R *)d.tau, (R *)d.fst, d.perm, (const R *)d.mnmx, d.mz, c->use_flist ? d.clist : nullptr,          \
+           staged && c->use_flist, (const R *)d.lld))
+    if (c->use_flist) LIMITER_LIST(CellTune<R>::MINB_LIM);
+    else LIMITER_LIST(CellTune<R>::MINB_LIM_G);
+#undef LIMITER_LIST
   }
   LAUNCH_CHECK();
   kt_end(c, KT_LIMITER);
@@ -929,8 +941,8 @@ static int enq_corr_flux(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_CORR_FLUX);
   const LearnBuf &lb = c->lb;
-#define CORR_FLUX(MODE, GRID)                                                                                   \
-  BULK(k_corr_flux<R, MODE><<<GRID, c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, \
+#define CORR_FLUX(MODE, GRID, ...)                                                                              \
+  BULK(k_corr_flux<R, MODE, ##__VA_ARGS__><<<GRID, c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.S, d.s12, d.geo, d.dr1, d.fflag, d.bnd, d.vel, \
                                                      d.tlast, (const R *)d.Wrec, (const R *)d.fst, (R *)d.fcon,   \
                                                      d.fcode, lb, d.flist, c->use_flist))
   if (c->learn_mode == 1) {
@@ -942,8 +954,10 @@ static int enq_corr_flux(fvm_ctx *c) {
     CORR_FLUX(LM_FINISH, nblk(c->nf, c->tune.bs_face));
   } else if (c->learn_mode == 2) {
     CORR_FLUX(LM_HARVEST, sgrid(c, c->nf, c->tune.bs_face));
-  } else {
+  } else if (c->use_flist) {
     CORR_FLUX(LM_EXACT, sgrid(c, c->nf, c->tune.bs_face));
+  } else {  // a global step: the instantiation with more resident blocks
+    CORR_FLUX(LM_EXACT, sgrid(c, c->nf, c->tune.bs_face), FVM_GLOBAL_FLUX_MINB(R));
   }
 #undef CORR_FLUX
   LAUNCH_CHECK();
@@ -954,11 +968,14 @@ static int enq_corr_flux(fvm_ctx *c) {
 static int enq_corr_cell(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_CORR_CELL);
-  BULK(k_corr_cell<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
-                                                          d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,
-                                                          (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU,
-                                                          d.stepdU, d.counters, d.perm, d.divb,
-                                                          c->use_flist ? d.clist : nullptr));
+#define CORR_CELL(K)                                                                                           \
+  BULK(K<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(                                   \
+      c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act, d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,     \
+      (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU, d.stepdU, d.counters, d.perm, d.divb,            \
+      c->use_flist ? d.clist : nullptr))
+  if (c->use_flist) CORR_CELL(k_corr_cell);
+  else CORR_CELL(k_corr_cell_g);  // a global step: more resident blocks
+#undef CORR_CELL
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_CELL);
   return 0;
@@ -1113,8 +1130,8 @@ static int enq_update0(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_FLUX);
   const LearnBuf &lb = c->lb;
-#define PRED_FLUX(MODE, GRID)                                                                                 \
-  BULK(k_pred_flux<R, MODE><<<GRID, c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
+#define PRED_FLUX(MODE, GRID, ...)                                                                            \
+  BULK(k_pred_flux<R, MODE, ##__VA_ARGS__><<<GRID, c->tune.bs_face, 0, c->st>>>(c->nf, c->P, d.s12, d.geo, d.dr1, d.fflag, d.bnd, \
                                                                  d.vel, (const R *)d.Wst, (R *)d.fcon2, d.fcode2, \
                                                                  d.S, d.rung, lb, d.flist, c->use_flist))
   if (c->learn_mode == 1) {
@@ -1126,8 +1143,10 @@ static int enq_update0(fvm_ctx *c) {
     PRED_FLUX(LM_FINISH, nblk(c->nf, c->tune.bs_face));
   } else if (c->learn_mode == 2) {
     PRED_FLUX(LM_HARVEST, sgrid(c, c->nf, c->tune.bs_face));
-  } else {
+  } else if (c->use_flist) {
     PRED_FLUX(LM_EXACT, sgrid(c, c->nf, c->tune.bs_face));
+  } else {  // a global step: the instantiation with more resident blocks
+    PRED_FLUX(LM_EXACT, sgrid(c, c->nf, c->tune.bs_face), FVM_GLOBAL_FLUX_MINB(R));
   }
 #undef PRED_FLUX
   LAUNCH_CHECK();
@@ -1138,16 +1157,24 @@ static int enq_update0(fvm_ctx *c) {
 static int enq_recon(fvm_ctx *c) {
   Dev &d = c->d;
   kt_begin(c, KT_PRED_CELL);
-  BULK(k_pred_cell<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act,
-                                                          d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2, d.rung,
-                                                          d.tend, (R *)d.Wrec, d.perm, c->use_flist ? d.clist : nullptr));
+#define PRED_CELL(K)                                                                                           \
+  BULK(K<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(                                   \
+      c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act, d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2,      \
+      d.rung, d.tend, (R *)d.Wrec, d.perm, c->use_flist ? d.clist : nullptr))
+  if (c->use_flist) PRED_CELL(k_pred_cell);
+  else PRED_CELL(k_pred_cell_g);  // a global step: more resident blocks
+#undef PRED_CELL
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_CELL);
   kt_begin(c, KT_RECON);
-  BULK(k_recon<R, CellTune<R>::KH_REC, CellTune<R>::MINB_REC>
-       <<<sgrid(c, (long long)(10 / CellTune<R>::KH_REC) * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>(
-           c->n, c->P, d.S, d.off, d.lfj, d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung, (R *)d.Wrec, d.perm,
-           (R *)d.mnmx, d.mz, (const R *)d.lrw, (const R *)d.lrd, c->use_flist ? d.clist : nullptr, d.bnb));
+#define RECON(MB)                                                                                              \
+  BULK(k_recon<R, CellTune<R>::KH_REC, MB>                                                                     \
+       <<<sgrid(c, (long long)(10 / CellTune<R>::KH_REC) * c->n, c->tune.bs_cell2), c->tune.bs_cell2, 0, c->st>>>( \
+           c->n, c->P, d.S, d.off, d.lfj, d.cvol, d.act, d.bnd, (const R *)d.Wst, d.rung, (R *)d.Wrec, d.perm,   \
+           (R *)d.mnmx, d.mz, (const R *)d.lrw, (const R *)d.lrd, c->use_flist ? d.clist : nullptr, d.bnb))
+  if (c->use_flist) RECON(CellTune<R>::MINB_REC);
+  else RECON(CellTune<R>::MINB_REC_G);  // a global step: more resident blocks (FP32)
+#undef RECON
   LAUNCH_CHECK();
   kt_end(c, KT_RECON);
   return 0;

@@ -89,17 +89,18 @@ using namespace fvm;
 // Minimum resident 128-thread blocks per SM for the face-flux kernels (caps
 // their registers): 3 (168 registers, FP64) or 4 (128, FP32).
 //
-// Global steps (every cell active) launch their own instantiations of the
-// exact face passes, the compute_update / compute_update0 cell passes and
-// (FP32) the limiter and the reconstruction, with more resident blocks: the
-// extra warps hide more of the gathers than the spills cost.  Partial steps
-// keep the instantiations whose bits the persistent rung kernel reproduces:
-// the compiler may contract a multiply and an add differently when the
-// register budget changes, so a kernel compiled to another budget need not
-// give the same last bit.  Measured on the 128^3 blast: exact flux at 4
-// (FP64, 128 registers, about 100 bytes of spills) and 6 (FP32, 80
-// registers): corrector flux 1.32 -> 1.24 ms and 0.85 -> 0.69 ms, predictor
-// 1.19 -> 1.08 and 0.80 -> 0.63.
+// FP32 global steps (every cell active) launch their own instantiations of
+// the exact face passes, the compute_update / compute_update0 cell passes,
+// the limiter and the reconstruction, with more resident blocks: the extra
+// warps hide more of the gathers than the spills cost (128^3 blast: exact
+// flux at 6 blocks, 80 registers: corrector 0.85 -> 0.69 ms, predictor
+// 0.80 -> 0.63 ms).  Partial steps keep the instantiations whose bits the
+// persistent rung kernel reproduces: the compiler may contract a multiply
+// and an add differently when the register budget changes, so a kernel
+// compiled to another budget need not give the same last bit.  FP64 keeps
+// one set of instantiations: at 4 blocks its face passes were 7-9% faster,
+// but the 32^3 Alfven wave's reconstruction then drifted from the oracle
+// by 1.18e-12 in ten steps, past the 1e-12 parity bound.
 #ifndef FVM_FLUX_MINB_D
 #define FVM_FLUX_MINB_D 3
 #endif
@@ -107,7 +108,7 @@ using namespace fvm;
 #define FVM_FLUX_MINB_F 4
 #endif
 #ifndef FVM_GLOBAL_FLUX_MINB_D
-#define FVM_GLOBAL_FLUX_MINB_D 4
+#define FVM_GLOBAL_FLUX_MINB_D FVM_FLUX_MINB_D
 #endif
 #ifndef FVM_GLOBAL_FLUX_MINB_F
 #define FVM_GLOBAL_FLUX_MINB_F 6
@@ -117,12 +118,11 @@ using namespace fvm;
 #ifndef FVM_CELL_LFJ
 #define FVM_CELL_LFJ 1  // cell kernels take (face, neighbour) from the link table instead of s12
 #endif
-// Resident blocks per SM that the global-step instantiations of the
-// compute_update and compute_update0 cell passes ask for (FP64 / FP32
-// bulk).  Measured on the 128^3 blast: FP32 corrector cells 1.04 -> 0.78 ms
-// and predictor cells 0.77 -> 0.74 ms at 5 (96 registers, a few bytes of
-// spills); FP64 corrector cells 0.970 -> 0.952 ms at 4 (121 registers),
-// FP64 predictor cells best at 1 (123).
+// Resident blocks per SM that the FP32 global-step instantiations of the
+// compute_update and compute_update0 cell passes ask for.  Measured on the
+// 128^3 blast: corrector cells 1.04 -> 0.78 ms and predictor cells 0.77 ->
+// 0.74 ms at 5 (96 registers, a few bytes of spills).  (FP64 global steps
+// launch the partial-step kernels.)
 #ifndef FVM_CORR_CELL_MINB_D
 #define FVM_CORR_CELL_MINB_D 4
 #endif

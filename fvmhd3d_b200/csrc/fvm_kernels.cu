@@ -973,8 +973,8 @@ static int enq_corr_cell(fvm_ctx *c) {
       c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act, d.bnd, d.pos, d.tlast, d.volp, (const R *)d.Wrec,     \
       (const R *)d.tau, (const R *)d.fcon, d.fcode, d.U, d.dU, d.stepdU, d.counters, d.perm, d.divb,            \
       c->use_flist ? d.clist : nullptr))
-  if (c->use_flist) CORR_CELL(k_corr_cell);
-  else CORR_CELL(k_corr_cell_g);  // a global step: more resident blocks
+  if (c->use_flist || !c->fp32) CORR_CELL(k_corr_cell);
+  else CORR_CELL(k_corr_cell_g);  // an FP32 global step: more resident blocks
 #undef CORR_CELL
   LAUNCH_CHECK();
   kt_end(c, KT_CORR_CELL);
@@ -1161,8 +1161,8 @@ static int enq_recon(fvm_ctx *c) {
   BULK(K<R><<<sgrid(c, c->n, c->tune.bs_cell), c->tune.bs_cell, 0, c->st>>>(                                   \
       c->n, c->P, d.S, d.off, d.lfj, d.s12, d.cvol, d.act, d.bnd, d.pos, d.U, (const R *)d.fcon2, d.fcode2,      \
       d.rung, d.tend, (R *)d.Wrec, d.perm, c->use_flist ? d.clist : nullptr))
-  if (c->use_flist) PRED_CELL(k_pred_cell);
-  else PRED_CELL(k_pred_cell_g);  // a global step: more resident blocks
+  if (c->use_flist || !c->fp32) PRED_CELL(k_pred_cell);
+  else PRED_CELL(k_pred_cell_g);  // an FP32 global step: more resident blocks
 #undef PRED_CELL
   LAUNCH_CHECK();
   kt_end(c, KT_PRED_CELL);

@@ -2423,6 +2423,14 @@ int fvm_autotune(fvm_ctx *c, int shared, int steps, int *choice) {
   const bool prof = c->prof;
   const unsigned long long tsys0 = c->tsysU;
   const double t0 = c->t_global;
+  // the trial steps are discarded, so they take no part in a reduction over
+  // ranks (one rank may tune while the others do not)
+  struct ReduceOff {
+    fvm_ctx *c;
+    fvm_reduce_fn fn;
+    ~ReduceOff() { c->reduce = fn; }
+  } reduce_off{c, c->reduce};
+  c->reduce = nullptr;
   // one trial: `steps` eager steps with per-kernel events, then the state back
   auto trial = [&](double *ms_out) -> int {
     int r = fvm_set_profiling(c, 1);

@@ -327,7 +327,8 @@ int fvm_get_harvest(fvm_ctx *c, long long n, float *X, float *Y);
  * limiter variant (face records staged in shared memory or not) and the
  * block sizes of the face kernels, the one-thread-per-cell gathers and the
  * two-threads-per-cell kernels.  choice (4 ints, may be NULL) receives
- * {staged limiter, face block, cell block, two-thread cell block}. */
+ * {staged limiter, face block, cell block, two-thread cell block}.  The
+ * trial steps do not call the reduction of fvm_set_reduce. */
 int fvm_autotune(fvm_ctx *c, int shared, int steps, int *choice);
 
 /* Persistent rung kernel: in steps replayed by fvm_run with individual

@@ -17,7 +17,7 @@ import socket
 import numpy as np
 import pytest
 
-from common import setup_case
+from common import golden_params, load_golden, setup_case
 
 KEYS = ("vel", "tlast", "tend", "rung", "U", "dU", "wrec")
 
@@ -32,28 +32,41 @@ def _case(nside):
     return setup_case(nside, "blast", seed=3, noise=0.02)
 
 
-def _make(engine, dtmax, precision):
+DISK = "ref_disk4k_individual.npz"
+
+
+def _problem(case):
+    """(mesh, W, boundary codes, system parameters) of a blast nside^3
+    (an int) or of the Keplerian disk fixture with its sink cells."""
+    if case == "disk":
+        m, z = load_golden(DISK)
+        return m, z["W"], z.get("bnd"), golden_params(z)
+    m, W = _case(case)
+    return m, W, None, {}
+
+
+def _make(engine, params, precision):
     def make(m):
         if engine == "oracle":
             from oracle.pyoracle import OracleSystem
-            s = OracleSystem(dtmax=dtmax)
+            s = OracleSystem(**params)
         else:
             import fvmhd3d_b200 as F
-            s = F.System(dtmax=dtmax, precision=precision)
+            s = F.System(precision=precision, **params)
         s.set_mesh(m)
         return s
     return make
 
 
-def _worker(rank, world, port, nside, nsteps, engine, dtmax, precision, depth, out):
+def _worker(rank, world, port, case, nsteps, engine, dtmax, precision, depth, out):
     import torch.distributed as dist
     from fvmhd3d_b200 import halo
     dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world)
     try:
-        m, W = _case(nside)
+        m, W, bnd, params = _problem(case)
         owner = halo.partition(m.pos, m.box, world)
-        d = halo.Domain(m, owner, rank, _make(engine, dtmax, precision), depth=depth)
-        d.init_problem(W)
+        d = halo.Domain(m, owner, rank, _make(engine, dict(params, dtmax=dtmax), precision), depth=depth)
+        d.init_problem(W, bnd=bnd)
         for _ in range(nsteps):
             d.step()
         owned, st = d.owned_state()
@@ -62,11 +75,11 @@ def _worker(rank, world, port, nside, nsteps, engine, dtmax, precision, depth, o
         dist.destroy_process_group()
 
 
-def run_partitioned(world, nside, nsteps, engine, dtmax, precision=0, depth=3):
+def run_partitioned(world, case, nsteps, engine, dtmax, precision=0, depth=3):
     import torch.multiprocessing as mp
     mgr = mp.get_context("spawn").Manager()
     out = mgr.dict()
-    mp.start_processes(_worker, args=(world, _free_port(), nside, nsteps, engine, dtmax, precision, depth, out),
+    mp.start_processes(_worker, args=(world, _free_port(), case, nsteps, engine, dtmax, precision, depth, out),
                        nprocs=world, join=True, start_method="spawn")
     return [out[r] for r in range(world)]
 
@@ -84,12 +97,12 @@ def assert_owned_bits(parts, whole, time, ticks, ncell):
     assert seen.all()
 
 
-def oracle_steps(nside, nsteps, dtmax):
+def oracle_steps(case, nsteps, dtmax):
     from oracle.pyoracle import OracleSystem
-    m, W = _case(nside)
-    o = OracleSystem(dtmax=dtmax)
+    m, W, bnd, params = _problem(case)
+    o = OracleSystem(**dict(params, dtmax=dtmax))
     o.set_mesh(m)
-    o.init_problem(W)
+    o.init_problem(W, bnd=bnd)
     for _ in range(nsteps):
         o.step(shared=True)
     return m, o
@@ -120,6 +133,16 @@ def test_partitioned_oracle_steps_give_the_whole_mesh_bits(world):
     nside, nsteps, dtmax = 16, 3, 1e-4
     m, o = oracle_steps(nside, nsteps, dtmax)
     parts = run_partitioned(world, nside, nsteps, "oracle", dtmax)
+    assert_owned_bits(parts, o.get_state(), o.time, o.clock()[0], m.ncell)
+
+
+def test_partitioned_oracle_steps_on_the_disk_with_its_sink():
+    """The Keplerian disk fixture (isothermal gas, moving generators, sink
+    cells with boundary codes): the copies carry their boundary codes and the
+    owned cells keep the whole mesh's bits."""
+    nsteps, dtmax = 3, 0.0625 / 1024
+    m, o = oracle_steps("disk", nsteps, dtmax)
+    parts = run_partitioned(2, "disk", nsteps, "oracle", dtmax)
     assert_owned_bits(parts, o.get_state(), o.time, o.clock()[0], m.ncell)
 
 

@@ -121,22 +121,17 @@ using namespace fvm;
 // Resident blocks per SM that the FP32 global-step instantiations of the
 // compute_update and compute_update0 cell passes ask for.  Measured on the
 // 128^3 blast: corrector cells 1.04 -> 0.78 ms and predictor cells 0.77 ->
-// 0.74 ms at 5 (96 registers, a few bytes of spills).  (FP64 global steps
-// launch the partial-step kernels.)
-#ifndef FVM_CORR_CELL_MINB_D
-#define FVM_CORR_CELL_MINB_D 4
-#endif
+// 0.74 ms at 5 (96 registers, a few bytes of spills).  FP64 global steps
+// launch the partial-step kernels (the FP64 instantiations of the global
+// ones are built but not launched).
 #ifndef FVM_CORR_CELL_MINB_F
 #define FVM_CORR_CELL_MINB_F 5
-#endif
-#ifndef FVM_PRED_CELL_MINB_D
-#define FVM_PRED_CELL_MINB_D 1
 #endif
 #ifndef FVM_PRED_CELL_MINB_F
 #define FVM_PRED_CELL_MINB_F 5
 #endif
-#define FVM_CORR_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CORR_CELL_MINB_F : FVM_CORR_CELL_MINB_D)
-#define FVM_PRED_CELL_MINB(R) (sizeof(R) == 4 ? FVM_PRED_CELL_MINB_F : FVM_PRED_CELL_MINB_D)
+#define FVM_CORR_CELL_MINB(R) (sizeof(R) == 4 ? FVM_CORR_CELL_MINB_F : 1)
+#define FVM_PRED_CELL_MINB(R) (sizeof(R) == 4 ? FVM_PRED_CELL_MINB_F : 1)
 #ifndef FVM_CELL_UNROLL
 #define FVM_CELL_UNROLL 1  // unroll factor of the cell kernels' face loops (1 and 2 time the same within 1%)
 #endif

@@ -128,7 +128,7 @@ def test_local_mesh_keeps_each_owned_cells_face_order():
     assert np.array_equal(p.cells, np.sort(p.cells))
 
 
-@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("world", [2, 3, 4])
 def test_partitioned_oracle_steps_give_the_whole_mesh_bits(world):
     nside, nsteps, dtmax = 16, 3, 1e-4
     m, o = oracle_steps(nside, nsteps, dtmax)
